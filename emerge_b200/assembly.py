@@ -1,0 +1,265 @@
+"""Assembly entry points with EMerge's signatures, computed by libemfem on the GPU.
+
+Drop-in functions (host numpy in, host numpy / SciPy out, as the reference):
+
+* :func:`_matrix_builder`               — ``ASM/curlcurl.py:419-466``
+* :func:`tet_mass_stiffness_matrices`   — ``ASM/curlcurl.py:145-173``
+* :func:`assemble_robin_bc_excited`     — ``ASM/robinbc.py:445-463``
+* :func:`assemble_robin_bc`             — ``ASM/robinbc.py:465-473``
+
+Device-resident building blocks (torch tensors, used by the frequency sweep and the benchmark):
+:class:`DeviceMesh`, :class:`CsrPlan`, :func:`tri_robin_device`.
+
+``ASM/`` = ``src/emerge/_emerge/physics/microwave/assembly/``.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+import torch
+from scipy.sparse import csr_matrix
+
+from . import _lib
+from ._lib import Handle, check, lib, ptr
+
+__all__ = ["DeviceMesh", "CsrPlan", "tet_mass_stiffness_matrices", "_matrix_builder",
+           "assemble_robin_bc", "assemble_robin_bc_excited", "tri_robin_device", "dunavant4"]
+
+
+def _device(device=None) -> torch.device:
+    if device is None:
+        return torch.device("cuda", torch.cuda.current_device())
+    return torch.device(device)
+
+
+def _to_dev(a, dtype, device) -> torch.Tensor:
+    if isinstance(a, torch.Tensor):
+        return a.to(device=device, dtype=dtype).contiguous()
+    return torch.from_numpy(np.ascontiguousarray(a)).to(device=device, dtype=dtype).contiguous()
+
+
+def dunavant4() -> np.ndarray:
+    """Dunavant's degree-4, 6-point triangle rule (4, 6) = [W, L1, L2, L3], in the point order of
+    ``gaus_quad_tri(4)`` (``src/emerge/_emerge/mth/optimized.py:87-118``)."""
+    pts = []
+    for w, l1, l2, l3 in ((0.223381589678011, 0.108103018168070, 0.445948490915965, 0.445948490915965),
+                          (0.109951743655322, 0.816847572980459, 0.091576213509771, 0.091576213509771)):
+        a, b, c = l1, l2, l3
+        for _ in range(3):
+            pts.append([w, a, b, c])
+            a, b, c = b, c, a
+    return np.array(pts, dtype=np.float64).T.copy()
+
+
+class DeviceMesh:
+    """Mesh arrays in HBM, in the reference's (structure-of-arrays) layouts."""
+
+    def __init__(self, mesh, field=None, device=None):
+        dev = _device(device)
+        self.device = dev
+        self.n_nodes, self.n_tets = mesh.nodes.shape[1], mesh.tets.shape[1]
+        self.n_edges, self.n_tris = mesh.edges.shape[1], mesh.tris.shape[1]
+        self.nodes = _to_dev(mesh.nodes, torch.float64, dev)
+        self.tets = _to_dev(mesh.tets, torch.int64, dev)
+        self.tet_to_edge = _to_dev(mesh.tet_to_edge, torch.int64, dev)
+        self.edge_lengths = _to_dev(mesh.edge_lengths, torch.float64, dev)
+        if field is not None:
+            self.tet_to_field = _to_dev(field.tet_to_field, torch.int64, dev)
+        else:
+            ne, nf = self.n_edges, self.n_tris
+            t2e = self.tet_to_edge
+            t2t = _to_dev(mesh.tet_to_tri, torch.int64, dev)
+            self.tet_to_field = torch.cat([t2e, t2t + ne, t2e + ne + nf, t2t + 2 * ne + nf]).contiguous()
+        self._mesh = mesh
+
+    @property
+    def n_field(self) -> int:
+        return 2 * self.n_edges + 2 * self.n_tris
+
+    def check(self) -> None:
+        """Verify the Mesh3D conventions the integrator relies on (raises on mismatch)."""
+        m = self._mesh
+        edges = _to_dev(m.edges, torch.int64, self.device)
+        tris = _to_dev(m.tris, torch.int64, self.device)
+        t2t = _to_dev(m.tet_to_tri, torch.int64, self.device)
+        h = Handle.get(self.device)
+        check(lib().emfem_mesh_check(h.h, self.n_nodes, self.n_tets, self.n_edges, self.n_tris, ptr(self.tets),
+                                     ptr(edges), ptr(tris), ptr(self.tet_to_edge), ptr(t2t)), "emfem_mesh_check")
+        h.raise_on_device_status("emfem_mesh_check")
+
+
+class CsrPlan:
+    """Device symbolic phase (``emfem_plan_*``): the CSR pattern of E/B and the row-owner map used
+    by the fused assembly.  Pattern = union of all tet DOF pairs, sorted, zeros kept."""
+
+    def __init__(self, dmesh: DeviceMesh):
+        self.device = dmesh.device
+        self.dmesh = dmesh
+        h = Handle.get(self.device)
+        p = ctypes.c_void_p()
+        check(lib().emfem_plan_create(h.h, dmesh.n_tets, dmesh.n_edges, dmesh.n_tris, ptr(dmesh.tet_to_field),
+                                      ctypes.byref(p)), "emfem_plan_create")
+        self._p = p
+        n, nnz = ctypes.c_int64(), ctypes.c_int64()
+        check(lib().emfem_plan_info(p, ctypes.byref(n), ctypes.byref(nnz)), "emfem_plan_info")
+        self.n_field, self.nnz = n.value, nnz.value
+        self.indptr = torch.empty(self.n_field + 1, dtype=torch.int32, device=self.device)
+        self.indices = torch.empty(self.nnz, dtype=torch.int32, device=self.device)
+        check(lib().emfem_plan_export_csr(p, ptr(self.indptr), ptr(self.indices)), "emfem_plan_export_csr")
+
+    def __del__(self):
+        p = getattr(self, "_p", None)
+        if p is not None and p.value:
+            try:
+                torch.cuda.synchronize(self.device)
+                lib().emfem_plan_destroy(p)
+            except Exception:
+                pass
+            self._p = None
+
+    def assemble(self, er: torch.Tensor, ur: torch.Tensor, E: torch.Tensor | None = None,
+                 B: torch.Tensor | None = None) -> tuple[torch.Tensor, torch.Tensor]:
+        """Fused integrator + deterministic CSR reduction: E (curl-curl) and B (mass) values."""
+        d = self.dmesh
+        er = _to_dev(er, torch.complex128, self.device)
+        ur = _to_dev(ur, torch.complex128, self.device)
+        if E is None:
+            E = torch.empty(self.nnz, dtype=torch.complex128, device=self.device)
+        if B is None:
+            B = torch.empty(self.nnz, dtype=torch.complex128, device=self.device)
+        h = Handle.get(self.device)
+        check(lib().emfem_plan_assemble(self._p, d.n_nodes, d.n_edges, ptr(d.nodes), ptr(d.tets), ptr(d.tet_to_edge),
+                                        ptr(d.edge_lengths), ptr(ur), ptr(er), ptr(E), ptr(B)), "emfem_plan_assemble")
+        return E, B
+
+    def find_slots(self, rows: torch.Tensor, cols: torch.Tensor) -> torch.Tensor:
+        rows = rows.to(self.device, torch.int64).contiguous()
+        cols = cols.to(self.device, torch.int64).contiguous()
+        out = torch.empty(rows.numel(), dtype=torch.int32, device=self.device)
+        Handle.get(self.device)
+        check(lib().emfem_plan_find_slots(self._p, rows.numel(), ptr(rows), ptr(cols), ptr(out)), "emfem_plan_find_slots")
+        return out
+
+    def to_scipy(self, vals: torch.Tensor) -> csr_matrix:
+        n = self.n_field
+        A = csr_matrix((vals.cpu().numpy(), self.indices.cpu().numpy(), self.indptr.cpu().numpy()), shape=(n, n))
+        A.has_sorted_indices = True
+        return A
+
+
+def _plan_for(field, device) -> tuple[DeviceMesh, CsrPlan]:
+    """Per-field cache of the device mesh and the symbolic plan (built once per mesh)."""
+    key = (str(device), id(field.mesh))
+    cache = getattr(field, "_emfem_cache", None)
+    if cache is None or cache[0] != key:
+        dm = DeviceMesh(field.mesh, field, device)
+        cache = (key, dm, CsrPlan(dm))
+        field._emfem_cache = cache
+    return cache[1], cache[2]
+
+
+def tet_mass_stiffness_matrices(field, er: np.ndarray, ur: np.ndarray, device=None) -> tuple[csr_matrix, csr_matrix]:
+    """Curl-curl (E) and mass (B) CSR matrices of a Nédélec-2 field (``ASM/curlcurl.py:145-173``).
+
+    Same inputs and outputs as the reference: ``er``/``ur`` are (3, 3, N_t) complex tensors; the
+    result is two N×N SciPy CSR matrices with int32 indices, sorted rows and explicit zeros kept.
+    """
+    dev = _device(device)
+    dm, plan = _plan_for(field, dev)
+    E, B = plan.assemble(er, ur)
+    h = Handle.get(dev)
+    h.raise_on_device_status("tet_mass_stiffness_matrices")
+    return plan.to_scipy(E), plan.to_scipy(B)
+
+
+def _matrix_builder(nodes, tets, tris, edges, all_edge_lengths, tet_to_field, tet_to_edge, ur, er, device=None):
+    """Per-tet element matrices and COO indices (``ASM/curlcurl.py:419-466``).
+
+    Returns ``(dataE, dataB, rows, cols)``, 400 entries per tet in row-major local order.  The
+    local edge/face orientation comes from the global node ids; ``edges``/``tris`` are used to
+    verify that the mesh follows the Mesh3D conventions that make this equivalent.
+    """
+    dev = _device(device)
+    nt = tets.shape[1]
+    ne = edges.shape[1]
+    d_nodes = _to_dev(nodes, torch.float64, dev)
+    d_tets = _to_dev(tets, torch.int64, dev)
+    d_t2e = _to_dev(tet_to_edge, torch.int64, dev)
+    d_t2f = _to_dev(tet_to_field, torch.int64, dev)
+    d_el = _to_dev(all_edge_lengths, torch.float64, dev)
+    d_ur = _to_dev(ur, torch.complex128, dev)
+    d_er = _to_dev(er, torch.complex128, dev)
+    h = Handle.get(dev)
+    d_edges = _to_dev(edges, torch.int64, dev)
+    d_tris = _to_dev(tris, torch.int64, dev)
+    d_t2t = (d_t2f[6:10] - ne).contiguous()
+    check(lib().emfem_mesh_check(h.h, nodes.shape[1], nt, ne, tris.shape[1], ptr(d_tets), ptr(d_edges), ptr(d_tris),
+                                 ptr(d_t2e), ptr(d_t2t)), "emfem_mesh_check")
+    dataE = torch.empty(400 * nt, dtype=torch.complex128, device=dev)
+    dataB = torch.empty(400 * nt, dtype=torch.complex128, device=dev)
+    rows = torch.empty(400 * nt, dtype=torch.int64, device=dev)
+    cols = torch.empty(400 * nt, dtype=torch.int64, device=dev)
+    check(lib().emfem_ned2_tet_matrices(h.h, nodes.shape[1], nt, ne, ptr(d_nodes), ptr(d_tets), ptr(d_t2e), ptr(d_el),
+                                        ptr(d_ur), ptr(d_er), ptr(dataE), ptr(dataB)), "emfem_ned2_tet_matrices")
+    check(lib().emfem_ned2_coo_indices(h.h, nt, ptr(d_t2f), ptr(rows), ptr(cols)), "emfem_ned2_coo_indices")
+    h.raise_on_device_status("_matrix_builder")
+    return dataE.cpu().numpy(), dataB.cpu().numpy(), rows.cpu().numpy(), cols.cpu().numpy()
+
+
+def tri_robin_device(dmesh: DeviceMesh, tri_nodes: torch.Tensor, gamma: complex, U: torch.Tensor | None = None,
+                     dpts: torch.Tensor | None = None) -> tuple[torch.Tensor, torch.Tensor | None]:
+    """Per-triangle Robin blocks (n_sel, 64) and, for an excited port, force vectors (n_sel, 8)."""
+    dev = dmesh.device
+    tri_nodes = tri_nodes.to(dev, torch.int64).contiguous()
+    ns = tri_nodes.shape[1]
+    blocks = torch.empty((ns, 64), dtype=torch.complex128, device=dev)
+    bvec = None
+    npts = 0
+    if U is not None:
+        U = U.to(dev, torch.complex128).contiguous()
+        dpts = dpts.to(dev, torch.float64).contiguous()
+        npts = dpts.shape[1]
+        bvec = torch.empty((ns, 8), dtype=torch.complex128, device=dev)
+    h = Handle.get(dev)
+    g = complex(gamma)
+    check(lib().emfem_ned2_tri_robin(h.h, dmesh.n_nodes, ptr(dmesh.nodes), ns, ptr(tri_nodes), g.real, g.imag,
+                                     ptr(U), ptr(dpts), npts, ptr(blocks), ptr(bvec)), "emfem_ned2_tri_robin")
+    return blocks, bvec
+
+
+def _robin_host(field, Bmat, tri_ids, gamma, U, DPTs, device):
+    dev = _device(device)
+    dm, _ = _plan_for(field, dev)
+    tri_ids = np.asarray(tri_ids, dtype=np.int64)
+    tri_nodes = torch.from_numpy(np.ascontiguousarray(field.mesh.tris[:, tri_ids])).to(dev)
+    Ud = None if U is None else torch.from_numpy(np.ascontiguousarray(U)).to(dev)
+    dp = None if DPTs is None else torch.from_numpy(np.ascontiguousarray(DPTs, dtype=np.float64)).to(dev)
+    blocks, bvec = tri_robin_device(dm, tri_nodes, gamma, Ud, dp)
+    Handle.get(dev).raise_on_device_status("robin")
+    blocks = blocks.cpu().numpy()
+    # accumulate in the reference's triangle order (compute_bc_entries*, robinbc.py:294-311, 429-443)
+    np.add.at(Bmat.reshape(-1, 64), tri_ids, blocks)
+    return None if bvec is None else bvec.cpu().numpy()
+
+
+def assemble_robin_bc_excited(field, Bmat: np.ndarray, surf_triangle_indices, Ufunc, gamma, DPTs, device=None):
+    """Robin matrix blocks plus the port force vector (``ASM/robinbc.py:445-463``).
+
+    ``Bmat`` (n_tris·64,) is updated in place and returned with the new force vector (N,)."""
+    tri_ids = np.asarray(surf_triangle_indices, dtype=np.int64)
+    nodes, tris = field.mesh.nodes, field.mesh.tris
+    v = nodes[:, tris[:, tri_ids]]                                 # (3 coords, 3 verts, ns)
+    pts = np.einsum("cvs,vp->cps", v, DPTs[1:4])                   # (3, npts, ns) == generate_points_3d
+    U = np.asarray(Ufunc(pts[0].ravel(), pts[1].ravel(), pts[2].ravel()), dtype=np.complex128)
+    U = U.reshape(3, DPTs.shape[1], len(tri_ids))
+    bv = _robin_host(field, Bmat, tri_ids, gamma, U, DPTs, device)
+    Bvec = np.zeros(field.n_field, dtype=np.complex128)
+    np.add.at(Bvec, field.tri_to_field[:, tri_ids].T.ravel(), bv.ravel())
+    return Bmat, Bvec
+
+
+def assemble_robin_bc(field, Bmat: np.ndarray, surf_triangle_indices, gamma, device=None):
+    """Robin matrix blocks without excitation (``ASM/robinbc.py:465-473``); ``Bmat`` updated in place."""
+    _robin_host(field, Bmat, surf_triangle_indices, gamma, None, None, device)
+    return Bmat

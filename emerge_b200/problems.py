@@ -1,0 +1,87 @@
+"""Seeded synthetic workloads with the shapes, sizes and value distributions of the benchmark
+configurations (no public dataset is involved; meshes come from :func:`mesh.box_tet_mesh`).
+
+* :func:`waveguide`  — air-filled 22.86×10.16×50 mm guide, TE10 ports at z=0 and z=l, PEC on the
+  four side walls (the 6 000-tet small case at 10×5×20).
+* :func:`cavity`     — dielectric-loaded 0.1 m cube, 40³ hex grid (384 000 tets) by default: each tet
+  takes the diagonal εr = εr'(1−j·tanδ) of the last of 8 seeded axis-aligned blocks containing its
+  centroid (air elsewhere), εr' ~ U[1,10], tanδ ~ U[1e-4,1e-2], μr = 1; one TE10 port on z=0 and PEC
+  on every other face.  The configuration names no excitation, so this port is a choice.
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass
+
+import numpy as np
+
+from .mesh import TetMesh, box_tet_mesh
+from .nedelec2 import Nedelec2
+from .ports import PortFrame, RectangularWaveguidePort
+
+
+@dataclass
+class Problem:
+    name: str
+    mesh: TetMesh
+    field: Nedelec2
+    er: np.ndarray          # (3, 3, N_t) complex
+    ur: np.ndarray          # (3, 3, N_t) complex
+    ports: list
+    pec_tris: np.ndarray
+    freqs: np.ndarray
+    dims: tuple
+
+    @property
+    def pec_ids(self) -> np.ndarray:
+        return self.field.pec_dofs(self.pec_tris)
+
+    @property
+    def solve_ids(self) -> np.ndarray:
+        return self.field.solve_ids(self.pec_ids)
+
+
+def identity_tensors(nt: int) -> np.ndarray:
+    t = np.zeros((3, 3, nt), dtype=np.complex128)
+    for i in range(3):
+        t[i, i] = 1.0
+    return t
+
+
+def waveguide(nx=10, ny=5, nz=20, a=22.86e-3, b=10.16e-3, l=50e-3, seed=0, jitter=0.1,
+              freqs=(10e9,), shuffle_local=False) -> Problem:
+    nodes, tets = box_tet_mesh(nx, ny, nz, a, b, l, jitter=jitter, seed=seed, shuffle_local=shuffle_local)
+    mesh = TetMesh(nodes, tets)
+    fld = Nedelec2(mesh)
+    nt = mesh.n_tets
+    ports = [RectangularWaveguidePort(1, PortFrame((a / 2, b / 2, 0.0)), (a, b), mesh.tris_on_plane(2, 0.0)),
+             RectangularWaveguidePort(2, PortFrame((a / 2, b / 2, l)), (a, b), mesh.tris_on_plane(2, l))]
+    walls = np.concatenate([mesh.tris_on_plane(0, 0.0), mesh.tris_on_plane(0, a),
+                            mesh.tris_on_plane(1, 0.0), mesh.tris_on_plane(1, b)])
+    return Problem("waveguide", mesh, fld, identity_tensors(nt), identity_tensors(nt), ports, walls,
+                   np.asarray(freqs, dtype=np.float64), (a, b, l))
+
+
+def cavity(n=40, L=0.1, seed=0, jitter=0.1, nblocks=8, nfreq=101, fmin=2e9, fmax=6e9) -> Problem:
+    nodes, tets = box_tet_mesh(n, n, n, L, L, L, jitter=jitter, seed=seed)
+    mesh = TetMesh(nodes, tets)
+    fld = Nedelec2(mesh)
+    nt = mesh.n_tets
+    rng = np.random.default_rng(seed + 1000)
+    cen = (nodes[:, tets[0]] + nodes[:, tets[1]] + nodes[:, tets[2]] + nodes[:, tets[3]]) / 4
+    eps = np.ones(nt, dtype=np.complex128)
+    for _ in range(nblocks):
+        lo = rng.uniform(0, 0.7 * L, 3)
+        hi = lo + rng.uniform(0.15 * L, 0.5 * L, 3)
+        epr = rng.uniform(1.0, 10.0)
+        tand = rng.uniform(1e-4, 1e-2)
+        inside = np.all((cen >= lo[:, None]) & (cen <= hi[:, None]), axis=0)
+        eps[inside] = epr * (1 - 1j * tand)
+    er = np.zeros((3, 3, nt), dtype=np.complex128)
+    for i in range(3):
+        er[i, i] = eps
+    port_tris = mesh.tris_on_plane(2, 0.0)
+    ports = [RectangularWaveguidePort(1, PortFrame((L / 2, L / 2, 0.0)), (L, L), port_tris)]
+    walls = np.concatenate([mesh.tris_on_plane(0, 0.0), mesh.tris_on_plane(0, L), mesh.tris_on_plane(1, 0.0),
+                            mesh.tris_on_plane(1, L), mesh.tris_on_plane(2, L)])
+    return Problem("cavity", mesh, fld, er, identity_tensors(nt), ports, walls,
+                   np.linspace(fmin, fmax, nfreq), (L, L, L))

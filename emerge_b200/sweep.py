@@ -1,0 +1,204 @@
+"""Device-resident frequency sweep: assembly once, then batched COCG solves of
+K_f = E − k0_f²·B + Σ_p γ_p(k0_f)·R̂_p with port excitations b_{f,p} = s_p(k0_f)·b̂_p.
+
+This is the GPU counterpart of ``Microwave3D.run_sweep`` → ``Assembler.assemble_freq_matrix`` →
+``SimJob.iter_Ab`` → ``SolveRoutine.solve`` (``MW/microwave_3d.py:663-878``,
+``ASM/assembler.py:189-429``, ``MW/simjob.py:82-107``, ``src/emerge/_emerge/solver.py:1241-1326``):
+
+* E/B come from the fused plan assembly (``CsrPlan``) and are shared by every frequency;
+* each port's Robin matrix is linear in γ (``ASM/robinbc.py:126-292``: Bmat·γ/(2A)²), so R̂_p is
+  assembled once with γ = 1 and scaled per frequency inside the SpMV;
+* the port force vector is linear in U_inc = s_p(k0)·shape (``MW/microwave_bc.py:864-883``), so b̂_p
+  is assembled once from the unit mode shape;
+* PEC DOFs (``ASM/assembler.py:274-307``) are a free-DOF mask, the exact equivalent of the
+  reference's submatrix elimination.
+
+``MW/`` = ``src/emerge/_emerge/physics/microwave/``; ``ASM/`` = ``MW/assembly/``.
+"""
+from __future__ import annotations
+
+import ctypes
+import time
+from dataclasses import dataclass
+
+import numpy as np
+import torch
+
+from ._lib import Handle, check, lib, ptr, ERR_NOT_CONVERGED
+from .assembly import CsrPlan, DeviceMesh, dunavant4, tri_robin_device
+from .ports import k0_of
+
+PRECOND = {"none": 0, "jacobi": 1, "block_jacobi": 2}
+PRECISION = {"fp64": 0, "mixed": 1}
+
+
+def _seg_from_keys(keys: np.ndarray):
+    """Stable grouping of equal keys: (unique_keys, seg (n_u+1), idx) with contributions in
+    original order inside each group."""
+    order = np.argsort(keys, kind="stable")
+    ks = keys[order]
+    first = np.ones(len(ks), dtype=bool)
+    first[1:] = ks[1:] != ks[:-1]
+    starts = np.flatnonzero(first)
+    seg = np.append(starts, len(ks)).astype(np.int32)
+    return ks[starts], seg, order.astype(np.int32)
+
+
+def gather_sum(seg: torch.Tensor, idx: torch.Tensor, src: torch.Tensor) -> torch.Tensor:
+    n_out = seg.numel() - 1
+    out = torch.empty(n_out, dtype=torch.complex128, device=src.device)
+    h = Handle.get(src.device)
+    check(lib().emfem_segmented_gather_sum(h.h, n_out, ptr(seg), ptr(idx), ptr(src.contiguous()), ptr(out)),
+          "emfem_segmented_gather_sum")
+    return out
+
+
+@dataclass
+class SolveResult:
+    x: torch.Tensor          # (N, nsys) complex128, device
+    status: np.ndarray
+    iters: np.ndarray
+    relres: np.ndarray
+    systems: list
+    seconds: float
+
+
+class FrequencySweep:
+    def __init__(self, problem, device=None, assemble: bool = True):
+        dev = torch.device("cuda", torch.cuda.current_device()) if device is None else torch.device(device)
+        self.device = dev
+        self.problem = problem
+        fld, mesh = problem.field, problem.mesh
+        self.dmesh = DeviceMesh(mesh, fld, dev)
+        self.plan = CsrPlan(self.dmesh)
+        self.n = self.plan.n_field
+        self.er = torch.from_numpy(np.ascontiguousarray(problem.er)).to(dev)
+        self.ur = torch.from_numpy(np.ascontiguousarray(problem.ur)).to(dev)
+        self.E = self.B = None
+        if assemble:
+            self.assemble()
+        self._build_ports()
+        mask = np.ones(self.n, dtype=np.uint8)
+        mask[problem.pec_ids] = 0
+        self.mask = torch.from_numpy(mask).to(dev)
+        self._ws = None
+
+    def assemble(self):
+        self.E, self.B = self.plan.assemble(self.er, self.ur, self.E, self.B)
+        return self.E, self.B
+
+    def _build_ports(self):
+        P, fld, mesh, dev = self.problem, self.problem.field, self.problem.mesh, self.device
+        dp = dunavant4()
+        self.dpts = torch.from_numpy(dp).to(dev)
+        N = self.n
+        blocks_all, meta_rows, meta_cols, meta_port = [], [], [], []
+        self.bhat = []
+        nports = len(P.ports)
+        off = 0
+        for q, port in enumerate(P.ports):
+            tid = np.asarray(port.tri_ids, dtype=np.int64)
+            tn = mesh.tris[:, tid]
+            v = mesh.nodes[:, tn]                                     # (3, 3, ns)
+            pts = np.einsum("cvs,vp->cps", v, dp[1:4])                # (3, npts, ns)
+            U = port.shape_global(pts[0], pts[1], pts[2]).astype(np.complex128)   # (3, npts, ns)
+            blocks, bvec = tri_robin_device(self.dmesh, torch.from_numpy(np.ascontiguousarray(tn)).to(dev), 1.0,
+                                            torch.from_numpy(np.ascontiguousarray(U)).to(dev), self.dpts)
+            t2f = fld.tri_to_field[:, tid]                            # (8, ns)
+            rows = np.repeat(t2f.T, 8, axis=1).ravel()                # entry 8a+b -> row t2f[a]
+            cols = np.tile(t2f.T, (1, 8)).ravel()                     # col t2f[b]
+            blocks_all.append(blocks.reshape(-1))
+            meta_rows.append(rows); meta_cols.append(cols); meta_port.append(np.full(rows.shape, q))
+            # port vector b̂_q: Bvec[tri_to_field[:, t]] += bvec[t] in triangle order
+            dofs = t2f.T.ravel()
+            ud, seg, idx = _seg_from_keys(dofs)
+            vals = gather_sum(torch.from_numpy(seg).to(dev), torch.from_numpy(idx).to(dev), bvec.reshape(-1))
+            bh = torch.zeros(N, dtype=torch.complex128, device=dev)
+            bh[torch.from_numpy(ud).to(dev)] = vals
+            self.bhat.append(bh)
+            off += len(rows)
+        rows = np.concatenate(meta_rows); cols = np.concatenate(meta_cols); port = np.concatenate(meta_port)
+        src = torch.cat(blocks_all)
+        keys = (rows * nports + port) * N + cols
+        uk, seg, idx = _seg_from_keys(keys)
+        self.patch_vals = gather_sum(torch.from_numpy(seg).to(dev), torch.from_numpy(idx).to(dev), src)
+        u_rows = uk // (nports * N)
+        u_port = (uk // N) % nports
+        u_cols = uk % N
+        prow, pstart = np.unique(u_rows, return_index=True)
+        self.patch_rows = torch.from_numpy(prow.astype(np.int32)).to(dev)
+        self.patch_rowptr = torch.from_numpy(np.append(pstart, len(uk)).astype(np.int32)).to(dev)
+        self.patch_cols = torch.from_numpy(u_cols.astype(np.int32)).to(dev)
+        self.patch_port = torch.from_numpy(u_port.astype(np.int32)).to(dev)
+        self.n_ports = nports
+
+    # ---------------------------------------------------------------- per-frequency data
+    def k0sq(self, freqs) -> np.ndarray:
+        return np.array([k0_of(f) ** 2 for f in freqs])
+
+    def gammas(self, freqs) -> np.ndarray:
+        """(nsys, n_ports) complex γ of every port at every frequency."""
+        return np.array([[complex(p.get_gamma(k0_of(f))) for p in self.problem.ports] for f in freqs])
+
+    def rhs(self, systems) -> torch.Tensor:
+        """(N, nsys) right-hand sides b + port_vector[p] (``MW/simjob.py:88-92``, b = 0)."""
+        cols = []
+        for f, q in systems:
+            s = self.problem.ports[q].uinc_scale(k0_of(f))
+            cols.append(self.bhat[q] * s)
+        return torch.stack(cols, dim=1).contiguous()
+
+    def workspace(self, nsys: int, precision: int) -> torch.Tensor:
+        sz = ctypes.c_size_t()
+        check(lib().emfem_cocg_workspace_size(self.n, self.plan.nnz, nsys, precision, ctypes.byref(sz)),
+              "emfem_cocg_workspace_size")
+        if self._ws is None or self._ws.numel() < sz.value:
+            self._ws = torch.empty(sz.value, dtype=torch.uint8, device=self.device)
+        return self._ws
+
+    def solve(self, systems, tol: float = 1e-8, maxit: int = 20000, precond: str = "block_jacobi",
+              precision: str = "fp64", x0: torch.Tensor | None = None, raise_on_fail: bool = False) -> SolveResult:
+        """Solve the listed (frequency, port index) systems in one batched COCG call (<= 64)."""
+        nsys = len(systems)
+        assert 1 <= nsys <= 64
+        freqs = [f for f, _ in systems]
+        k0 = self.k0sq(freqs)
+        g = self.gammas(freqs)
+        gam = np.ascontiguousarray(np.stack([g.real, g.imag], axis=-1).reshape(-1))
+        b = self.rhs(systems)
+        x = torch.zeros_like(b) if x0 is None else x0.clone().contiguous()
+        prec = PRECISION[precision]
+        ws = self.workspace(nsys, prec)
+        status = (ctypes.c_int * nsys)()
+        iters = (ctypes.c_int * nsys)()
+        relres = (ctypes.c_double * nsys)()
+        k0a = (ctypes.c_double * nsys)(*k0)
+        ga = (ctypes.c_double * len(gam))(*gam)
+        h = Handle.get(self.device)
+        t0 = time.perf_counter()
+        st = lib().emfem_cocg_solve(h.h, self.n, self.plan.nnz, ptr(self.plan.indptr), ptr(self.plan.indices),
+                                    ptr(self.E), ptr(self.B), nsys, k0a,
+                                    self.patch_rows.numel(), ptr(self.patch_rows), ptr(self.patch_rowptr),
+                                    ptr(self.patch_cols), ptr(self.patch_vals), ptr(self.patch_port), self.n_ports, ga,
+                                    ptr(self.mask), ptr(b), ptr(x), tol, maxit, PRECOND[precond], prec,
+                                    ptr(ws), ws.numel(), status, iters, relres)
+        dt = time.perf_counter() - t0
+        if st not in (0, ERR_NOT_CONVERGED) or (raise_on_fail and st != 0):
+            check(st, "emfem_cocg_solve")
+        return SolveResult(x, np.array(status[:]), np.array(iters[:]), np.array(relres[:]), list(systems), dt)
+
+    def apply(self, systems, x: torch.Tensor) -> torch.Tensor:
+        """y = K_f x for each system (FP64; PEC rows/cols eliminated)."""
+        nsys = len(systems)
+        freqs = [f for f, _ in systems]
+        k0 = torch.from_numpy(self.k0sq(freqs)).to(self.device)
+        g = self.gammas(freqs)
+        gam = torch.from_numpy(np.ascontiguousarray(np.stack([g.real, g.imag], axis=-1).reshape(-1))).to(self.device)
+        y = torch.empty_like(x)
+        h = Handle.get(self.device)
+        check(lib().emfem_sweep_spmv(h.h, self.n, ptr(self.plan.indptr), ptr(self.plan.indices), ptr(self.E),
+                                     ptr(self.B), nsys, ptr(k0), self.patch_rows.numel(), ptr(self.patch_rows),
+                                     ptr(self.patch_rowptr), ptr(self.patch_cols), ptr(self.patch_vals),
+                                     ptr(self.patch_port), self.n_ports, ptr(gam), ptr(self.mask), ptr(x.contiguous()),
+                                     ptr(y)), "emfem_sweep_spmv")
+        return y

@@ -1,0 +1,162 @@
+/*
+ * libemfem — B200 (sm_100a) kernels for EMerge's Nedelec-2 FEM hot path, behind a C ABI.
+ *
+ * Every pointer argument named *_dev (or documented as "device") is a device pointer on the
+ * handle's device; "host" arrays are plain host memory.  Complex numbers are interleaved
+ * (re, im) float64 pairs, the memory layout of numpy/torch complex128.  Arrays follow the
+ * reference's layouts: nodes (3, N_n) f64, tets (4, N_t) i64, tet_to_edge (6, N_t) i64,
+ * tet_to_field (20, N_t) i64, er/ur (3, 3, N_t) c128 — all row-major, i.e. structure-of-arrays
+ * over elements.  All calls are asynchronous on the handle's stream unless stated otherwise and
+ * return an int status (EMFEM_OK = 0, negative on error); emfem_last_error() gives the text.
+ *
+ * Reference paths below are relative to the EMerge source tree; ASM/ =
+ * src/emerge/_emerge/physics/microwave/assembly/.
+ */
+#ifndef EMFEM_H
+#define EMFEM_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define EMFEM_OK 0
+#define EMFEM_ERR_INVALID_ARG -1   /* bad size, null pointer, unsupported option */
+#define EMFEM_ERR_CUDA -2          /* a CUDA runtime call failed */
+#define EMFEM_ERR_DEVICE_CHECK -3  /* a kernel's own bounds / consistency check fired */
+#define EMFEM_ERR_WORKSPACE -4     /* caller-provided workspace too small */
+#define EMFEM_ERR_NOT_CONVERGED -5 /* iterative solve hit its iteration cap or broke down */
+
+/* Device status bits reported by emfem_device_status(). */
+#define EMFEM_DEV_BAD_INDEX 1
+#define EMFEM_DEV_DEGENERATE 2
+#define EMFEM_DEV_NONFINITE 4
+#define EMFEM_DEV_CAPACITY 8
+#define EMFEM_DEV_BREAKDOWN 16
+
+typedef struct emfem_handle_s *emfem_handle;
+typedef struct emfem_plan_s *emfem_plan;
+
+/* ---- library / handle ------------------------------------------------------------------- */
+int emfem_version(void);
+/* Copies the calling thread's last error message (NUL-terminated, truncated to len). */
+int emfem_last_error(char *buf, size_t len);
+/* stream: a cudaStream_t (NULL = legacy default stream). */
+int emfem_create(emfem_handle *h, int device, void *stream);
+int emfem_set_stream(emfem_handle h, void *stream);
+int emfem_destroy(emfem_handle h);
+/* Synchronises the stream, returns the sticky device status bits (EMFEM_DEV_*) and clears them. */
+int emfem_device_status(emfem_handle h, int *status);
+
+/* ---- per-element integrator -------------------------------------------------------------
+ * Replaces the numeric part of _matrix_builder (ASM/curlcurl.py:419-466), i.e. per tet
+ * ned2_tet_stiff_mass(..., matinv(ur), er) (ASM/curlcurl.py:180-412).  Writes, for every tet t,
+ * the row-major 20x20 curl-curl matrix to E_out[400 t ...] and the mass matrix to B_out, exactly
+ * the reference's dataE/dataB.  Local edge/face orientation is taken from the global node ids
+ * of `tets`, which is what the reference's local_mapping of the sorted edge/triangle node lists
+ * yields for a mesh in Mesh3D conventions (mesh3d.py:387-497).
+ * All arrays device.  edge_lengths has n_edges entries (indexed through tet_to_edge). */
+int emfem_ned2_tet_matrices(emfem_handle h, int64_t n_nodes, int64_t n_tets, int64_t n_edges,
+                            const double *nodes, const int64_t *tets, const int64_t *tet_to_edge,
+                            const double *edge_lengths, const void *ur, const void *er,
+                            void *E_out, void *B_out);
+
+/* COO row/column indices of _matrix_builder (ASM/curlcurl.py:459-465): for k = 20 i + j of tet t,
+ * rows[400 t + k] = tet_to_field[i, t], cols[400 t + k] = tet_to_field[j, t].  Device arrays. */
+int emfem_ned2_coo_indices(emfem_handle h, int64_t n_tets, const int64_t *tet_to_field,
+                           int64_t *rows, int64_t *cols);
+
+/* Mesh consistency check against the Mesh3D conventions the integrator relies on
+ * (mesh3d.py:395-441): edges[:, tet_to_edge[e, t]] is the sorted pair of local vertices e and
+ * tris[:, tet_to_tri[f, t]] the sorted triple of local face f.  Sets EMFEM_DEV_BAD_INDEX on a
+ * mismatch or out-of-range id; read it with emfem_device_status().  Device arrays. */
+int emfem_mesh_check(emfem_handle h, int64_t n_nodes, int64_t n_tets, int64_t n_edges, int64_t n_tris,
+                     const int64_t *tets, const int64_t *edges, const int64_t *tris,
+                     const int64_t *tet_to_edge, const int64_t *tet_to_tri);
+
+/* ---- CSR plan (symbolic phase) + fused assembly -----------------------------------------
+ * Replaces tet_mass_stiffness_matrices (ASM/curlcurl.py:145-173): the COO emission of
+ * _matrix_builder plus coo_matrix(...).tocsr() with duplicate summation.  The plan is built once
+ * per mesh on the device from tet_to_field (device, (20, n_tets) i64): the pattern is the union of
+ * all tet DOF pairs, rows sorted, explicit zeros kept — bit-identical to SciPy's tocsr() of the
+ * reference's COO.  n_field = 2 n_edges + 2 n_tris.  The plan owns its device memory. */
+int emfem_plan_create(emfem_handle h, int64_t n_tets, int64_t n_edges, int64_t n_tris,
+                      const int64_t *tet_to_field, emfem_plan *plan);
+int emfem_plan_info(emfem_plan plan, int64_t *n_field, int64_t *nnz);
+int emfem_plan_destroy(emfem_plan plan);
+/* indptr (n_field + 1) and indices (nnz), int32, device. */
+int emfem_plan_export_csr(emfem_plan plan, int32_t *indptr, int32_t *indices);
+/* Fused integrate + deterministic segmented reduction: writes the CSR values of E (curl-curl) and
+ * B (mass), nnz complex each, device.  Every CSR slot is the sum of its tets' contributions in
+ * ascending tet order, so repeated calls are bit-identical.  Inputs as emfem_ned2_tet_matrices. */
+int emfem_plan_assemble(emfem_plan plan, int64_t n_nodes, int64_t n_edges, const double *nodes,
+                        const int64_t *tets, const int64_t *tet_to_edge, const double *edge_lengths,
+                        const void *ur, const void *er, void *E_vals, void *B_vals);
+/* CSR slot of each (row, col) pair (device int64 arrays of length n), -1 where absent. */
+int emfem_plan_find_slots(emfem_plan plan, int64_t n, const int64_t *rows, const int64_t *cols,
+                          int32_t *slots);
+
+/* ---- Robin / port triangles ----------------------------------------------------------------
+ * Replaces ned2_tri_stiff_force / ned2_tri_stiff (ASM/robinbc.py:126-292, :314-427) for a batch of
+ * boundary triangles.  tri_nodes: (3, n_sel) i64 global node ids of the selected triangles (the
+ * reference's tris[:, surf_triangle_indices]); U: (3, npts, n_sel) c128 incident field at the
+ * quadrature points as assemble_robin_bc_excited reshapes it (ASM/robinbc.py:445-463), or NULL;
+ * dpts: (4, npts) f64 [W, L1, L2, L3] with npts <= 16.  Outputs: blocks (n_sel, 64) c128 — the
+ * row-major 8x8 γ-scaled matrices — and, when U is given, bvec (n_sel, 8) c128.  Device arrays. */
+int emfem_ned2_tri_robin(emfem_handle h, int64_t n_nodes, const double *nodes, int64_t n_sel,
+                         const int64_t *tri_nodes, double gamma_re, double gamma_im,
+                         const void *U, const double *dpts, int npts, void *blocks, void *bvec);
+
+/* Deterministic segmented sum: out[i] = sum_{k=seg[i]}^{seg[i+1]-1} src[idx[k]] in k order
+ * (complex128, device).  Used to scatter Robin blocks and port vectors onto CSR slots / DOFs. */
+int emfem_segmented_gather_sum(emfem_handle h, int64_t n_out, const int32_t *seg, const int32_t *idx,
+                               const void *src, void *out);
+
+/* ---- frequency-sweep system ------------------------------------------------------------------
+ * K = (E - k0^2 B) on the plan pattern, then K[patch_slot[i]] += gamma * patch_vals[i]
+ * (ASM/assembler.py:255 and :349-350).  Device arrays; nnz complex each. */
+int emfem_sweep_combine(emfem_handle h, int64_t nnz, const void *E_vals, const void *B_vals, double k0sq,
+                        int64_t n_patch, const int32_t *patch_slot, const void *patch_vals,
+                        double gamma_re, double gamma_im, void *K_vals);
+
+/* ---- batched COCG solver ---------------------------------------------------------------------
+ * Solves nsys complex-symmetric systems A_s x_s = b_s on one CSR pattern, replacing the
+ * per-frequency direct solve (SolverSuperLU, src/emerge/_emerge/solver.py:535-572, reached through
+ * SolveRoutine.solve :1241-1326).  A_s = E - k0sq[s] * B + sum_p gamma[s, p] * R_p, where B may be
+ * NULL (then A_s = E + ...), and the Robin terms R_p are given as a small row-compressed "patch"
+ * (patch_rowptr over patch_rows, patch_cols, patch_vals, patch_port).  Rows/columns where
+ * free_mask == 0 are eliminated exactly as SolveRoutine's submatrix A[ids, ids] (solution zero).
+ * Vectors are (n, nsys) c128, DOF-major (entry (i, s) at i * nsys + s).  x is the initial guess on
+ * entry (zero for the reference's behaviour) and the solution on exit.
+ *   precond: 0 none, 1 point Jacobi, 2 block Jacobi on DOF pairs (i, i + n/2) — the first- and
+ *            second-kind DOFs of one edge/face (elements/nedelec2.py:42-58).
+ *   precision: 0 = FP64 COCG; 1 = FP32 inner COCG inside FP64 iterative refinement (FP64 true
+ *            residual and solution update).
+ * Host outputs per system: status (0 converged, 1 iteration cap, 2 breakdown), iters, relres
+ * (FP64 true relative residual ||b - A x|| / ||b||).  workspace (device) must hold
+ * emfem_cocg_workspace_size() bytes.  Synchronises the stream. */
+int emfem_cocg_workspace_size(int64_t n, int64_t nnz, int nsys, int precision, size_t *bytes);
+int emfem_cocg_solve(emfem_handle h, int64_t n, int64_t nnz, const int32_t *indptr, const int32_t *indices,
+                     const void *E_vals, const void *B_vals, int nsys, const double *k0sq,
+                     int64_t n_patch_rows, const int32_t *patch_rows, const int32_t *patch_rowptr,
+                     const int32_t *patch_cols, const void *patch_vals, const int32_t *patch_port,
+                     int n_ports, const double *gamma,
+                     const uint8_t *free_mask, const void *rhs, void *x,
+                     double tol, int maxit, int precond, int precision,
+                     void *workspace, size_t workspace_bytes,
+                     int *status, int *iters, double *relres);
+
+/* y_s = A_s x_s for the operator of emfem_cocg_solve (FP64), with eliminated rows/cols as there. */
+int emfem_sweep_spmv(emfem_handle h, int64_t n, const int32_t *indptr, const int32_t *indices,
+                     const void *E_vals, const void *B_vals, int nsys, const double *k0sq_dev,
+                     int64_t n_patch_rows, const int32_t *patch_rows, const int32_t *patch_rowptr,
+                     const int32_t *patch_cols, const void *patch_vals, const int32_t *patch_port,
+                     int n_ports, const double *gamma_dev, const uint8_t *free_mask,
+                     const void *x, void *y);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,202 @@
+"""Generate the golden fixtures in this folder by running EMerge's own numba code.
+
+Run in a container that has the reference checkout (``EMERGE_REFERENCE_SRC``, default the
+``src/emerge`` of the read-only checkout); the GPU box never runs this file, it only reads the
+``.npz`` files it wrote.  First numba compile takes about a minute.
+
+    python tests/golden/make_golden.py
+
+Fixtures
+--------
+``element_small.npz``  72-tet box, shuffled local vertex order, general complex 3×3 εr
+    (non-symmetric) and μr (half diagonal, half full): ``_matrix_builder`` COO output
+    (``ASM/curlcurl.py:419-466``) and the E/B CSR of ``tet_mass_stiffness_matrices`` (``:145-173``).
+``robin_small.npz``    the same mesh's z=0 face through ``assemble_robin_bc_excited`` and its z=l face
+    through ``assemble_robin_bc`` (``ASM/robinbc.py:445-473``) with a reference ``RectangularWaveguide``
+    TE10 port's γ and U_inc (``MW/microwave_bc.py:846-866``).
+``config1.npz``        the 6 000-tet air waveguide (10×5×20 hex grid, 22.86×10.16×50 mm, seed 0) at
+    10 GHz with TE10 ports at z=0 and z=l and PEC on the four walls: E/B/K CSR checksums and sampled
+    slots, port vectors, both SuperLU solutions (``E/solver.py:561-572`` through the
+    ``SolveRoutine.solve`` submatrix path ``:1266-1313``) and the raw S-matrix from the reference's
+    ``sparam_field_power``/``sparam_mode_power`` (``MW/sparam.py:71-138``).
+
+``ASM/`` = ``src/emerge/_emerge/physics/microwave/assembly/``; ``MW/`` = ``src/emerge/_emerge/physics/microwave/``.
+"""
+from __future__ import annotations
+
+import hashlib
+import os
+import sys
+import time
+import types
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
+sys.path.insert(0, HERE)
+
+import reference_import  # noqa: E402
+from emerge_b200.mesh import box_tet_mesh, TetMesh  # noqa: E402
+from emerge_b200 import constants as K  # noqa: E402
+
+R = reference_import.load()
+
+
+def sha(a: np.ndarray) -> str:
+    return hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()
+
+
+def random_tensors(rng, nt, kind):
+    """Complex 3×3 tensors (3, 3, N_t)."""
+    if kind == "full":
+        t = rng.uniform(0.5, 2.0, (3, 3, nt)) + 1j * rng.uniform(-0.3, 0.3, (3, 3, nt))
+        for i in range(3):
+            t[i, i] += 3.0
+        return t
+    if kind == "diag":
+        t = np.zeros((3, 3, nt), dtype=np.complex128)
+        for i in range(3):
+            t[i, i] = rng.uniform(1.0, 4.0, nt) - 1j * rng.uniform(0.0, 0.2, nt)
+        return t
+    raise ValueError(kind)
+
+
+def make_port(pnum, origin, dims):
+    cs = R.cs.CoordinateSystem(R.cs.Axis(np.array([1.0, 0, 0])), R.cs.Axis(np.array([0, 1.0, 0])),
+                               R.cs.Axis(np.array([0, 0, 1.0])), np.array(origin, dtype=np.float64))
+    return R.bc.RectangularWaveguide(types.SimpleNamespace(tags=[pnum]), pnum, (1, 0), 1.0, cs, dims)
+
+
+def element_small():
+    nodes, tets = box_tet_mesh(2, 2, 3, 1.0e-2, 0.8e-2, 1.3e-2, jitter=0.15, seed=11, shuffle_local=True)
+    mesh = TetMesh(nodes, tets)
+    fld = R.nedelec2.Nedelec2(mesh)
+    rng = np.random.default_rng(5)
+    nt = mesh.n_tets
+    er = random_tensors(rng, nt, "full")
+    ur = random_tensors(rng, nt, "full")
+    ur_diag = random_tensors(rng, nt, "diag")
+    ur[:, :, ::2] = ur_diag[:, :, ::2]
+    dataE, dataB, rows, cols = R.curlcurl._matrix_builder(
+        mesh.nodes, mesh.tets, mesh.tris, mesh.edges, mesh.edge_lengths, fld.tet_to_field,
+        mesh.tet_to_edge, ur, er)
+    E, B = R.curlcurl.tet_mass_stiffness_matrices(fld, er, ur)
+    np.savez_compressed(os.path.join(HERE, "element_small.npz"),
+                        nodes=mesh.nodes, tets=mesh.tets, er=er, ur=ur,
+                        dataE=dataE, dataB=dataB, rows=rows, cols=cols,
+                        E_indptr=E.indptr, E_indices=E.indices, E_data=E.data,
+                        B_indptr=B.indptr, B_indices=B.indices, B_data=B.data)
+    return mesh, fld
+
+
+def robin_small(mesh, fld):
+    a, b, l = 1.0e-2, 0.8e-2, 1.3e-2
+    f = 25e9
+    k0 = 2 * np.pi * f / K.C0
+    p1 = make_port(1, (a / 2, b / 2, 0.0), (a, b))
+    p2 = make_port(2, (a / 2, b / 2, l), (a, b))
+    t1 = mesh.tris_on_plane(2, 0.0)
+    t2 = mesh.tris_on_plane(2, l)
+    DPTs = R.optimized.gaus_quad_tri(4)
+    Bm = fld.empty_tri_matrix()
+    Bm, bvec = R.robinbc.assemble_robin_bc_excited(fld, Bm, t1, lambda x, y, z: p1.get_Uinc(x, y, z, k0),
+                                                   p1.get_gamma(k0), DPTs)
+    Bm = R.robinbc.assemble_robin_bc(fld, Bm, t2, p2.get_gamma(k0))
+    Bp = fld.generate_csr(Bm)
+    touched = np.concatenate([t1, t2])
+    blocks = Bm.reshape(-1, 64)[touched]
+    np.savez_compressed(os.path.join(HERE, "robin_small.npz"), f=f, k0=k0, tris_port1=t1, tris_port2=t2,
+                        gamma1=p1.get_gamma(k0), gamma2=p2.get_gamma(k0), DPTs=DPTs,
+                        blocks=blocks, touched=touched, bvec=bvec,
+                        Bp_indptr=Bp.indptr, Bp_indices=Bp.indices, Bp_data=Bp.data,
+                        beta=p1.get_beta(k0), Zmode=p1.Zmode(k0), amp=p1.get_amplitude(k0))
+
+
+def config1():
+    a, b, l = 22.86e-3, 10.16e-3, 50e-3
+    f = 10e9
+    nodes, tets = box_tet_mesh(10, 5, 20, a, b, l, jitter=0.1, seed=0)
+    mesh = TetMesh(nodes, tets)
+    fld = R.nedelec2.Nedelec2(mesh)
+    nt = mesh.n_tets
+    er = np.zeros((3, 3, nt), dtype=np.complex128)
+    ur = np.zeros((3, 3, nt), dtype=np.complex128)
+    for i in range(3):
+        er[i, i] = 1.0
+        ur[i, i] = 1.0
+    t0 = time.time()
+    E, B = R.curlcurl.tet_mass_stiffness_matrices(fld, er, ur)
+    t_asm = time.time() - t0
+    k0 = 2 * np.pi * f / K.C0
+    Kmat = (E - B * (k0 ** 2)).tocsr()
+    ports = [make_port(1, (a / 2, b / 2, 0.0), (a, b)), make_port(2, (a / 2, b / 2, l), (a, b))]
+    port_tris = [mesh.tris_on_plane(2, 0.0), mesh.tris_on_plane(2, l)]
+    DPTs = R.optimized.gaus_quad_tri(4)
+    Bm = fld.empty_tri_matrix()
+    port_vectors = {}
+    for p, tr in zip(ports, port_tris):
+        Bm, bp = R.robinbc.assemble_robin_bc_excited(fld, Bm, tr, lambda x, y, z, p=p: p.get_Uinc(x, y, z, k0),
+                                                     p.get_gamma(k0), DPTs)
+        port_vectors[p.port_number] = bp
+    Kmat = Kmat + fld.generate_csr(Bm)
+    walls = np.concatenate([mesh.tris_on_plane(0, 0.0), mesh.tris_on_plane(0, a),
+                            mesh.tris_on_plane(1, 0.0), mesh.tris_on_plane(1, b)])
+    pec_ids = []
+    for ii in mesh.tri_to_edge[:, walls].ravel():
+        pec_ids.extend(fld.edge_to_field[:, ii])
+    for ii in walls:
+        pec_ids.extend(fld.tri_to_field[:, ii])
+    pec_set = set(int(i) for i in pec_ids)
+    solve_ids = np.array([i for i in range(Kmat.shape[0]) if i not in pec_set])
+
+    routine = R.solver.SolveRoutine()
+    sols = {}
+    t_solve = []
+    for pn, pv in port_vectors.items():
+        t0 = time.time()
+        x, rep = routine.solve(Kmat, pv, solve_ids, reuse=(pn != 1), id=pn)
+        t_solve.append(time.time() - t0)
+        sols[pn] = x
+
+    # raw S-matrix through the reference's own overlap integrals (_post_process, microwave_3d.py:1110-1247)
+    S = np.zeros((2, 2), dtype=np.complex128)
+    for ja, act in enumerate(ports):
+        act.active = True
+        sol = sols[act.port_number]
+        for ib, bc in enumerate(ports):
+            tets_face = mesh.face_tets(port_tris[ib])
+            fieldf = fld.interpolate_Ef(sol, tetids=tets_face)
+            tri_vertices = mesh.tris[:, port_tris[ib]]
+            const = np.ones(tri_vertices.shape[1], dtype=np.complex128)   # TE: 1/mean(diag ur) = 1 in air
+            fp = R.sparam.sparam_field_power(mesh.nodes, tri_vertices, bc, k0, fieldf, const, 4)
+            mp = R.sparam.sparam_mode_power(mesh.nodes, tri_vertices, bc, k0, const, 4)
+            S[ib, ja] = (fp / mp) / np.sqrt(act.power)
+        act.active = False
+
+    rng = np.random.default_rng(123)
+    samp = rng.choice(E.nnz, 4000, replace=False)
+    np.savez_compressed(
+        os.path.join(HERE, "config1.npz"),
+        f=f, k0=k0, nodes_sha=sha(mesh.nodes), tets_sha=sha(mesh.tets),
+        n_field=fld.n_field, E_nnz=E.nnz, B_nnz=B.nnz, K_nnz=Kmat.nnz,
+        E_indptr=E.indptr.astype(np.int64), E_indices_sha=sha(E.indices.astype(np.int32)),
+        K_indptr=Kmat.indptr.astype(np.int64), K_indices_sha=sha(Kmat.indices.astype(np.int32)),
+        E_fro=np.linalg.norm(E.data), B_fro=np.linalg.norm(B.data), K_fro=np.linalg.norm(Kmat.data),
+        samp=samp, E_samp=E.data[samp], B_samp=B.data[samp], K_samp=Kmat.data[samp],
+        E_samp_col=E.indices[samp],
+        pv1_idx=np.flatnonzero(port_vectors[1]), pv1_val=port_vectors[1][np.flatnonzero(port_vectors[1])],
+        pv2_idx=np.flatnonzero(port_vectors[2]), pv2_val=port_vectors[2][np.flatnonzero(port_vectors[2])],
+        n_solve=len(solve_ids), solve_ids_sha=sha(solve_ids.astype(np.int64)),
+        x1=sols[1], x2=sols[2], S=S,
+        t_assemble_s=t_asm, t_superlu_s=np.array(t_solve))
+    print(f"config1: nnz={E.nnz} K.nnz={Kmat.nnz} solve={len(solve_ids)} S=\n{S}\n|S|={np.abs(S)}")
+
+
+if __name__ == "__main__":
+    m, f = element_small()
+    robin_small(m, f)
+    config1()
+    for fn in sorted(os.listdir(HERE)):
+        if fn.endswith(".npz"):
+            print(fn, os.path.getsize(os.path.join(HERE, fn)))

@@ -1,0 +1,319 @@
+"""Benchmark: Nédélec-2 tets assembled/s (fused integrator + deterministic CSR scatter of E and B)
+on the dielectric-loaded cavity (40³ hex grid × 6 = 384 000 tets, 2 480 240 DOF), plus the
+frequency-sweep solve rate of block-Jacobi COCG on the same system.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference] [--no-sweep]
+
+One JSON line on rank 0.  Under torchrun every rank assembles its own copy of the mesh
+(replicas: the path has no exchange step), timed on the device; the step time is the max over
+ranks and ``value`` counts the tets of all ranks.  ``--impl reference`` times the CPU oracle (a
+restatement of the reference's numba integrator plus SciPy's COO→CSR) on the host's cores.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "Nedelec-2 tets assembled/s"
+UNIT = "tets/s"
+L2_BYTES = 126 * 2 ** 20
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
+    FIELDS = "index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown," \
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown," \
+             "clocks_event_reasons.sw_power_cap"
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        rows = []
+        if self.path and os.path.exists(self.path):
+            for line in open(self.path):
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+            os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        smax = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({n for r in rows for n, v in zip(names, r[5:9]) if v.lower() == "active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def dist_init(gpus: int):
+    import torch
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if ws > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+    elif torch.cuda.is_available():
+        torch.cuda.set_device(0)
+    return ws, rank, local
+
+
+def barrier(ws):
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(ws, v: float) -> float:
+    if ws == 1:
+        return v
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def cpu_baseline(problem, seconds_target: float = 15.0) -> dict:
+    """The CPU oracle (restated reference integrator + SciPy COO->CSR) on a prefix sample of tets."""
+    import oracle
+    from scipy.sparse import coo_matrix
+    cores = len(os.sched_getaffinity(0))
+    oracle.set_threads(cores)
+    m, f = problem.mesh, problem.field
+    nt = m.n_tets
+    n = f.n_field
+
+    def run(k):
+        t0 = time.perf_counter()
+        dE, dB, r, c = oracle.matrix_builder(m.nodes, m.tets[:, :k], m.tris, m.edges, m.edge_lengths,
+                                             f.tet_to_field[:, :k], m.tet_to_edge[:, :k], problem.ur[:, :, :k],
+                                             problem.er[:, :, :k])
+        coo_matrix((dE, (r, c)), shape=(n, n)).tocsr()
+        coo_matrix((dB, (r, c)), shape=(n, n)).tocsr()
+        return time.perf_counter() - t0
+
+    k = min(nt, 20000)
+    dt = run(k)
+    # grow the sample to ~seconds_target of work (bounded by the full mesh)
+    k2 = int(min(nt, max(k, k * seconds_target / max(dt, 1e-3))))
+    if k2 > k:
+        k, dt = k2, run(k2)
+    return {"value": k / dt, "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": f"first {k} of {nt} tets: oracle _matrix_builder restatement (OpenMP) + SciPy coo->csr of E and B"}
+
+
+def run_reference(args, ws, rank):
+    if rank != 0:
+        return
+    from emerge_b200 import problems
+    P = problems.cavity()
+    t_all = []
+    cb = None
+    for i in range(args.warmup + args.steps):
+        cb = cpu_baseline(P, seconds_target=8.0)
+        if i >= args.warmup:
+            t_all.append(cb["value"])
+    v = float(np.mean(t_all))
+    cb["value"] = v
+    out = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
+           "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "dtype": "c128",
+           "data": "synthetic", "config": workload_config(P), "cpu_baseline": cb,
+           "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out), flush=True)
+
+
+def workload_config(P) -> dict:
+    g = round((P.mesh.n_tets / 6) ** (1 / 3))
+    return {"workload": f"dielectric-loaded cavity, {g}x{g}x{g} hex grid x6 tets, 8 seeded eps blocks, Nedelec-2 c128",
+            "n_tets": int(P.mesh.n_tets), "n_dof": int(P.field.n_field), "frequencies": int(len(P.freqs)),
+            "l2_policy": "inputs+outputs larger than L2 (126 MB) every step", "parallelism": "replicas"}
+
+
+def sweep_measure(P, nsys: int, maxit: int, precision: str, precond: str) -> dict:
+    import torch
+    from emerge_b200.sweep import FrequencySweep
+    sw = FrequencySweep(P)
+    freqs = P.freqs[:: max(1, len(P.freqs) // nsys)][:nsys]
+    systems = [(float(f), 0) for f in freqs]
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    res = sw.solve(systems, tol=1e-8, maxit=maxit, precond=precond, precision=precision)
+    torch.cuda.synchronize()
+    dt = time.perf_counter() - t0
+    conv = int((res.status == 0).sum())
+    return {"precision": precision, "precond": precond, "systems": nsys, "converged": conv,
+            "seconds": dt, "solves_per_s": conv / dt, "iters_max": int(res.iters.max()),
+            "iters_mean": float(res.iters.mean()), "relres_max": float(res.relres.max()), "maxit": maxit,
+            "tol": 1e-8}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="native", choices=["native", "reference"])
+    ap.add_argument("--no-sweep", action="store_true")
+    ap.add_argument("--sweep-systems", type=int, default=8)
+    ap.add_argument("--sweep-maxit", type=int, default=3000)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--grid", type=int, default=40, help="cavity hex grid size (40 = the 384 000-tet workload)")
+    args = ap.parse_args()
+    ws, rank, local = dist_init(args.gpus)
+    if args.impl == "reference":
+        run_reference(args, ws, rank)
+        if ws > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+        return
+
+    import torch
+    from emerge_b200 import assembly, problems
+    from emerge_b200._lib import Handle
+
+    assert torch.cuda.is_available(), "bench.py needs a GPU"
+    dev = torch.device("cuda", local if ws > 1 else 0)
+    P = problems.cavity(n=args.grid)
+    nt, N = P.mesh.n_tets, P.field.n_field
+    dm = assembly.DeviceMesh(P.mesh, P.field, dev)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    plan = assembly.CsrPlan(dm)
+    torch.cuda.synchronize()
+    t_plan = time.perf_counter() - t0
+    nnz = plan.nnz
+    er = torch.from_numpy(np.ascontiguousarray(P.er)).to(dev)
+    ur = torch.from_numpy(np.ascontiguousarray(P.ur)).to(dev)
+    E = torch.empty(nnz, dtype=torch.complex128, device=dev)
+    B = torch.empty(nnz, dtype=torch.complex128, device=dev)
+    stream = torch.cuda.current_stream(dev)
+
+    for _ in range(args.warmup):
+        plan.assemble(er, ur, E, B)
+    torch.cuda.synchronize()
+    Handle.get(dev).raise_on_device_status("bench warm-up")
+
+    # ---- device-resident timed region (inputs resident in HBM) ----
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    step_events = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    barrier(ws)
+    torch.cuda.synchronize()
+    with ClockSampler(dev.index) as clk:
+        ev0.record(stream)
+        for a, b in step_events:
+            a.record(stream)
+            plan.assemble(er, ur, E, B)
+            b.record(stream)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+    barrier(ws)
+    total_ms = ev0.elapsed_time(ev1)
+    step_ms = [a.elapsed_time(b) for a, b in step_events]
+    ms_step = max_over_ranks(ws, total_ms / args.steps)
+    value = ws * nt / (ms_step / 1e3)
+    clocks = clk.summary()
+
+    # ---- roofline of the assembly launch pair (invariants + row-owner assembly) ----
+    hbm, peak_kind = peaks()
+    alg_bytes_per_tet = 480 + 32.0 * nnz / nt
+    achieved = nt * alg_bytes_per_tet / (float(np.mean(step_ms)) / 1e3) / 1e9
+
+    # ---- end-to-end through the public API with host buffers ----
+    from emerge_b200.assembly import tet_mass_stiffness_matrices
+    host_in = [torch.from_numpy(np.ascontiguousarray(a)).pin_memory() for a in
+               (P.mesh.nodes, P.mesh.tets, P.mesh.tet_to_edge, P.mesh.edge_lengths, P.er, P.ur)]
+    h2d = sum(t.numel() * t.element_size() for t in host_in)
+    d2h = 2 * nnz * 16 + (N + 1) * 4 * 2 + nnz * 4 * 2
+    P.field._emfem_cache = (("cuda:%d" % dev.index, id(P.mesh)), dm, plan)
+    e2e_steps = max(2, min(args.steps, 4))
+    for _ in range(1):
+        tet_mass_stiffness_matrices(P.field, host_in[4], host_in[5], device=dev)
+    barrier(ws)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        dm.nodes.copy_(host_in[0], non_blocking=True)
+        dm.tets.copy_(host_in[1], non_blocking=True)
+        dm.tet_to_edge.copy_(host_in[2], non_blocking=True)
+        dm.edge_lengths.copy_(host_in[3], non_blocking=True)
+        Eh, Bh = tet_mass_stiffness_matrices(P.field, host_in[4], host_in[5], device=dev)
+    torch.cuda.synchronize()
+    e2e_s = max_over_ranks(ws, (time.perf_counter() - t0) / e2e_steps)
+    e2e_value = ws * nt / e2e_s
+
+    out = None
+    if rank == 0:
+        sweep = None
+        if not args.no_sweep:
+            sweep = {"fp64": sweep_measure(P, args.sweep_systems, args.sweep_maxit, "fp64", "block_jacobi"),
+                     "mixed": sweep_measure(P, args.sweep_systems, args.sweep_maxit, "mixed", "block_jacobi")}
+        cb = None if args.no_cpu_baseline else cpu_baseline(P)
+        out = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "c128", "data": "synthetic",
+            "config": workload_config(P),
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                         "frac": achieved / hbm, "traffic": None, "peak_kind": peak_kind,
+                         "alg_bytes_per_tet": alg_bytes_per_tet, "kernels": "tet_invariants_kernel+assemble_kernel"},
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+                    "api": "emerge_b200.assembly.tet_mass_stiffness_matrices (host numpy in, SciPy CSR out)"},
+            "gpu_launches": 2 * args.steps,
+            "clocks": clocks,
+            "plan_seconds": t_plan, "nnz": int(nnz),
+            "sweep": sweep,
+            "cpu_baseline": cb,
+        }
+        print(json.dumps(out), flush=True)
+    if ws > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -60,8 +60,8 @@ _SIGS = {
     "emfem_ned2_tri_robin": ([_vp, _i64, _vp, _i64, _vp, _dbl, _dbl, _vp, _vp, _i32, _vp, _vp], _i32),
     "emfem_segmented_gather_sum": ([_vp, _i64, _vp, _vp, _vp, _vp], _i32),
     "emfem_sweep_combine": ([_vp, _i64, _vp, _vp, _dbl, _i64, _vp, _vp, _dbl, _dbl, _vp], _i32),
-    "emfem_cocg_workspace_size": ([_i64, _i64, _i32, _i32, ctypes.POINTER(ctypes.c_size_t)], _i32),
-    "emfem_cocg_solve": ([_vp, _i64, _i64, _vp, _vp, _vp, _vp, _i32, _dblp,
+    "emfem_krylov_workspace_size": ([_i64, _i64, _i32, _i32, ctypes.POINTER(ctypes.c_size_t)], _i32),
+    "emfem_krylov_solve": ([_vp, _i32, _i64, _i64, _vp, _vp, _vp, _vp, _i32, _dblp,
                           _i64, _vp, _vp, _vp, _vp, _vp, _i32, _dblp, _vp, _vp, _vp,
                           _dbl, _i32, _i32, _i32, _vp, ctypes.c_size_t, _i32p, _i32p, _dblp], _i32),
     "emfem_sweep_spmv": ([_vp, _i64, _vp, _vp, _vp, _vp, _i32, _vp, _i64, _vp, _vp, _vp, _vp, _vp, _i32, _vp,

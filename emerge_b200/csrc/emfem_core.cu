@@ -66,7 +66,7 @@ __global__ void scan_total_kernel(int* out, long long n, const int* block_off, c
 size_t scan_scratch_ints(long long n) {
     long long nb = (n + SCAN_BLOCK - 1) / SCAN_BLOCK;
     if (nb < 1) nb = 1;
-    return (size_t)(2 * nb) + (nb > 1 ? scan_scratch_ints(nb) : 0);
+    return (size_t)(2 * nb + 1) + (nb > 1 ? scan_scratch_ints(nb) : 0);
 }
 
 int exclusive_scan_i32(Handle* h, const int* in, int* out, long long n, int* scratch) {
@@ -83,7 +83,7 @@ int exclusive_scan_i32(Handle* h, const int* in, int* out, long long n, int* scr
     if (nb == 1) {
         EMFEM_CUDA(cudaMemsetAsync(boff, 0, sizeof(int), h->stream));
     } else {
-        EMFEM_TRY(exclusive_scan_i32(h, bsum, boff, nb, scratch + 2 * nb));
+        EMFEM_TRY(exclusive_scan_i32(h, bsum, boff, nb, scratch + 2 * nb + 1));
         scan_add_kernel<<<(unsigned)nb, SCAN_BLOCK, 0, h->stream>>>(out, n, boff);
         EMFEM_LAUNCH("scan_add_kernel");
     }

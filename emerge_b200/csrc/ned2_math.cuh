@@ -72,6 +72,7 @@ constexpr int INV_SD = 116;       // 1/(6V)^3  (D scale: 6V from the coefficient
 constexpr int INV_SF = 117;       // 1/(6V)    (F scale)
 constexpr int INV_RANK = 118;     // vertex ranks packed as a double-encoded int (2 bits each)
 constexpr int INV_NDOUBLE = 119;
+constexpr int INV_STRIDE = 120;   // per-tet record length in the array-of-structs buffer (960 B)
 
 // Orientation of the tet's local entities from the rank (0..3) of each vertex's global id.
 struct Orient {

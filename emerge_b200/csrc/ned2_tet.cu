@@ -13,6 +13,8 @@
 #include "emfem_internal.cuh"
 #include "ned2_math.cuh"
 
+#include <vector>
+
 namespace emfem {
 
 constexpr int INC_REC = 16;         // bytes per incidence record: 10 positions + own slot + pad
@@ -33,34 +35,32 @@ __global__ void __launch_bounds__(128) tet_invariants_kernel(
     if (t >= nt) return;
     int64_t ids[4];
     double xs[4], ys[4], zs[4], el[6];
-    bool bad = false;
+    bool bad = false, finite = true;
 #pragma unroll
     for (int i = 0; i < 4; i++) {
         int64_t v = tets[i * nt + t];
         if (v < 0 || v >= nn) { bad = true; v = 0; }
         ids[i] = v;
         xs[i] = nodes[v]; ys[i] = nodes[nn + v]; zs[i] = nodes[2 * nn + v];
+        finite &= isfinite(xs[i]) && isfinite(ys[i]) && isfinite(zs[i]);
     }
 #pragma unroll
     for (int e = 0; e < 6; e++) {
         int64_t id = t2e[e * nt + t];
         if (id < 0 || id >= ne) { bad = true; id = 0; }
         el[e] = elen[id];
+        finite &= isfinite(el[e]);
     }
     if (bad) flag(status, DEV_BAD_INDEX);
     cd U[9], E[9];
 #pragma unroll
-    for (int k = 0; k < 9; k++) { U[k] = load_c(ur, k * nt + t); E[k] = load_c(er, k * nt + t); }
-    double loc[INV_NDOUBLE];
-    tet_invariants(xs, ys, zs, ids, el, U, E, loc);
-    if (!(loc[INV_SF] < 1e300)) flag(status, DEV_DEGENERATE);
-    bool finite = true;
-#pragma unroll 1
-    for (int f = 0; f < INV_NDOUBLE; f++) {
-        double v = loc[f];
-        if (!isfinite(v)) finite = false;
-        inv[(long long)f * nt + t] = v;
+    for (int k = 0; k < 9; k++) {
+        U[k] = load_c(ur, k * nt + t); E[k] = load_c(er, k * nt + t);
+        finite &= isfinite(U[k].x) && isfinite(U[k].y) && isfinite(E[k].x) && isfinite(E[k].y);
     }
+    double* out = inv + t * INV_STRIDE;
+    tet_invariants(xs, ys, zs, ids, el, U, E, out);
+    if (!(out[INV_SF] < 1e300)) flag(status, DEV_DEGENERATE);
     if (!finite) flag(status, DEV_NONFINITE);
 }
 
@@ -190,14 +190,16 @@ __global__ void inc_count_kernel(long long nt, long long ne, long long H, const 
     atomicAdd(&cnt[X], 1);
 }
 
-__global__ void inc_fill_kernel(long long nt, const int64_t* __restrict__ t2f, const int* __restrict__ inc_ptr,
+__global__ void inc_fill_kernel(long long nt, long long ne, const int64_t* __restrict__ t2f, const int* __restrict__ inc_ptr,
                                 int* __restrict__ cursor, uint32_t* __restrict__ inc_code, long long H) {
     long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (g >= nt * 10) return;
     int s = (int)(g / nt);
     long long t = g % nt;
     int64_t X = t2f[s * nt + t];
-    if (X < 0 || X >= H) return;
+    int64_t X2 = t2f[(s + 10) * nt + t];
+    bool ok = s < 6 ? (X >= 0 && X < ne) : (X >= ne && X < H);
+    if (!ok || X2 != X + H) return;
     int p = atomicAdd(&cursor[X], 1);
     inc_code[inc_ptr[X] + p] = (uint32_t)(t * 16 + s);
 }
@@ -338,52 +340,78 @@ __global__ void export_indices_kernel(long long H, long long sum_m, const int* _
 }
 
 // ---------------------------------------------------------------- fused numeric assembly
-constexpr int ASM_BLOCK = 256;
+// One CTA per chunk of consecutive entities of one kind (all edges or all faces) holding at most
+// CH_INC incidences.  Phase 1: one thread per (incidence, column entity) pair block, column-entity
+// major so that every warp evaluates the same edge/face block type; results staged in shared
+// memory.  Phase 2: one thread per output (X, k) sums its tets' staged blocks in ascending tet
+// order and writes the 4 E and 4 B CSR values of its column pair.
+constexpr int CH_INC = 64;
+constexpr int CH_THREADS = 320;
+constexpr int CH_SMEM = CH_INC * 10 * 8 * 16 + 625 * 8 + CH_INC * 16 + CH_INC * 4 + 16;
 
-__global__ void __launch_bounds__(ASM_BLOCK) assemble_kernel(
-    long long H, long long sum_m, long long nt, const int* __restrict__ mptr,
+__global__ void __launch_bounds__(CH_THREADS) assemble_chunk_kernel(
+    const int* __restrict__ chunk_ptr, long long H, const int* __restrict__ mptr,
     const int* __restrict__ inc_ptr, const uint32_t* __restrict__ inc_code, const uint4* __restrict__ rec,
     const double* __restrict__ inv, double2* __restrict__ Ev, double2* __restrict__ Bv) {
-    __shared__ double vtab[625];
-    __shared__ long long sX0;
+    extern __shared__ __align__(16) unsigned char smem[];
+    double2* stage = reinterpret_cast<double2*>(smem);                                  // [CH_INC][10][8]
+    double* vtab = reinterpret_cast<double*>(smem + CH_INC * 10 * 8 * 16);               // 625
+    uint4* srec = reinterpret_cast<uint4*>(smem + CH_INC * 10 * 8 * 16 + 625 * 8 + 8);   // CH_INC (16 B aligned)
+    uint32_t* scode = reinterpret_cast<uint32_t*>(srec + CH_INC);                         // CH_INC
     load_vtab(vtab);
-    long long j0 = (long long)blockIdx.x * ASM_BLOCK;
-    if (threadIdx.x == 0) sX0 = find_entity(mptr, H, j0, 0, H);
-    __syncthreads();
-    long long j = j0 + threadIdx.x;
-    if (j >= sum_m) return;
-    long long X0 = sX0;
-    long long hiX = X0 + ASM_BLOCK + 1;
-    if (hiX > H) hiX = H;
-    long long X = find_entity(mptr, H, j, X0, hiX);
-    int mb = mptr[X];
-    int k = (int)(j - mb), m = mptr[X + 1] - mb;
-    VTab T{vtab};
-    cd d[4] = {mk(0, 0), mk(0, 0), mk(0, 0), mk(0, 0)};
-    cd f[4] = {mk(0, 0), mk(0, 0), mk(0, 0), mk(0, 0)};
-    int ib = inc_ptr[X], ie = inc_ptr[X + 1];
-    for (int i = ib; i < ie; i++) {
-        uint4 r4 = rec[i];
-        uint8_t r[16];
-        memcpy(r, &r4, 16);
-        int sy = -1;
-#pragma unroll
-        for (int q = 0; q < 10; q++) if (r[q] == k) sy = q;
-        if (sy < 0) continue;
-        long long t = inc_code[i] >> 4;
-        int sx = r[10];
-        InvView I{inv + t, nt};
-        Orient o = unpack_rank((int)I.g(INV_RANK));
-        cd dd[4], ff[4];
-        pair_block(I, o, T, sx, sy, dd, ff);
-#pragma unroll
-        for (int q = 0; q < 4; q++) { d[q] += dd[q]; f[q] += ff[q]; }
+    const int X0 = chunk_ptr[blockIdx.x], X1 = chunk_ptr[blockIdx.x + 1];
+    const int i0 = inc_ptr[X0], ninc = inc_ptr[X1] - i0;
+    for (int li = threadIdx.x; li < ninc; li += CH_THREADS) {
+        srec[li] = rec[i0 + li];
+        scode[li] = inc_code[i0 + li];
     }
-    long long b1 = 2LL * mb + k, b2 = 2LL * mptr[H] + 2LL * mb + k;
-    Ev[b1] = make_double2(d[0].x, d[0].y);      Bv[b1] = make_double2(f[0].x, f[0].y);
-    Ev[b1 + m] = make_double2(d[1].x, d[1].y);  Bv[b1 + m] = make_double2(f[1].x, f[1].y);
-    Ev[b2] = make_double2(d[2].x, d[2].y);      Bv[b2] = make_double2(f[2].x, f[2].y);
-    Ev[b2 + m] = make_double2(d[3].x, d[3].y);  Bv[b2 + m] = make_double2(f[3].x, f[3].y);
+    __syncthreads();
+    VTab T{vtab};
+    const int npad = (ninc + 31) & ~31;
+    for (int w = threadIdx.x; w < 10 * npad; w += CH_THREADS) {
+        int sy = w / npad, li = w - sy * npad;
+        if (li >= ninc) continue;
+        uint4 r4 = srec[li];
+        int sx = (int)((r4.z >> 16) & 0xff);  // byte 10 of the record
+        long long t = scode[li] >> 4;
+        InvView I{inv + t * INV_STRIDE, 1};
+        Orient o = unpack_rank((int)I.g(INV_RANK));
+        cd d[4], f[4];
+        pair_block(I, o, T, sx, sy, d, f);
+        double2* dst = stage + (li * 10 + sy) * 8;
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            dst[q] = make_double2(d[q].x, d[q].y);
+            dst[4 + q] = make_double2(f[q].x, f[q].y);
+        }
+    }
+    __syncthreads();
+    const int m0 = mptr[X0], total = mptr[X1] - m0;
+    const long long two_mH = 2LL * mptr[H];
+    for (int o = threadIdx.x; o < total; o += CH_THREADS) {
+        int j = m0 + o;
+        int lo = X0, hi = X1;  // largest X in [X0, X1) with mptr[X] <= j
+        while (hi - lo > 1) { int mid = (lo + hi) >> 1; if (mptr[mid] <= j) lo = mid; else hi = mid; }
+        const int X = lo;
+        const int mb = mptr[X], k = j - mb, m = mptr[X + 1] - mb;
+        double2 acc[8];
+#pragma unroll
+        for (int q = 0; q < 8; q++) acc[q] = make_double2(0.0, 0.0);
+        for (int li = inc_ptr[X] - i0; li < inc_ptr[X + 1] - i0; li++) {
+            uint4 r4 = srec[li];
+            uint32_t wds[4] = {r4.x, r4.y, r4.z, r4.w};
+            int sy = -1;
+#pragma unroll
+            for (int q = 0; q < 10; q++) if ((int)((wds[q >> 2] >> (8 * (q & 3))) & 0xff) == k) sy = q;
+            if (sy < 0) continue;
+            const double2* src = stage + (li * 10 + sy) * 8;
+#pragma unroll
+            for (int q = 0; q < 8; q++) { acc[q].x += src[q].x; acc[q].y += src[q].y; }
+        }
+        long long b1 = 2LL * mb + k, b2 = two_mH + 2LL * mb + k;
+        Ev[b1] = acc[0]; Ev[b1 + m] = acc[1]; Ev[b2] = acc[2]; Ev[b2 + m] = acc[3];
+        Bv[b1] = acc[4]; Bv[b1 + m] = acc[5]; Bv[b2] = acc[6]; Bv[b2 + m] = acc[7];
+    }
 }
 
 __global__ void find_slots_kernel(long long n, long long H, const int* __restrict__ mptr, const int* __restrict__ S,
@@ -418,13 +446,15 @@ struct emfem_plan_s {
     uint8_t* rec = nullptr;        // 16 * 10 nt
     int* mptr = nullptr;           // H + 1
     int* S = nullptr;              // sum_m
-    double* inv = nullptr;         // INV_NDOUBLE * nt
+    double* inv = nullptr;         // INV_STRIDE * nt (array of structs)
+    int* chunk_ptr = nullptr;      // n_chunks + 1 entity boundaries
+    int n_chunks = 0;
 };
 
 static void plan_free(emfem_plan p) {
     if (!p) return;
     cudaFree(p->inc_ptr); cudaFree(p->inc_code); cudaFree(p->rec);
-    cudaFree(p->mptr); cudaFree(p->S); cudaFree(p->inv);
+    cudaFree(p->mptr); cudaFree(p->S); cudaFree(p->inv); cudaFree(p->chunk_ptr);
     delete p;
 }
 
@@ -483,12 +513,13 @@ int emfem_plan_create(emfem_handle h, int64_t n_tets, int64_t n_edges, int64_t n
     PTRY(check_cuda(cudaMalloc(&p->inc_code, 10 * n_tets * sizeof(uint32_t)), "cudaMalloc(inc_code)"));
     PTRY(check_cuda(cudaMalloc(&p->rec, 10 * n_tets * (size_t)INC_REC), "cudaMalloc(rec)"));
     PTRY(check_cuda(cudaMalloc(&p->mptr, (H + 1) * sizeof(int)), "cudaMalloc(mptr)"));
-    PTRY(check_cuda(cudaMalloc(&p->inv, (size_t)INV_NDOUBLE * n_tets * sizeof(double)), "cudaMalloc(inv)"));
+    PTRY(check_cuda(cudaMalloc(&p->inv, (size_t)INV_STRIDE * n_tets * sizeof(double)), "cudaMalloc(inv)"));
     PTRY(check_cuda(cudaMalloc(&cnt, H * sizeof(int)), "cudaMalloc(cnt)"));
     PTRY(check_cuda(cudaMalloc(&cursor, H * sizeof(int)), "cudaMalloc(cursor)"));
     PTRY(check_cuda(cudaMalloc(&scratch, nscr * sizeof(int)), "cudaMalloc(scan)"));
     PTRY(check_cuda(cudaMalloc(&tmp, 100 * n_tets * sizeof(int)), "cudaMalloc(tmp)"));
     PTRY(check_cuda(cudaMalloc(&m, H * sizeof(int)), "cudaMalloc(m)"));
+    PTRY(check_cuda(cudaMemsetAsync(h->h.dev_status, 0, sizeof(int), s), "memset"));
     PTRY(check_cuda(cudaMemsetAsync(cnt, 0, H * sizeof(int), s), "memset"));
     PTRY(check_cuda(cudaMemsetAsync(cursor, 0, H * sizeof(int), s), "memset"));
     inc_count_kernel<<<grid_for(10 * n_tets, 256), 256, 0, s>>>(n_tets, n_edges, H, tet_to_field, cnt, h->h.dev_status);
@@ -505,7 +536,7 @@ int emfem_plan_create(emfem_handle h, int64_t n_tets, int64_t n_edges, int64_t n
         }
     }
     PTRY(exclusive_scan_i32(&h->h, cnt, p->inc_ptr, H, scratch));
-    inc_fill_kernel<<<grid_for(10 * n_tets, 256), 256, 0, s>>>(n_tets, tet_to_field, p->inc_ptr, cursor, p->inc_code, H);
+    inc_fill_kernel<<<grid_for(10 * n_tets, 256), 256, 0, s>>>(n_tets, n_edges, tet_to_field, p->inc_ptr, cursor, p->inc_code, H);
     PTRY(check_cuda(cudaGetLastError(), "inc_fill_kernel"));
     inc_sort_kernel<<<grid_for(H, 256), 256, 0, s>>>(H, p->inc_ptr, p->inc_code);
     PTRY(check_cuda(cudaGetLastError(), "inc_sort_kernel"));
@@ -532,6 +563,32 @@ int emfem_plan_create(emfem_handle h, int64_t n_tets, int64_t n_edges, int64_t n
     cols_fill_kernel<<<grid_for(H, 128), 128, 0, s>>>(H, n_tets, tet_to_field, p->inc_ptr, p->inc_code, tmp, p->mptr,
                                                       p->S, p->rec, h->h.dev_status);
     PTRY(check_cuda(cudaGetLastError(), "cols_fill_kernel"));
+    {
+        // greedy chunks of whole entities of one kind with at most CH_INC incidences each
+        std::vector<int> hptr(H + 1);
+        PTRY(check_cuda(cudaMemcpyAsync(hptr.data(), p->inc_ptr, (H + 1) * sizeof(int), cudaMemcpyDeviceToHost, s), "copy"));
+        PTRY(check_cuda(cudaStreamSynchronize(s), "sync"));
+        std::vector<int> cptr;
+        cptr.push_back(0);
+        int cur = 0;
+        for (long long X = 0; X < H; X++) {
+            int deg = hptr[X + 1] - hptr[X];
+            if (deg > CH_INC) {
+                set_error("emfem_plan_create: an edge or face is shared by %d tets (at most %d supported)", deg, CH_INC);
+                st = EMFEM_ERR_INVALID_ARG;
+                goto fail;
+            }
+            bool kind_change = X == n_edges && X > cptr.back();
+            if ((cur + deg > CH_INC && X > cptr.back()) || kind_change) { cptr.push_back((int)X); cur = 0; }
+            cur += deg;
+        }
+        cptr.push_back((int)H);
+        p->n_chunks = (int)cptr.size() - 1;
+        PTRY(check_cuda(cudaMalloc(&p->chunk_ptr, cptr.size() * sizeof(int)), "cudaMalloc(chunk_ptr)"));
+        PTRY(check_cuda(cudaMemcpyAsync(p->chunk_ptr, cptr.data(), cptr.size() * sizeof(int), cudaMemcpyHostToDevice, s), "copy"));
+        PTRY(check_cuda(cudaFuncSetAttribute(assemble_chunk_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, CH_SMEM),
+                        "cudaFuncSetAttribute"));
+    }
     PTRY(check_cuda(cudaStreamSynchronize(s), "sync"));
     cudaFree(cnt); cudaFree(cursor); cudaFree(scratch); cudaFree(tmp); cudaFree(m);
     *out = p;
@@ -576,10 +633,10 @@ int emfem_plan_assemble(emfem_plan p, int64_t n_nodes, int64_t n_edges, const do
                                                                 edge_lengths, (const double2*)ur, (const double2*)er,
                                                                 p->inv, p->h->dev_status);
     EMFEM_LAUNCH("tet_invariants_kernel");
-    assemble_kernel<<<grid_for(p->sum_m, ASM_BLOCK), ASM_BLOCK, 0, s>>>(
-        p->H, p->sum_m, p->nt, p->mptr, p->inc_ptr, p->inc_code, (const uint4*)p->rec, p->inv,
+    assemble_chunk_kernel<<<p->n_chunks, CH_THREADS, CH_SMEM, s>>>(
+        p->chunk_ptr, p->H, p->mptr, p->inc_ptr, p->inc_code, (const uint4*)p->rec, p->inv,
         (double2*)E_vals, (double2*)B_vals);
-    EMFEM_LAUNCH("assemble_kernel");
+    EMFEM_LAUNCH("assemble_chunk_kernel");
     return EMFEM_OK;
 }
 

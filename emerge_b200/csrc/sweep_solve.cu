@@ -1,4 +1,4 @@
-// Frequency-sweep operator and batched COCG solver.
+// Frequency-sweep operator and batched Krylov solvers (COCG and BiCGStab).
 //
 // Replaces the per-frequency direct solve (SolverSuperLU, src/emerge/_emerge/solver.py:535-572,
 // through SolveRoutine.solve :1241-1326) for the systems K_f = E - k0_f^2 B + sum_p gamma_{f,p} R_p
@@ -8,8 +8,13 @@
 // contiguous.  PEC elimination (SolveRoutine's A[ids, ids], solver.py:1266-1269) is a free-DOF
 // mask: eliminated rows produce 0 and eliminated entries of every Krylov vector stay 0.
 //
-// COCG (conjugate orthogonal CG; van der Vorst & Melissen 1990) for complex-symmetric A uses the
-// unconjugated bilinear form x^T y.  Every reduction is a fixed-order tree, so runs are
+// Methods.  COCG (van der Vorst & Melissen 1990) is CG with the unconjugated form x^T y and is
+// exact for complex-symmetric A.  The reference's mass matrix is not symmetric: its face-face
+// block uses coefficient tables whose index lists differ between (i, j) and (j, i)
+// (ASM/curlcurl.py:348-357, e.g. VBCDE = VOLUME_COEFF_CACHE[B,C,D,F]), about 0.5 % of ||B||, and
+// COCG stalls near 1e-5 on it.  The default is therefore right-preconditioned BiCGStab
+// (van der Vorst 1992), the general-matrix member of the same BiCG family, with the same batched
+// operator and preconditioner.  Every reduction is a fixed-order tree, so runs are
 // bit-reproducible.  Iterations run in CUDA-graph chunks with all scalars on the device; the host
 // reads only the per-system active flags between chunks.
 #include "emfem_internal.cuh"
@@ -47,20 +52,60 @@ struct OpArgs {
     const uint8_t* mask;            // [n]
 };
 
-// y = A x for all systems; optional: partial[block][s] = sum over the block's rows of x_i * y_i
-// (unconjugated) when partial != null.  One thread per (row, system).
+template <typename T>
+__device__ __forceinline__ double2 dotu(T a, T b) {  // a^T b contribution (unconjugated)
+    return make_double2((double)a.x * b.x - (double)a.y * b.y, (double)a.x * b.y + (double)a.y * b.x);
+}
+template <typename T>
+__device__ __forceinline__ double2 dotc(T a, T b) {  // conj(a) b
+    return make_double2((double)a.x * b.x + (double)a.y * b.y, (double)a.x * b.y - (double)a.y * b.x);
+}
+template <typename T>
+__device__ __forceinline__ double nrm2(T a) { return (double)a.x * a.x + (double)a.y * a.y; }
+
+enum DotMode { DOT_NONE = 0, DOT_XY = 1, DOT_CONJW_Y = 2, DOT_CONJY_W_YY = 3 };
+
+// Block-level fixed-order tree reduction of up to three components per thread (two complex, one
+// real); thread s < S stores component c of this block at partial[(c * nblocks + block) * S + s].
+__device__ __forceinline__ void block_store3(double2 v0, double2 v1, double v2, int ncomp, int S, double2* partial) {
+    __shared__ double2 r0[VB], r1[VB];
+    __shared__ double r2[VB];
+    r0[threadIdx.x] = v0;
+    r1[threadIdx.x] = v1;
+    r2[threadIdx.x] = v2;
+    __syncthreads();
+    for (int off = VB / 2; off >= S; off >>= 1) {
+        if (threadIdx.x < off) {
+            r0[threadIdx.x].x += r0[threadIdx.x + off].x; r0[threadIdx.x].y += r0[threadIdx.x + off].y;
+            r1[threadIdx.x].x += r1[threadIdx.x + off].x; r1[threadIdx.x].y += r1[threadIdx.x + off].y;
+            r2[threadIdx.x] += r2[threadIdx.x + off];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x < S) {
+        partial[(long long)blockIdx.x * S + threadIdx.x] = r0[threadIdx.x];
+        if (ncomp > 1) partial[((long long)gridDim.x + blockIdx.x) * S + threadIdx.x] = r1[threadIdx.x];
+        if (ncomp > 2) partial[(2LL * gridDim.x + blockIdx.x) * S + threadIdx.x] = make_double2(r2[threadIdx.x], 0.0);
+    }
+}
+__device__ __forceinline__ void block_store2(double2 v0, double2 v1, int ncomp, int S, double2* partial) {
+    block_store3(v0, v1, 0.0, ncomp, S, partial);
+}
+
+// y = A x for all systems, one thread per (row, system); optional dot-product epilogue (DotMode).
 template <typename R>
 __global__ void __launch_bounds__(VB) spmv_kernel(OpArgs a, const typename V2<R>::T* __restrict__ x,
-                                                   typename V2<R>::T* __restrict__ y, double2* __restrict__ partial) {
+                                                   typename V2<R>::T* __restrict__ y, double2* __restrict__ partial,
+                                                   int dotmode, const typename V2<R>::T* __restrict__ w) {
     typedef typename V2<R>::T T;
-    __shared__ double2 red[VB];
     const int S = a.S;
     long long g = (long long)blockIdx.x * VB + threadIdx.x;
     long long i = g / S;
     int s = (int)(g % S);
-    double2 contrib = make_double2(0.0, 0.0);
+    double2 c0 = make_double2(0.0, 0.0), c1 = c0;
+    double c2 = 0.0;
     if (i < a.n) {
-        T out = mk2<R>(0, 0);
+        R yr = 0, yi = 0;
         if (a.mask[i]) {
             const T* Ev = (const T*)a.E;
             const T* Bv = (const T*)a.B;
@@ -79,7 +124,8 @@ __global__ void __launch_bounds__(VB) spmv_kernel(OpArgs a, const typename V2<R>
                 }
             }
             R k2 = (R)a.k0sq[s];
-            R yr = er - k2 * br, yi = ei - k2 * bi;
+            yr = er - k2 * br;
+            yi = ei - k2 * bi;
             int pr = a.patch_of_row ? a.patch_of_row[i] : -1;
             if (pr >= 0) {
                 const T* Pv = (const T*)a.patch_vals;
@@ -97,47 +143,65 @@ __global__ void __launch_bounds__(VB) spmv_kernel(OpArgs a, const typename V2<R>
                     yi += gr * pi_ + gi * pr_;
                 }
             }
-            out = mk2<R>(yr, yi);
-            if (partial) {
-                T xi = x[i * S + s];
-                contrib = make_double2((double)xi.x * yr - (double)xi.y * yi, (double)xi.x * yi + (double)xi.y * yr);
-            }
         }
-        y[i * S + s] = out;
-    }
-    if (partial) {
-        red[threadIdx.x] = contrib;
-        __syncthreads();
-        for (int off = VB / 2; off >= S; off >>= 1) {
-            if (threadIdx.x < off) {
-                red[threadIdx.x].x += red[threadIdx.x + off].x;
-                red[threadIdx.x].y += red[threadIdx.x + off].y;
-            }
-            __syncthreads();
+        y[i * S + s] = mk2<R>(yr, yi);
+        if (dotmode == DOT_XY) {
+            T xi = x[i * S + s];
+            c0 = make_double2((double)xi.x * yr - (double)xi.y * yi, (double)xi.x * yi + (double)xi.y * yr);
+        } else if (dotmode == DOT_CONJW_Y) {
+            T wi = w[i * S + s];
+            c0 = make_double2((double)wi.x * yr + (double)wi.y * yi, (double)wi.x * yi - (double)wi.y * yr);
+        } else if (dotmode == DOT_CONJY_W_YY) {
+            T wi = w[i * S + s];
+            c0 = make_double2((double)yr * wi.x + (double)yi * wi.y, (double)yr * wi.y - (double)yi * wi.x);
+            c1 = make_double2((double)yr * yr + (double)yi * yi, 0.0);
+            c2 = nrm2(wi);
         }
-        if (threadIdx.x < S) partial[(long long)blockIdx.x * S + threadIdx.x] = red[threadIdx.x];
     }
+    if (dotmode != DOT_NONE) block_store3(c0, c1, c2, dotmode == DOT_CONJY_W_YY ? 3 : 1, S, partial);
 }
 
 // Solver state per system (device).
 struct SysState {
-    double2 rho;      // r^T z
-    double2 mu;       // p^T A p
+    double2 rho;      // COCG: r^T z;   BiCGStab: (r_hat, r)
     double2 alpha;
     double2 beta;
+    double2 omega;
     double rn2;       // ||r||^2 (conjugated)
     double bn2;       // ||b||^2
     double tol2;      // tol^2 * bn2
+    double rh2;       // BiCGStab: ||r_hat||^2 (shadow residual)
     int active;
     int iters;
-    int status;       // 0 running/converged, 1 cap, 2 breakdown
-    int pad;
+    int status;       // 0 converged, 1 cap, 2 breakdown
+    int restart;      // BiCGStab: take r_hat = r at the next p update
 };
 
-// sum partial[b][s] over blocks in fixed order, one block per system; results to out[s]
-__global__ void reduce_partials_kernel(const double2* __restrict__ partial, int nblocks, int S, double2* out,
-                                       int ncomp) {
+__device__ __forceinline__ double2 cdiv2(double2 a, double2 b) {
+    if (fabs(b.x) >= fabs(b.y)) {
+        double r = b.y / b.x, d = b.x + b.y * r;
+        return make_double2((a.x + a.y * r) / d, (a.y - a.x * r) / d);
+    } else {
+        double r = b.x / b.y, d = b.x * r + b.y;
+        return make_double2((a.x * r + a.y) / d, (a.y * r - a.x) / d);
+    }
+}
+__device__ __forceinline__ double2 cmul2(double2 a, double2 b) { return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x); }
+__device__ __forceinline__ double cabs1(double2 a) { return fabs(a.x) + fabs(a.y); }
+
+enum UpdateMode { UPD_INIT = 0, UPD_SET_RHO = 1, UPD_COCG_ALPHA = 2, UPD_COCG_BETA = 3,
+                  UPD_BICG_ALPHA = 4, UPD_BICG_OMEGA = 5, UPD_BICG_RHO = 6 };
+
+__device__ void stop(SysState& q, int status) {
+    q.active = 0; q.status = status;
+    q.alpha = make_double2(0, 0); q.omega = make_double2(0, 0); q.beta = make_double2(0, 0);
+}
+
+// One block per system: fixed-order sum of the block partials, then the scalar recurrences.
+__global__ void reduce_update_kernel(const double2* __restrict__ partial, int nblocks, int S, int ncomp,
+                                     SysState* st, int mode, int maxit, double tol, int nsys) {
     __shared__ double2 red[VB];
+    __shared__ double2 sums[3];
     int s = blockIdx.x;
     for (int comp = 0; comp < ncomp; comp++) {
         double2 acc = make_double2(0, 0);
@@ -151,121 +215,155 @@ __global__ void reduce_partials_kernel(const double2* __restrict__ partial, int 
             if (threadIdx.x < off) { red[threadIdx.x].x += red[threadIdx.x + off].x; red[threadIdx.x].y += red[threadIdx.x + off].y; }
             __syncthreads();
         }
-        if (threadIdx.x == 0) out[comp * S + s] = red[0];
+        if (threadIdx.x == 0) sums[comp] = red[0];
         __syncthreads();
     }
-}
-
-__device__ __forceinline__ double2 cdiv2(double2 a, double2 b) {
-    if (fabs(b.x) >= fabs(b.y)) {
-        double r = b.y / b.x, d = b.x + b.y * r;
-        return make_double2((a.x + a.y * r) / d, (a.y - a.x * r) / d);
-    } else {
-        double r = b.x / b.y, d = b.x * r + b.y;
-        return make_double2((a.x * r + a.y) / d, (a.y * r - a.x) / d);
+    if (threadIdx.x != 0) return;
+    SysState& q = st[s];
+    double2 c0 = sums[0], c1 = ncomp > 1 ? sums[1] : make_double2(0, 0);
+    double c2 = ncomp > 2 ? sums[2].x : 0.0;
+    switch (mode) {
+    case UPD_INIT: {  // c0 = ||b||^2, c1 = ||r||^2
+        SysState z;
+        z.rho = z.alpha = z.beta = z.omega = make_double2(0, 0);
+        z.alpha.x = 1.0; z.omega.x = 1.0;
+        z.bn2 = c0.x; z.rn2 = c1.x; z.tol2 = tol * tol * c0.x;
+        z.iters = 0; z.status = 0; z.restart = 0; z.rh2 = 0;
+        z.active = (s < nsys) && (z.bn2 > 0) && (z.rn2 > z.tol2);
+        st[s] = z;
+        break;
+    }
+    case UPD_SET_RHO:
+        q.rho = c0;
+        q.rh2 = c0.x;
+        break;
+    case UPD_COCG_ALPHA:
+        if (!q.active) { q.alpha = make_double2(0, 0); break; }
+        if (!(cabs1(c0) > 0) || !isfinite(cabs1(c0))) { stop(q, 2); break; }
+        q.alpha = cdiv2(q.rho, c0);
+        break;
+    case UPD_COCG_BETA:
+        if (!q.active) { q.beta = make_double2(0, 0); break; }
+        q.rn2 = c1.x;
+        q.iters += 1;
+        if (q.rn2 <= q.tol2) { stop(q, 0); break; }
+        if (!isfinite(q.rn2)) { stop(q, 2); break; }
+        if (q.iters >= maxit) { stop(q, 1); break; }
+        if (!(cabs1(q.rho) > 0)) { stop(q, 2); break; }
+        q.beta = cdiv2(c0, q.rho);
+        q.rho = c0;
+        break;
+    case UPD_BICG_ALPHA:
+        q.restart = 0;
+        if (!q.active) { q.alpha = make_double2(0, 0); break; }
+        if (!(cabs1(c0) > 0) || !isfinite(cabs1(c0))) { stop(q, 2); break; }
+        q.alpha = cdiv2(q.rho, c0);
+        break;
+    case UPD_BICG_OMEGA: {
+        // c0 = (t, s), c1 = ||t||^2, c2 = ||s||^2.  Minimal-residual omega, enlarged when t and s are
+        // nearly orthogonal (Sleijpen & van der Vorst 1995, "maintaining convergence properties of
+        // BiCGstab methods in finite precision arithmetic": |cos| >= 0.7).
+        if (!q.active) { q.omega = make_double2(0, 0); break; }
+        if (!(c1.x > 0)) { q.omega = make_double2(0, 0); break; }
+        q.omega = make_double2(c0.x / c1.x, c0.y / c1.x);
+        double cosang = sqrt(c0.x * c0.x + c0.y * c0.y) / sqrt(c1.x * c2);
+        if (cosang > 0 && cosang < 0.7) { double f = 0.7 / cosang; q.omega.x *= f; q.omega.y *= f; }
+        break;
+    }
+    case UPD_BICG_RHO: {
+        if (!q.active) { q.beta = make_double2(0, 0); break; }
+        q.rn2 = c1.x;
+        q.iters += 1;
+        if (q.rn2 <= q.tol2) { stop(q, 0); break; }
+        if (!isfinite(q.rn2)) { stop(q, 2); break; }
+        if (q.iters >= maxit) { stop(q, 1); break; }
+        if (!(cabs1(q.rho) > 0) || !(cabs1(q.omega) > 0)) { stop(q, 2); break; }
+        // restart with r_hat = r when (r_hat, r) is nearly orthogonal (tol carries the threshold)
+        if (sqrt(c0.x * c0.x + c0.y * c0.y) < tol * sqrt(q.rh2 * q.rn2)) {
+            q.restart = 1;
+            q.rho = make_double2(q.rn2, 0.0);
+            q.rh2 = q.rn2;
+            q.beta = make_double2(0, 0);
+            break;
+        }
+        q.beta = cmul2(cdiv2(c0, q.rho), cdiv2(q.alpha, q.omega));
+        q.rho = c0;
+        break;
+    }
     }
 }
 
-// alpha = rho / mu for active systems; breakdown check
-__global__ void alpha_kernel(SysState* st, const double2* mu, int S) {
-    int s = threadIdx.x;
-    if (s >= S) return;
-    SysState& q = st[s];
-    q.mu = mu[s];
-    if (!q.active) { q.alpha = make_double2(0, 0); return; }
-    double m = fabs(q.mu.x) + fabs(q.mu.y);
-    if (!(m > 0) || !isfinite(m)) { q.active = 0; q.status = 2; q.alpha = make_double2(0, 0); return; }
-    q.alpha = cdiv2(q.rho, q.mu);
-}
-
-// Preconditioner application: z = M^-1 r on DOF pairs (i, i + h)
+// Preconditioner: z = M^-1 r on DOF pairs (i, i + h); precond 0 = identity.
 template <typename R>
-__device__ __forceinline__ void apply_block(int precond, const typename V2<R>::T* __restrict__ minv, long long h, int S,
-                                            long long i, int s, const typename V2<R>::T* r, typename V2<R>::T& z_lo,
-                                            typename V2<R>::T& z_hi) {
-    typedef typename V2<R>::T T;
-    T a = r[i * S + s], b = r[(i + h) * S + s];
+__device__ __forceinline__ void apply_pair(int precond, const typename V2<R>::T* __restrict__ minv, int S,
+                                           long long i, int s, typename V2<R>::T a, typename V2<R>::T b,
+                                           typename V2<R>::T& z_lo, typename V2<R>::T& z_hi) {
     if (precond == 0) { z_lo = a; z_hi = b; return; }
+    typedef typename V2<R>::T T;
     const T* m = minv + (i * S + s) * 4;
     T m00 = m[0], m01 = m[1], m10 = m[2], m11 = m[3];
     z_lo = mk2<R>(m00.x * a.x - m00.y * a.y + m01.x * b.x - m01.y * b.y, m00.x * a.y + m00.y * a.x + m01.x * b.y + m01.y * b.x);
     z_hi = mk2<R>(m10.x * a.x - m10.y * a.y + m11.x * b.x - m11.y * b.y, m10.x * a.y + m10.y * a.x + m11.x * b.y + m11.y * b.x);
 }
 
-// x += alpha p; r -= alpha q; z = M^-1 r; partial rho' = r^T z and ||r||^2.  Thread per (pair i, s).
+
+// ---- COCG vector kernels (thread per DOF pair i < h and system s) ----
 template <typename R>
-__global__ void __launch_bounds__(VB) update_kernel(long long h, int S, int precond, const SysState* __restrict__ st,
-                                                    typename V2<R>::T* __restrict__ x, typename V2<R>::T* __restrict__ r,
-                                                    typename V2<R>::T* __restrict__ z, const typename V2<R>::T* __restrict__ p,
-                                                    const typename V2<R>::T* __restrict__ q, const typename V2<R>::T* __restrict__ minv,
-                                                    double2* __restrict__ partial, long long nblocks) {
+__global__ void __launch_bounds__(VB) cocg_init_kernel(long long h, int S, int precond, const typename V2<R>::T* __restrict__ r,
+                                                       typename V2<R>::T* __restrict__ z, typename V2<R>::T* __restrict__ p,
+                                                       const typename V2<R>::T* __restrict__ minv, double2* __restrict__ partial) {
     typedef typename V2<R>::T T;
-    __shared__ double2 red[VB];
-    __shared__ double red2[VB];
     long long g = (long long)blockIdx.x * VB + threadIdx.x;
     long long i = g / S;
     int s = (int)(g % S);
     double2 rz = make_double2(0, 0);
-    double rr = 0;
+    if (i < h) {
+        T rl = r[i * S + s], rh = r[(i + h) * S + s], zl, zh;
+        apply_pair<R>(precond, minv, S, i, s, rl, rh, zl, zh);
+        z[i * S + s] = zl; z[(i + h) * S + s] = zh;
+        p[i * S + s] = zl; p[(i + h) * S + s] = zh;
+        double2 a = dotu(rl, zl), b = dotu(rh, zh);
+        rz = make_double2(a.x + b.x, a.y + b.y);
+    }
+    block_store2(rz, rz, 1, S, partial);
+}
+
+template <typename R>
+__global__ void __launch_bounds__(VB) cocg_update_kernel(long long h, int S, int precond, const SysState* __restrict__ st,
+                                                         typename V2<R>::T* __restrict__ x, typename V2<R>::T* __restrict__ r,
+                                                         typename V2<R>::T* __restrict__ z, const typename V2<R>::T* __restrict__ p,
+                                                         const typename V2<R>::T* __restrict__ q, const typename V2<R>::T* __restrict__ minv,
+                                                         double2* __restrict__ partial) {
+    typedef typename V2<R>::T T;
+    long long g = (long long)blockIdx.x * VB + threadIdx.x;
+    long long i = g / S;
+    int s = (int)(g % S);
+    double2 rz = make_double2(0, 0), rr = make_double2(0, 0);
     if (i < h) {
         double2 al = st[s].alpha;
         R ar = (R)al.x, ai = (R)al.y;
+        T rv2[2];
 #pragma unroll
         for (int half = 0; half < 2; half++) {
             long long k = (i + half * h) * S + s;
             T pv = p[k], qv = q[k], xv = x[k], rv = r[k];
             xv.x += ar * pv.x - ai * pv.y; xv.y += ar * pv.y + ai * pv.x;
             rv.x -= ar * qv.x - ai * qv.y; rv.y -= ar * qv.y + ai * qv.x;
-            x[k] = xv; r[k] = rv;
+            x[k] = xv; r[k] = rv; rv2[half] = rv;
         }
         T zl, zh;
-        apply_block<R>(precond, minv, h, S, i, s, r, zl, zh);
-        z[i * S + s] = zl;
-        z[(i + h) * S + s] = zh;
-        T rl = r[i * S + s], rh = r[(i + h) * S + s];
-        rz.x = (double)rl.x * zl.x - (double)rl.y * zl.y + (double)rh.x * zh.x - (double)rh.y * zh.y;
-        rz.y = (double)rl.x * zl.y + (double)rl.y * zl.x + (double)rh.x * zh.y + (double)rh.y * zh.x;
-        rr = (double)rl.x * rl.x + (double)rl.y * rl.y + (double)rh.x * rh.x + (double)rh.y * rh.y;
+        apply_pair<R>(precond, minv, S, i, s, rv2[0], rv2[1], zl, zh);
+        z[i * S + s] = zl; z[(i + h) * S + s] = zh;
+        double2 a = dotu(rv2[0], zl), b = dotu(rv2[1], zh);
+        rz = make_double2(a.x + b.x, a.y + b.y);
+        rr.x = nrm2(rv2[0]) + nrm2(rv2[1]);
     }
-    red[threadIdx.x] = rz;
-    red2[threadIdx.x] = rr;
-    __syncthreads();
-    for (int off = VB / 2; off >= S; off >>= 1) {
-        if (threadIdx.x < off) {
-            red[threadIdx.x].x += red[threadIdx.x + off].x;
-            red[threadIdx.x].y += red[threadIdx.x + off].y;
-            red2[threadIdx.x] += red2[threadIdx.x + off];
-        }
-        __syncthreads();
-    }
-    if (threadIdx.x < S) {
-        partial[(long long)blockIdx.x * S + threadIdx.x] = red[threadIdx.x];
-        partial[(nblocks + blockIdx.x) * S + threadIdx.x] = make_double2(red2[threadIdx.x], 0.0);
-    }
+    block_store2(rz, rr, 2, S, partial);
 }
 
-// beta = rho'/rho, convergence / breakdown / iteration bookkeeping
-__global__ void beta_kernel(SysState* st, const double2* red, int S, int maxit) {
-    int s = threadIdx.x;
-    if (s >= S) return;
-    SysState& q = st[s];
-    if (!q.active) { q.beta = make_double2(0, 0); return; }
-    double2 rho_new = red[s];
-    q.rn2 = red[S + s].x;
-    q.iters += 1;
-    if (q.rn2 <= q.tol2) { q.active = 0; q.status = 0; q.beta = make_double2(0, 0); return; }
-    if (!isfinite(q.rn2)) { q.active = 0; q.status = 2; q.beta = make_double2(0, 0); return; }
-    if (q.iters >= maxit) { q.active = 0; q.status = 1; q.beta = make_double2(0, 0); return; }
-    double m = fabs(q.rho.x) + fabs(q.rho.y);
-    if (!(m > 0)) { q.active = 0; q.status = 2; q.beta = make_double2(0, 0); return; }
-    q.beta = cdiv2(rho_new, q.rho);
-    q.rho = rho_new;
-}
-
-// p = z + beta p (active systems only)
 template <typename R>
-__global__ void pupdate_kernel(long long n, int S, const SysState* __restrict__ st, const typename V2<R>::T* __restrict__ z,
-                               typename V2<R>::T* __restrict__ p) {
+__global__ void cocg_pupdate_kernel(long long n, int S, const SysState* __restrict__ st, const typename V2<R>::T* __restrict__ z,
+                                    typename V2<R>::T* __restrict__ p) {
     long long g = (long long)blockIdx.x * VB + threadIdx.x;
     if (g >= n * S) return;
     int s = (int)(g % S);
@@ -276,45 +374,137 @@ __global__ void pupdate_kernel(long long n, int S, const SysState* __restrict__ 
     p[g] = mk2<R>(zv.x + br * pv.x - bi * pv.y, zv.y + br * pv.y + bi * pv.x);
 }
 
+// ---- BiCGStab vector kernels ----
+// r_hat = r, p = v = 0, partial (r_hat, r) = ||r||^2
+template <typename R>
+__global__ void __launch_bounds__(VB) bicg_init_kernel(long long n, int S, const typename V2<R>::T* __restrict__ r,
+                                                       typename V2<R>::T* __restrict__ rh, typename V2<R>::T* __restrict__ p,
+                                                       typename V2<R>::T* __restrict__ v, double2* __restrict__ partial) {
+    long long g = (long long)blockIdx.x * VB + threadIdx.x;
+    double2 c = make_double2(0, 0);
+    if (g < n * S) {
+        typename V2<R>::T rv = r[g];
+        rh[g] = rv;
+        p[g] = mk2<R>(0, 0);
+        v[g] = mk2<R>(0, 0);
+        c.x = nrm2(rv);
+    }
+    block_store2(c, c, 1, S, partial);
+}
+
+// p = r + beta (p - omega v); p_hat = M^-1 p   (thread per DOF pair)
+template <typename R>
+__global__ void __launch_bounds__(VB) bicg_p_kernel(long long h, int S, int precond, const SysState* __restrict__ st,
+                                                    const typename V2<R>::T* __restrict__ r, typename V2<R>::T* __restrict__ p,
+                                                    const typename V2<R>::T* __restrict__ v, typename V2<R>::T* __restrict__ ph,
+                                                    const typename V2<R>::T* __restrict__ minv, typename V2<R>::T* __restrict__ rh) {
+    typedef typename V2<R>::T T;
+    long long g = (long long)blockIdx.x * VB + threadIdx.x;
+    long long i = g / S;
+    int s = (int)(g % S);
+    if (i >= h) return;
+    double2 b = st[s].beta, w = st[s].omega;
+    R br = (R)b.x, bi = (R)b.y, wr = (R)w.x, wi = (R)w.y;
+    if (st[s].restart) {
+        rh[i * S + s] = r[i * S + s];
+        rh[(i + h) * S + s] = r[(i + h) * S + s];
+    }
+    T pn[2];
+#pragma unroll
+    for (int half = 0; half < 2; half++) {
+        long long k = (i + half * h) * S + s;
+        T rv = r[k], pv = p[k], vv = v[k];
+        R tr = pv.x - (wr * vv.x - wi * vv.y), ti = pv.y - (wr * vv.y + wi * vv.x);
+        pn[half] = mk2<R>(rv.x + br * tr - bi * ti, rv.y + br * ti + bi * tr);
+        p[k] = pn[half];
+    }
+    T zl, zh;
+    apply_pair<R>(precond, minv, S, i, s, pn[0], pn[1], zl, zh);
+    ph[i * S + s] = zl;
+    ph[(i + h) * S + s] = zh;
+}
+
+// s = r - alpha v (stored in r); s_hat = M^-1 s
+template <typename R>
+__global__ void __launch_bounds__(VB) bicg_s_kernel(long long h, int S, int precond, const SysState* __restrict__ st,
+                                                    typename V2<R>::T* __restrict__ r, const typename V2<R>::T* __restrict__ v,
+                                                    typename V2<R>::T* __restrict__ sh, const typename V2<R>::T* __restrict__ minv) {
+    typedef typename V2<R>::T T;
+    long long g = (long long)blockIdx.x * VB + threadIdx.x;
+    long long i = g / S;
+    int s = (int)(g % S);
+    if (i >= h) return;
+    double2 a = st[s].alpha;
+    R ar = (R)a.x, ai = (R)a.y;
+    T sn[2];
+#pragma unroll
+    for (int half = 0; half < 2; half++) {
+        long long k = (i + half * h) * S + s;
+        T rv = r[k], vv = v[k];
+        sn[half] = mk2<R>(rv.x - (ar * vv.x - ai * vv.y), rv.y - (ar * vv.y + ai * vv.x));
+        r[k] = sn[half];
+    }
+    T zl, zh;
+    apply_pair<R>(precond, minv, S, i, s, sn[0], sn[1], zl, zh);
+    sh[i * S + s] = zl;
+    sh[(i + h) * S + s] = zh;
+}
+
+// x += alpha p_hat + omega s_hat; r = s - omega t; partial (r_hat, r) and ||r||^2
+template <typename R>
+__global__ void __launch_bounds__(VB) bicg_x_kernel(long long n, int S, const SysState* __restrict__ st,
+                                                    typename V2<R>::T* __restrict__ x, typename V2<R>::T* __restrict__ r,
+                                                    const typename V2<R>::T* __restrict__ ph, const typename V2<R>::T* __restrict__ sh,
+                                                    const typename V2<R>::T* __restrict__ t, const typename V2<R>::T* __restrict__ rh,
+                                                    double2* __restrict__ partial) {
+    typedef typename V2<R>::T T;
+    long long g = (long long)blockIdx.x * VB + threadIdx.x;
+    double2 c0 = make_double2(0, 0), c1 = c0;
+    if (g < n * S) {
+        int s = (int)(g % S);
+        double2 a = st[s].alpha, w = st[s].omega;
+        R ar = (R)a.x, ai = (R)a.y, wr = (R)w.x, wi = (R)w.y;
+        T xv = x[g], pv = ph[g], sv = sh[g], rv = r[g], tv = t[g];
+        xv.x += ar * pv.x - ai * pv.y + wr * sv.x - wi * sv.y;
+        xv.y += ar * pv.y + ai * pv.x + wr * sv.y + wi * sv.x;
+        rv.x -= wr * tv.x - wi * tv.y;
+        rv.y -= wr * tv.y + wi * tv.x;
+        x[g] = xv;
+        r[g] = rv;
+        c0 = dotc(rh[g], rv);
+        c1.x = nrm2(rv);
+    }
+    block_store2(c0, c1, 2, S, partial);
+}
+
 // ---- setup kernels -------------------------------------------------------------------
-// r = b - A x (FP64) into r64 (masked), also ||b||^2, ||r||^2 partials. x masked entries zeroed first.
 __global__ void mask_vec_kernel(long long n, int S, const uint8_t* mask, double2* v) {
     long long g = (long long)blockIdx.x * VB + threadIdx.x;
     if (g >= n * S) return;
     if (!mask[g / S]) v[g] = make_double2(0, 0);
 }
 
+// r = b - Ax on free DOFs; partials ||b||^2 and ||r||^2
 __global__ void __launch_bounds__(VB) residual_kernel(long long n, int S, const uint8_t* __restrict__ mask,
                                                        const double2* __restrict__ b, const double2* __restrict__ Ax,
-                                                       double2* __restrict__ r, double2* __restrict__ partial, long long nblocks) {
-    __shared__ double rb[VB], rr[VB];
+                                                       double2* __restrict__ r, double2* __restrict__ partial) {
     long long g = (long long)blockIdx.x * VB + threadIdx.x;
-    double vb = 0, vr = 0;
+    double2 cb = make_double2(0, 0), cr = cb;
     if (g < n * S) {
         long long i = g / S;
         double2 res = make_double2(0, 0);
         if (mask[i]) {
             double2 bv = b[g], av = Ax[g];
             res = make_double2(bv.x - av.x, bv.y - av.y);
-            vb = bv.x * bv.x + bv.y * bv.y;
-            vr = res.x * res.x + res.y * res.y;
+            cb.x = bv.x * bv.x + bv.y * bv.y;
+            cr.x = res.x * res.x + res.y * res.y;
         }
         r[g] = res;
     }
-    rb[threadIdx.x] = vb; rr[threadIdx.x] = vr;
-    __syncthreads();
-    int S_ = S;
-    for (int off = VB / 2; off >= S_; off >>= 1) {
-        if (threadIdx.x < off) { rb[threadIdx.x] += rb[threadIdx.x + off]; rr[threadIdx.x] += rr[threadIdx.x + off]; }
-        __syncthreads();
-    }
-    if (threadIdx.x < S_) {
-        partial[(long long)blockIdx.x * S_ + threadIdx.x] = make_double2(rb[threadIdx.x], 0);
-        partial[(nblocks + blockIdx.x) * S_ + threadIdx.x] = make_double2(rr[threadIdx.x], 0);
-    }
+    block_store2(cb, cr, 2, S, partial);
 }
 
-// Block-Jacobi / point-Jacobi inverse blocks from the operator's diagonal 2x2 pair blocks.
+// Operator entry (row, col) of system s (E - k0^2 B + patch), used by the preconditioner setup.
 __device__ __forceinline__ double2 row_value(const OpArgs& a, long long row, long long col, int s) {
     const double2* Ev = (const double2*)a.E;
     const double2* Bv = (const double2*)a.B;
@@ -344,6 +534,7 @@ __device__ __forceinline__ double2 row_value(const OpArgs& a, long long row, lon
     return v;
 }
 
+// Inverse 2x2 pair blocks (precond 2) or inverse diagonals (precond 1); op is the FP64 operator.
 template <typename R>
 __global__ void precond_setup_kernel(OpArgs a, int precond, typename V2<R>::T* __restrict__ minv) {
     long long h = a.n / 2;
@@ -359,78 +550,25 @@ __global__ void precond_setup_kernel(OpArgs a, int precond, typename V2<R>::T* _
     double2 a11 = fj ? row_value(a, j, j, s) : make_double2(1, 0);
     double2 a01 = (fi && fj) ? row_value(a, i, j, s) : make_double2(0, 0);
     double2 a10 = (fi && fj) ? row_value(a, j, i, s) : make_double2(0, 0);
-    auto inv1 = [](double2 v) {
-        double m = fabs(v.x) + fabs(v.y);
-        return m > 0 ? cdiv2(make_double2(1, 0), v) : make_double2(1, 0);
-    };
+    auto inv1 = [](double2 v) { return cabs1(v) > 0 ? cdiv2(make_double2(1, 0), v) : make_double2(1, 0); };
+    bool done = false;
     if (precond == 2) {
         double2 det = make_double2(a00.x * a11.x - a00.y * a11.y - (a01.x * a10.x - a01.y * a10.y),
                                    a00.x * a11.y + a00.y * a11.x - (a01.x * a10.y + a01.y * a10.x));
-        double dm = fabs(det.x) + fabs(det.y);
-        double sc = fabs(a00.x) + fabs(a00.y) + fabs(a11.x) + fabs(a11.y);
-        if (dm > 1e-14 * sc * sc && isfinite(dm)) {
+        double sc = cabs1(a00) * cabs1(a11);
+        if (cabs1(det) > 1e-12 * sc && isfinite(cabs1(det))) {
             double2 id = cdiv2(make_double2(1, 0), det);
-            auto mul = [](double2 u, double2 v) { return make_double2(u.x * v.x - u.y * v.y, u.x * v.y + u.y * v.x); };
-            m00 = mul(a11, id);
-            m11 = mul(a00, id);
-            m01 = mul(make_double2(-a01.x, -a01.y), id);
-            m10 = mul(make_double2(-a10.x, -a10.y), id);
-        } else {
-            m00 = inv1(a00); m11 = inv1(a11);
+            m00 = cmul2(a11, id);
+            m11 = cmul2(a00, id);
+            m01 = cmul2(make_double2(-a01.x, -a01.y), id);
+            m10 = cmul2(make_double2(-a10.x, -a10.y), id);
+            done = true;
         }
-    } else {
-        m00 = inv1(a00); m11 = inv1(a11);
     }
+    if (!done) { m00 = inv1(a00); m11 = inv1(a11); }
     typename V2<R>::T* m = minv + (i * S + s) * 4;
     m[0] = mk2<R>((R)m00.x, (R)m00.y); m[1] = mk2<R>((R)m01.x, (R)m01.y);
     m[2] = mk2<R>((R)m10.x, (R)m10.y); m[3] = mk2<R>((R)m11.x, (R)m11.y);
-}
-
-__global__ void init_state_kernel(SysState* st, const double2* red, int S, int nsys, double tol, int use_x0) {
-    int s = threadIdx.x;
-    if (s >= S) return;
-    SysState q;
-    q.rho = make_double2(0, 0); q.mu = q.rho; q.alpha = q.rho; q.beta = q.rho;
-    q.bn2 = red[s].x;
-    q.rn2 = red[S + s].x;
-    q.tol2 = tol * tol * q.bn2;
-    q.iters = 0; q.status = 0; q.pad = 0;
-    q.active = (s < nsys) && (q.rn2 > q.tol2) && (q.bn2 > 0);
-    st[s] = q;
-}
-
-// after z = M^-1 r for the initial residual: rho = r^T z, p = z
-template <typename R>
-__global__ void __launch_bounds__(VB) init_z_kernel(long long h, int S, int precond, const typename V2<R>::T* __restrict__ r,
-                                                    typename V2<R>::T* __restrict__ z, typename V2<R>::T* __restrict__ p,
-                                                    const typename V2<R>::T* __restrict__ minv, double2* __restrict__ partial) {
-    typedef typename V2<R>::T T;
-    __shared__ double2 red[VB];
-    long long g = (long long)blockIdx.x * VB + threadIdx.x;
-    long long i = g / S;
-    int s = (int)(g % S);
-    double2 rz = make_double2(0, 0);
-    if (i < h) {
-        T zl, zh;
-        apply_block<R>(precond, minv, h, S, i, s, r, zl, zh);
-        z[i * S + s] = zl; z[(i + h) * S + s] = zh;
-        p[i * S + s] = zl; p[(i + h) * S + s] = zh;
-        T rl = r[i * S + s], rh = r[(i + h) * S + s];
-        rz.x = (double)rl.x * zl.x - (double)rl.y * zl.y + (double)rh.x * zh.x - (double)rh.y * zh.y;
-        rz.y = (double)rl.x * zl.y + (double)rl.y * zl.x + (double)rh.x * zh.y + (double)rh.y * zh.x;
-    }
-    red[threadIdx.x] = rz;
-    __syncthreads();
-    for (int off = VB / 2; off >= S; off >>= 1) {
-        if (threadIdx.x < off) { red[threadIdx.x].x += red[threadIdx.x + off].x; red[threadIdx.x].y += red[threadIdx.x + off].y; }
-        __syncthreads();
-    }
-    if (threadIdx.x < S) partial[(long long)blockIdx.x * S + threadIdx.x] = red[threadIdx.x];
-}
-
-__global__ void set_rho_kernel(SysState* st, const double2* red, int S) {
-    int s = threadIdx.x;
-    if (s < S) st[s].rho = red[s];
 }
 
 // conversions / scaled copies for the mixed-precision refinement
@@ -447,11 +585,11 @@ __global__ void to_f32_scaled_kernel(long long n, int S, const double2* __restri
 }
 
 __global__ void add_scaled_f32_kernel(long long n, int S, const float2* __restrict__ d, const double* __restrict__ scale,
-                                      const int* __restrict__ outer_active, double2* __restrict__ x) {
+                                      const SysState* __restrict__ outer, double2* __restrict__ x) {
     long long g = (long long)blockIdx.x * VB + threadIdx.x;
     if (g >= n * S) return;
     int s = (int)(g % S);
-    if (!outer_active[s]) return;
+    if (!outer[s].active) return;
     double sc = scale[s];
     float2 v = d[g];
     x[g].x += sc * (double)v.x;
@@ -461,6 +599,21 @@ __global__ void add_scaled_f32_kernel(long long n, int S, const float2* __restri
 __global__ void cast_values_kernel(long long nnz, const double2* __restrict__ src, float2* __restrict__ dst) {
     long long g = (long long)blockIdx.x * VB + threadIdx.x;
     if (g < nnz) dst[g] = make_float2((float)src[g].x, (float)src[g].y);
+}
+
+// inner state for one refinement step: unit-norm rhs, relative tolerance `itol`, active = outer active
+__global__ void inner_init_kernel(SysState* inner, const SysState* outer, int S, double itol) {
+    int s = threadIdx.x;
+    if (s >= S) return;
+    SysState z;
+    z.rho = z.alpha = z.beta = z.omega = make_double2(0, 0);
+    z.alpha.x = 1.0; z.omega.x = 1.0;
+    z.active = outer[s].active;
+    z.bn2 = z.active ? 1.0 : 0.0;
+    z.rn2 = z.bn2;
+    z.tol2 = itol * itol;
+    z.iters = 0; z.status = 0; z.restart = 0; z.rh2 = 0;
+    inner[s] = z;
 }
 
 __global__ void patch_map_kernel(long long np, const int* rows, int* patch_of_row) {
@@ -489,7 +642,7 @@ __global__ void combine_kernel(long long nnz, const double2* __restrict__ E, con
     long long g = (long long)blockIdx.x * VB + threadIdx.x;
     if (g >= nnz) return;
     double2 e = E[g], b = B[g];
-    // (E - (k0^2 B)) with the product rounded first, as the reference's E - B*k0**2
+    // (E - (B k0^2)) with the product rounded first, as the reference's E - B*k0**2
     double bx = __dmul_rn(b.x, k0sq), by = __dmul_rn(b.y, k0sq);
     K[g] = make_double2(__dsub_rn(e.x, bx), __dsub_rn(e.y, by));
 }
@@ -512,10 +665,11 @@ static int pow2_at_least(int v) {
 
 // ---- workspace layout ----------------------------------------------------------------------
 struct Layout {
-    size_t off_state, off_gamma, off_k0, off_partial, off_red, off_patchmap, off_scale, off_oactive;
+    size_t off_state, off_gamma, off_k0, off_partial, off_patchmap, off_scale;
     size_t off_x, off_b, off_r64, off_Ax;                  // FP64 vectors (n, S)
-    size_t off_r, off_z, off_p, off_q, off_minv;           // Krylov vectors of the inner precision
-    size_t off_E32, off_B32, off_P32;                      // FP32 matrix copies (mixed)
+    size_t off_v[8];                                       // Krylov vectors of the inner precision
+    size_t off_minv;
+    size_t off_E32, off_B32, off_P32;                      // FP32 operator copies (mixed)
     size_t total;
 };
 
@@ -530,19 +684,14 @@ static Layout make_layout(long long n, long long nnz, long long npatch, int S, i
     L.off_state = o; o = align256(o + sizeof(SysState) * 2 * S);
     L.off_gamma = o; o = align256(o + sizeof(double) * 2 * S * (nports > 0 ? nports : 1));
     L.off_k0 = o; o = align256(o + sizeof(double) * S);
-    L.off_partial = o; o = align256(o + sizeof(double2) * 2 * nb * S);
-    L.off_red = o; o = align256(o + sizeof(double2) * 2 * S);
+    L.off_partial = o; o = align256(o + sizeof(double2) * 3 * nb * S);
     L.off_patchmap = o; o = align256(o + sizeof(int) * n);
     L.off_scale = o; o = align256(o + sizeof(double) * S);
-    L.off_oactive = o; o = align256(o + sizeof(int) * S);
     L.off_x = o; o = align256(o + vec64);
     L.off_b = o; o = align256(o + vec64);
     L.off_r64 = o; o = align256(o + vec64);
     L.off_Ax = o; o = align256(o + vec64);
-    L.off_r = o; o = align256(o + vecw);
-    L.off_z = o; o = align256(o + vecw);
-    L.off_p = o; o = align256(o + vecw);
-    L.off_q = o; o = align256(o + vecw);
+    for (int k = 0; k < 8; k++) { L.off_v[k] = o; o = align256(o + vecw); }
     L.off_minv = o; o = align256(o + vecw * 2);  // (n/2) * S * 4 entries
     if (precision) {
         L.off_E32 = o; o = align256(o + sizeof(float2) * nnz);
@@ -555,46 +704,73 @@ static Layout make_layout(long long n, long long nnz, long long npatch, int S, i
     return L;
 }
 
-// One Krylov solve (inner precision R) on the operator `op` for rhs already in r (= b - A x0 form
-// is handled by the caller): runs COCG iterations from x = 0 with initial residual r.
+// Batched Krylov solve in precision R from x = 0 with the initial residual already in r and the
+// per-system state (bn2, tol2, active) in st.
 template <typename R>
-struct Cocg {
+struct Krylov {
     typedef typename V2<R>::T T;
+    int method = 1;            // 0 COCG, 1 BiCGStab
     OpArgs op;
-    long long n, h;
-    int S, precond, maxit;
-    T *x, *r, *z, *p, *q, *minv;
-    double2 *partial, *red;
-    SysState* st;
-    long long nb_rows, nb_pairs;
-    cudaStream_t s;
+    long long n = 0, h = 0;
+    int S = 1, precond = 2, maxit = 1000, nsys = 1;
+    T *x = nullptr, *r = nullptr, *minv = nullptr;
+    T* v[7] = {nullptr};       // work vectors
+    double2* partial = nullptr;
+    SysState* st = nullptr;
+    cudaStream_t s = nullptr;
 
-    int launch_iteration() {
-        spmv_kernel<R><<<(unsigned)nb_rows, VB, 0, s>>>(op, p, q, partial);
-        reduce_partials_kernel<<<S, VB, 0, s>>>(partial, (int)nb_rows, S, red, 1);
-        alpha_kernel<<<1, 64, 0, s>>>(st, red, S);
-        update_kernel<R><<<(unsigned)nb_pairs, VB, 0, s>>>(h, S, precond, st, x, r, z, p, q, minv, partial, nb_pairs);
-        reduce_partials_kernel<<<S, VB, 0, s>>>(partial, (int)nb_pairs, S, red, 2);
-        beta_kernel<<<1, 64, 0, s>>>(st, red, S, maxit);
-        pupdate_kernel<R><<<grid_for(n * S, VB), VB, 0, s>>>(n, S, st, z, p);
-        return check_cuda(cudaGetLastError(), "cocg iteration");
+    unsigned nb_all() const { return grid_for(n * (long long)S, VB); }
+    unsigned nb_pair() const { return grid_for(h * (long long)S, VB); }
+
+    double restart_eps = sizeof(R) == 8 ? 1e-9 : 1e-4;
+    void reduce(int ncomp, unsigned nblocks, int mode) {
+        reduce_update_kernel<<<S, VB, 0, s>>>(partial, (int)nblocks, S, ncomp, st, mode, maxit, restart_eps, nsys);
     }
 
-    // start: r holds the initial residual (masked), x holds 0; st[].bn2/tol2/active set.
     int start() {
-        init_z_kernel<R><<<(unsigned)nb_pairs, VB, 0, s>>>(h, S, precond, r, z, p, minv, partial);
-        reduce_partials_kernel<<<S, VB, 0, s>>>(partial, (int)nb_pairs, S, red, 1);
-        set_rho_kernel<<<1, 64, 0, s>>>(st, red, S);
-        return check_cuda(cudaGetLastError(), "cocg start");
+        if (method == 0) {
+            T *z = v[0], *p = v[1];
+            cocg_init_kernel<R><<<nb_pair(), VB, 0, s>>>(h, S, precond, r, z, p, minv, partial);
+            reduce(1, nb_pair(), UPD_SET_RHO);
+        } else {
+            T *rh = v[0], *p = v[1], *vv = v[2];
+            bicg_init_kernel<R><<<nb_all(), VB, 0, s>>>(n, S, r, rh, p, vv, partial);
+            reduce(1, nb_all(), UPD_SET_RHO);
+        }
+        return check_cuda(cudaGetLastError(), "krylov start");
     }
 
+    int iteration() {
+        if (method == 0) {
+            T *z = v[0], *p = v[1], *q = v[2];
+            spmv_kernel<R><<<nb_all(), VB, 0, s>>>(op, p, q, partial, DOT_XY, nullptr);
+            reduce(1, nb_all(), UPD_COCG_ALPHA);
+            cocg_update_kernel<R><<<nb_pair(), VB, 0, s>>>(h, S, precond, st, x, r, z, p, q, minv, partial);
+            reduce(2, nb_pair(), UPD_COCG_BETA);
+            cocg_pupdate_kernel<R><<<nb_all(), VB, 0, s>>>(n, S, st, z, p);
+        } else {
+            T *rh = v[0], *p = v[1], *vv = v[2], *ph = v[3], *sh = v[4], *t = v[5];
+            bicg_p_kernel<R><<<nb_pair(), VB, 0, s>>>(h, S, precond, st, r, p, vv, ph, minv, rh);
+            spmv_kernel<R><<<nb_all(), VB, 0, s>>>(op, ph, vv, partial, DOT_CONJW_Y, rh);
+            reduce(1, nb_all(), UPD_BICG_ALPHA);
+            bicg_s_kernel<R><<<nb_pair(), VB, 0, s>>>(h, S, precond, st, r, vv, sh, minv);
+            spmv_kernel<R><<<nb_all(), VB, 0, s>>>(op, sh, t, partial, DOT_CONJY_W_YY, r);
+            reduce(3, nb_all(), UPD_BICG_OMEGA);
+            bicg_x_kernel<R><<<nb_all(), VB, 0, s>>>(n, S, st, x, r, ph, sh, t, rh, partial);
+            reduce(2, nb_all(), UPD_BICG_RHO);
+        }
+        return check_cuda(cudaGetLastError(), "krylov iteration");
+    }
+
+    // one eager iteration (loads every kernel before capture), then `chunk` iterations captured once
+    // and replayed until no system is active or the iteration cap is reached
     int run(int chunk) {
-        // capture `chunk` iterations once, replay until no system is active
+        EMFEM_TRY(iteration());
         cudaGraph_t graph = nullptr;
         cudaGraphExec_t exec = nullptr;
         EMFEM_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
         int st_cap = EMFEM_OK;
-        for (int k = 0; k < chunk && st_cap == EMFEM_OK; k++) st_cap = launch_iteration();
+        for (int k = 0; k < chunk && st_cap == EMFEM_OK; k++) st_cap = iteration();
         cudaError_t e = cudaStreamEndCapture(s, &graph);
         if (st_cap != EMFEM_OK) { if (graph) cudaGraphDestroy(graph); return st_cap; }
         EMFEM_CUDA(e);
@@ -620,12 +796,20 @@ struct Cocg {
 
 using namespace emfem;
 
+static void build_op(OpArgs& a, int64_t n, int S, const int32_t* indptr, const int32_t* indices, const void* E,
+                     const void* B, const double* k0dev, const int* pmap, const int32_t* prowptr, const int32_t* pcols,
+                     const void* pvals, const int32_t* pport, int nports, const double* gdev, const uint8_t* mask) {
+    a.n = n; a.S = S; a.indptr = indptr; a.indices = indices; a.E = E; a.B = B; a.k0sq = k0dev;
+    a.patch_of_row = pmap; a.patch_rowptr = prowptr; a.patch_cols = pcols; a.patch_vals = pvals; a.patch_port = pport;
+    a.n_ports = nports; a.gamma = gdev; a.mask = mask;
+}
+
 extern "C" {
 
-int emfem_cocg_workspace_size(int64_t n, int64_t nnz, int nsys, int precision, size_t* bytes) {
-    EMFEM_REQUIRE(bytes && n > 0 && nsys > 0 && nsys <= 64, "emfem_cocg_workspace_size: bad argument");
+int emfem_krylov_workspace_size(int64_t n, int64_t nnz, int nsys, int precision, size_t* bytes) {
+    EMFEM_REQUIRE(bytes && n > 0 && nsys > 0 && nsys <= 64 && nnz >= 0, "emfem_krylov_workspace_size: bad argument");
+    EMFEM_REQUIRE(precision == 0 || precision == 1, "emfem_krylov_workspace_size: precision must be 0 or 1");
     int S = pow2_at_least(nsys);
-    // patch size bound: callers pass npatch <= nnz; reserve for nnz/8 (ports touch few rows)
     Layout L = make_layout(n, nnz, nnz, S, 8, precision);
     *bytes = L.total;
     return EMFEM_OK;
@@ -649,15 +833,6 @@ int emfem_sweep_combine(emfem_handle h, int64_t nnz, const void* E_vals, const v
     return EMFEM_OK;
 }
 
-static int build_op(OpArgs& a, int64_t n, int S, const int32_t* indptr, const int32_t* indices, const void* E,
-                    const void* B, const double* k0dev, const int* pmap, const int32_t* prowptr, const int32_t* pcols,
-                    const void* pvals, const int32_t* pport, int nports, const double* gdev, const uint8_t* mask) {
-    a.n = n; a.S = S; a.indptr = indptr; a.indices = indices; a.E = E; a.B = B; a.k0sq = k0dev;
-    a.patch_of_row = pmap; a.patch_rowptr = prowptr; a.patch_cols = pcols; a.patch_vals = pvals; a.patch_port = pport;
-    a.n_ports = nports; a.gamma = gdev; a.mask = mask;
-    return EMFEM_OK;
-}
-
 int emfem_sweep_spmv(emfem_handle h, int64_t n, const int32_t* indptr, const int32_t* indices,
                      const void* E_vals, const void* B_vals, int nsys, const double* k0sq_dev,
                      int64_t n_patch_rows, const int32_t* patch_rows, const int32_t* patch_rowptr,
@@ -665,7 +840,7 @@ int emfem_sweep_spmv(emfem_handle h, int64_t n, const int32_t* indptr, const int
                      int n_ports, const double* gamma_dev, const uint8_t* free_mask, const void* x, void* y) {
     EMFEM_REQUIRE(h && indptr && indices && E_vals && k0sq_dev && free_mask && x && y && n > 0,
                   "emfem_sweep_spmv: bad argument");
-    EMFEM_REQUIRE(nsys >= 1 && nsys <= 256 && (VB % nsys) == 0 && (nsys & (nsys - 1)) == 0,
+    EMFEM_REQUIRE(nsys >= 1 && nsys <= 256 && (nsys & (nsys - 1)) == 0,
                   "emfem_sweep_spmv: nsys must be a power of two <= 256");
     EMFEM_REQUIRE(n_patch_rows == 0 || (patch_rows && patch_rowptr && patch_cols && patch_vals && patch_port && gamma_dev),
                   "emfem_sweep_spmv: patch arrays missing");
@@ -679,28 +854,30 @@ int emfem_sweep_spmv(emfem_handle h, int64_t n, const int32_t* indptr, const int
     OpArgs a;
     build_op(a, n, nsys, indptr, indices, E_vals, B_vals, k0sq_dev, pmap, patch_rowptr, patch_cols, patch_vals,
              patch_port, n_ports, gamma_dev, free_mask);
-    spmv_kernel<double><<<grid_for(n * nsys, VB), VB, 0, h->h.stream>>>(a, (const double2*)x, (double2*)y, nullptr);
+    spmv_kernel<double><<<grid_for(n * nsys, VB), VB, 0, h->h.stream>>>(a, (const double2*)x, (double2*)y, nullptr,
+                                                                          DOT_NONE, nullptr);
     EMFEM_LAUNCH("spmv_kernel");
     if (pmap) EMFEM_CUDA(cudaFreeAsync(pmap, h->h.stream));
     return EMFEM_OK;
 }
 
-int emfem_cocg_solve(emfem_handle hd, int64_t n, int64_t nnz, const int32_t* indptr, const int32_t* indices,
-                     const void* E_vals, const void* B_vals, int nsys, const double* k0sq,
-                     int64_t n_patch_rows, const int32_t* patch_rows, const int32_t* patch_rowptr,
-                     const int32_t* patch_cols, const void* patch_vals, const int32_t* patch_port,
-                     int n_ports, const double* gamma, const uint8_t* free_mask, const void* rhs, void* x,
-                     double tol, int maxit, int precond, int precision, void* workspace, size_t workspace_bytes,
-                     int* status, int* iters, double* relres) {
+int emfem_krylov_solve(emfem_handle hd, int method, int64_t n, int64_t nnz, const int32_t* indptr, const int32_t* indices,
+                       const void* E_vals, const void* B_vals, int nsys, const double* k0sq,
+                       int64_t n_patch_rows, const int32_t* patch_rows, const int32_t* patch_rowptr,
+                       const int32_t* patch_cols, const void* patch_vals, const int32_t* patch_port,
+                       int n_ports, const double* gamma, const uint8_t* free_mask, const void* rhs, void* x,
+                       double tol, int maxit, int precond, int precision, void* workspace, size_t workspace_bytes,
+                       int* status, int* iters, double* relres) {
     EMFEM_REQUIRE(hd && indptr && indices && E_vals && k0sq && free_mask && rhs && x && workspace,
-                  "emfem_cocg_solve: null argument");
-    EMFEM_REQUIRE(n > 0 && (n % 2) == 0, "emfem_cocg_solve: n must be even (DOF pairs i, i + n/2)");
-    EMFEM_REQUIRE(nsys >= 1 && nsys <= 64, "emfem_cocg_solve: 1 <= nsys <= 64");
-    EMFEM_REQUIRE(precond >= 0 && precond <= 2 && (precision == 0 || precision == 1), "emfem_cocg_solve: bad option");
-    EMFEM_REQUIRE(n_ports >= 0 && n_ports <= 8, "emfem_cocg_solve: at most 8 ports");
+                  "emfem_krylov_solve: null argument");
+    EMFEM_REQUIRE(method == 0 || method == 1, "emfem_krylov_solve: method must be 0 (COCG) or 1 (BiCGStab)");
+    EMFEM_REQUIRE(n > 0 && (n % 2) == 0, "emfem_krylov_solve: n must be even (DOF pairs i, i + n/2)");
+    EMFEM_REQUIRE(nsys >= 1 && nsys <= 64, "emfem_krylov_solve: 1 <= nsys <= 64");
+    EMFEM_REQUIRE(precond >= 0 && precond <= 2 && (precision == 0 || precision == 1), "emfem_krylov_solve: bad option");
+    EMFEM_REQUIRE(n_ports >= 0 && n_ports <= 8, "emfem_krylov_solve: at most 8 ports");
     EMFEM_REQUIRE(n_patch_rows == 0 || (patch_rows && patch_rowptr && patch_cols && patch_vals && patch_port && gamma),
-                  "emfem_cocg_solve: patch arrays missing");
-    EMFEM_REQUIRE(tol > 0 && maxit > 0, "emfem_cocg_solve: tol and maxit must be positive");
+                  "emfem_krylov_solve: patch arrays missing");
+    EMFEM_REQUIRE(tol > 0 && maxit > 0, "emfem_krylov_solve: tol and maxit must be positive");
     Handle* h = &hd->h;
     int S = pow2_at_least(nsys);
     int64_t npatch = 0;
@@ -709,39 +886,47 @@ int emfem_cocg_solve(emfem_handle hd, int64_t n, int64_t nnz, const int32_t* ind
         EMFEM_CUDA(cudaMemcpy(&last, patch_rowptr + n_patch_rows, sizeof(int32_t), cudaMemcpyDeviceToHost));
         npatch = last;
     }
+    EMFEM_REQUIRE(npatch <= nnz, "emfem_krylov_solve: more patch entries than nnz");
     Layout L = make_layout(n, nnz, npatch, S, n_ports, precision);
-    if (workspace_bytes < L.total) {
-        set_error("emfem_cocg_solve: workspace of %zu bytes, %zu needed", workspace_bytes, L.total);
+    size_t need = make_layout(n, nnz, nnz, S, 8, precision).total;
+    if (workspace_bytes < need) {
+        set_error("emfem_krylov_solve: workspace of %zu bytes, %zu needed (emfem_krylov_workspace_size)", workspace_bytes, need);
         return EMFEM_ERR_WORKSPACE;
     }
     char* ws = (char*)workspace;
     cudaStream_t s = nullptr;
     EMFEM_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
     cudaEvent_t ev;
-    EMFEM_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
-    EMFEM_CUDA(cudaEventRecord(ev, h->stream));
-    EMFEM_CUDA(cudaStreamWaitEvent(s, ev, 0));
-
+    if (cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess) {
+        cudaStreamDestroy(s);
+        set_error("emfem_krylov_solve: cudaEventCreate failed");
+        return EMFEM_ERR_CUDA;
+    }
     SysState* st = (SysState*)(ws + L.off_state);
     SysState* st_outer = st + S;
     double* gdev = (double*)(ws + L.off_gamma);
     double* k0dev = (double*)(ws + L.off_k0);
     double2* partial = (double2*)(ws + L.off_partial);
-    double2* red = (double2*)(ws + L.off_red);
     int* pmap = (int*)(ws + L.off_patchmap);
     double* scale = (double*)(ws + L.off_scale);
-    int* oactive = (int*)(ws + L.off_oactive);
     double2* x64 = (double2*)(ws + L.off_x);
     double2* b64 = (double2*)(ws + L.off_b);
     double2* r64 = (double2*)(ws + L.off_r64);
     double2* Ax = (double2*)(ws + L.off_Ax);
-
+    long long nS = n * (long long)S;
+    unsigned gv = grid_for(nS, VB);
     std::vector<double> hk0(S, 0.0), hg(2 * S * (n_ports > 0 ? n_ports : 1), 0.0);
     for (int k = 0; k < nsys; k++) hk0[k] = k0sq[k];
     for (int k = 0; k < nsys; k++)
-        for (int q = 0; q < n_ports; q++) { hg[2 * (k * n_ports + q)] = gamma[2 * (k * n_ports + q)]; hg[2 * (k * n_ports + q) + 1] = gamma[2 * (k * n_ports + q) + 1]; }
+        for (int q = 0; q < n_ports; q++) {
+            hg[2 * (k * n_ports + q)] = gamma[2 * (k * n_ports + q)];
+            hg[2 * (k * n_ports + q) + 1] = gamma[2 * (k * n_ports + q) + 1];
+        }
+    OpArgs op64;
     int rc = EMFEM_OK;
 #define STRY(x) do { rc = (x); if (rc != EMFEM_OK) goto done; } while (0)
+    STRY(check_cuda(cudaEventRecord(ev, h->stream), "event"));
+    STRY(check_cuda(cudaStreamWaitEvent(s, ev, 0), "wait"));
     STRY(check_cuda(cudaMemcpyAsync(k0dev, hk0.data(), sizeof(double) * S, cudaMemcpyHostToDevice, s), "copy k0"));
     STRY(check_cuda(cudaMemcpyAsync(gdev, hg.data(), sizeof(double) * hg.size(), cudaMemcpyHostToDevice, s), "copy gamma"));
     STRY(check_cuda(cudaMemsetAsync(pmap, 0xff, sizeof(int) * n, s), "memset"));
@@ -749,150 +934,137 @@ int emfem_cocg_solve(emfem_handle hd, int64_t n, int64_t nnz, const int32_t* ind
         patch_map_kernel<<<grid_for(n_patch_rows, VB), VB, 0, s>>>(n_patch_rows, patch_rows, pmap);
         STRY(check_cuda(cudaGetLastError(), "patch_map_kernel"));
     }
-    {
-        long long nS = n * (long long)S;
-        unsigned gv = grid_for(nS, VB);
-        pad_copy_kernel<<<gv, VB, 0, s>>>(n, nsys, S, (const double2*)rhs, b64);
-        pad_copy_kernel<<<gv, VB, 0, s>>>(n, nsys, S, (const double2*)x, x64);
-        mask_vec_kernel<<<gv, VB, 0, s>>>(n, S, free_mask, b64);
-        mask_vec_kernel<<<gv, VB, 0, s>>>(n, S, free_mask, x64);
-        STRY(check_cuda(cudaGetLastError(), "setup copies"));
+    pad_copy_kernel<<<gv, VB, 0, s>>>(n, nsys, S, (const double2*)rhs, b64);
+    pad_copy_kernel<<<gv, VB, 0, s>>>(n, nsys, S, (const double2*)x, x64);
+    mask_vec_kernel<<<gv, VB, 0, s>>>(n, S, free_mask, b64);
+    mask_vec_kernel<<<gv, VB, 0, s>>>(n, S, free_mask, x64);
+    STRY(check_cuda(cudaGetLastError(), "setup copies"));
+    build_op(op64, n, S, indptr, indices, E_vals, B_vals, k0dev, n_patch_rows ? pmap : nullptr, patch_rowptr,
+             patch_cols, patch_vals, patch_port, n_ports, gdev, free_mask);
+    // initial residual r64 = b - A x0 and the outer state (||b||, tolerance, active)
+    spmv_kernel<double><<<gv, VB, 0, s>>>(op64, x64, Ax, nullptr, DOT_NONE, nullptr);
+    residual_kernel<<<gv, VB, 0, s>>>(n, S, free_mask, b64, Ax, r64, partial);
+    reduce_update_kernel<<<S, VB, 0, s>>>(partial, (int)gv, S, 2, st_outer, UPD_INIT, maxit, tol, nsys);
+    STRY(check_cuda(cudaGetLastError(), "initial residual"));
 
-        OpArgs op64;
-        build_op(op64, n, S, indptr, indices, E_vals, B_vals, k0dev, n_patch_rows ? pmap : nullptr, patch_rowptr,
-                 patch_cols, patch_vals, patch_port, n_ports, gdev, free_mask);
-        long long nb_rows = grid_for(nS, VB);
-        long long nb_pairs = grid_for((n / 2) * (long long)S, VB);
-        // initial residual r64 = b - A x0, norms
-        spmv_kernel<double><<<(unsigned)nb_rows, VB, 0, s>>>(op64, x64, Ax, nullptr);
-        residual_kernel<<<(unsigned)nb_rows, VB, 0, s>>>(n, S, free_mask, b64, Ax, r64, partial, nb_rows);
-        reduce_partials_kernel<<<S, VB, 0, s>>>(partial, (int)nb_rows, S, red, 2);
-        init_state_kernel<<<1, 64, 0, s>>>(st_outer, red, S, nsys, tol, 1);
-        STRY(check_cuda(cudaGetLastError(), "initial residual"));
-
-        if (precision == 0) {
-            Cocg<double> c;
-            c.op = op64; c.n = n; c.h = n / 2; c.S = S; c.precond = precond; c.maxit = maxit;
-            c.x = x64; c.r = (double2*)(ws + L.off_r); c.z = (double2*)(ws + L.off_z); c.p = (double2*)(ws + L.off_p);
-            c.q = (double2*)(ws + L.off_q); c.minv = (double2*)(ws + L.off_minv);
-            c.partial = partial; c.red = red; c.st = st; c.nb_rows = nb_rows; c.nb_pairs = nb_pairs; c.s = s;
-            if (precond) {
-                precond_setup_kernel<double><<<grid_for((n / 2) * (long long)S, VB), VB, 0, s>>>(op64, precond, c.minv);
-                STRY(check_cuda(cudaGetLastError(), "precond_setup"));
-            }
-            STRY(check_cuda(cudaMemcpyAsync(c.r, r64, sizeof(double2) * nS, cudaMemcpyDeviceToDevice, s), "copy r"));
-            STRY(check_cuda(cudaMemcpyAsync(st, st_outer, sizeof(SysState) * S, cudaMemcpyDeviceToDevice, s), "copy st"));
-            STRY(c.start());
-            STRY(c.run(16));
-        } else {
-            // FP32 operator copies
-            float2* E32 = (float2*)(ws + L.off_E32);
-            float2* B32 = (float2*)(ws + L.off_B32);
-            float2* P32 = (float2*)(ws + L.off_P32);
-            cast_values_kernel<<<grid_for(nnz, VB), VB, 0, s>>>(nnz, (const double2*)E_vals, E32);
-            if (B_vals) cast_values_kernel<<<grid_for(nnz, VB), VB, 0, s>>>(nnz, (const double2*)B_vals, B32);
-            if (npatch > 0) cast_values_kernel<<<grid_for(npatch, VB), VB, 0, s>>>(npatch, (const double2*)patch_vals, P32);
-            STRY(check_cuda(cudaGetLastError(), "cast values"));
-            OpArgs op32 = op64;
-            op32.E = E32; op32.B = B_vals ? B32 : nullptr; op32.patch_vals = P32;
-            Cocg<float> c;
-            c.op = op32; c.n = n; c.h = n / 2; c.S = S; c.precond = precond;
-            c.r = (float2*)(ws + L.off_r); c.z = (float2*)(ws + L.off_z); c.p = (float2*)(ws + L.off_p);
-            c.q = (float2*)(ws + L.off_q); c.minv = (float2*)(ws + L.off_minv);
-            c.x = (float2*)(ws + L.off_Ax);  // reuse: d (FP32) lives in the Ax buffer's first half
-            c.partial = partial; c.red = red; c.st = st; c.nb_rows = nb_rows; c.nb_pairs = nb_pairs; c.s = s;
-            if (precond) {
-                precond_setup_kernel<float><<<grid_for((n / 2) * (long long)S, VB), VB, 0, s>>>(op64, precond, c.minv);
-                STRY(check_cuda(cudaGetLastError(), "precond_setup"));
-            }
-            float2* d32 = (float2*)(ws + L.off_Ax);
-            std::vector<SysState> ho(S);
-            int total_inner = 0;
-            std::vector<int> inner_iters(S, 0);
-            const int max_outer = 40;
-            for (int outer = 0; outer < max_outer; outer++) {
-                STRY(check_cuda(cudaMemcpyAsync(ho.data(), st_outer, sizeof(SysState) * S, cudaMemcpyDeviceToHost, s), "copy"));
-                STRY(check_cuda(cudaStreamSynchronize(s), "sync"));
-                std::vector<int> act(S, 0);
-                bool any = false;
-                for (int k = 0; k < S; k++) { act[k] = ho[k].active; any |= act[k] != 0; }
-                if (!any || total_inner >= maxit) break;
-                STRY(check_cuda(cudaMemcpyAsync(oactive, act.data(), sizeof(int) * S, cudaMemcpyHostToDevice, s), "copy"));
-                // inner: A d = r64 / ||r64|| in FP32 to a relative 1e-4 (bounded by remaining budget)
-                to_f32_scaled_kernel<<<gv, VB, 0, s>>>(n, S, r64, st_outer, c.r, scale);
-                STRY(check_cuda(cudaMemsetAsync(d32, 0, sizeof(float2) * nS, s), "memset d"));
-                std::vector<SysState> hin(S);
-                for (int k = 0; k < S; k++) {
-                    SysState q;
-                    memset(&q, 0, sizeof(q));
-                    q.bn2 = act[k] ? 1.0 : 0.0;
-                    q.rn2 = q.bn2;
-                    q.tol2 = 1e-8;  // inner relative tolerance 1e-4
-                    q.active = act[k];
-                    hin[k] = q;
-                }
-                STRY(check_cuda(cudaMemcpyAsync(st, hin.data(), sizeof(SysState) * S, cudaMemcpyHostToDevice, s), "copy"));
-                c.maxit = std::max(1, maxit - total_inner);
-                STRY(c.start());
-                STRY(c.run(16));
-                STRY(check_cuda(cudaMemcpyAsync(hin.data(), st, sizeof(SysState) * S, cudaMemcpyDeviceToHost, s), "copy"));
-                STRY(check_cuda(cudaStreamSynchronize(s), "sync"));
-                int mx = 0;
-                for (int k = 0; k < S; k++) { inner_iters[k] += act[k] ? hin[k].iters : 0; mx = std::max(mx, act[k] ? hin[k].iters : 0); }
-                total_inner += std::max(mx, 1);
-                add_scaled_f32_kernel<<<gv, VB, 0, s>>>(n, S, d32, scale, oactive, x64);
-                // new FP64 residual
-                spmv_kernel<double><<<(unsigned)nb_rows, VB, 0, s>>>(op64, x64, Ax, nullptr);
-                residual_kernel<<<(unsigned)nb_rows, VB, 0, s>>>(n, S, free_mask, b64, Ax, r64, partial, nb_rows);
-                reduce_partials_kernel<<<S, VB, 0, s>>>(partial, (int)nb_rows, S, red, 2);
-                // refresh outer state: keep bn2/tol2, update rn2 and active
-                STRY(check_cuda(cudaGetLastError(), "refinement"));
-                std::vector<double2> hred(2 * S);
-                STRY(check_cuda(cudaMemcpyAsync(hred.data(), red, sizeof(double2) * 2 * S, cudaMemcpyDeviceToHost, s), "copy"));
-                STRY(check_cuda(cudaStreamSynchronize(s), "sync"));
-                for (int k = 0; k < S; k++) {
-                    ho[k].rn2 = hred[S + k].x;
-                    ho[k].iters = inner_iters[k];
-                    if (ho[k].active) {
-                        if (ho[k].rn2 <= ho[k].tol2) { ho[k].active = 0; ho[k].status = 0; }
-                        else if (!std::isfinite(ho[k].rn2) || hin[k].status == 2) { ho[k].active = 0; ho[k].status = 2; }
-                    }
-                }
-                STRY(check_cuda(cudaMemcpyAsync(st_outer, ho.data(), sizeof(SysState) * S, cudaMemcpyHostToDevice, s), "copy"));
-            }
+    if (precision == 0) {
+        Krylov<double> k;
+        k.method = method; k.op = op64; k.n = n; k.h = n / 2; k.S = S; k.precond = precond; k.maxit = maxit; k.nsys = nsys;
+        k.x = x64; k.r = (double2*)(ws + L.off_r64); k.minv = (double2*)(ws + L.off_minv);
+        for (int q = 0; q < 7; q++) k.v[q] = (double2*)(ws + L.off_v[q]);
+        k.partial = partial; k.st = st; k.s = s;
+        if (precond) {
+            precond_setup_kernel<double><<<grid_for((n / 2) * (long long)S, VB), VB, 0, s>>>(op64, precond, k.minv);
+            STRY(check_cuda(cudaGetLastError(), "precond_setup"));
+        }
+        // the recurrence tolerance is half the requested one so the FP64 true residual meets it
+        reduce_update_kernel<<<S, VB, 0, s>>>(partial, (int)gv, S, 2, st, UPD_INIT, maxit, 0.5 * tol, nsys);
+        STRY(check_cuda(cudaGetLastError(), "init state"));
+        STRY(k.start());
+        STRY(k.run(16));
+    } else {
+        float2* E32 = (float2*)(ws + L.off_E32);
+        float2* B32 = (float2*)(ws + L.off_B32);
+        float2* P32 = (float2*)(ws + L.off_P32);
+        cast_values_kernel<<<grid_for(nnz, VB), VB, 0, s>>>(nnz, (const double2*)E_vals, E32);
+        if (B_vals) cast_values_kernel<<<grid_for(nnz, VB), VB, 0, s>>>(nnz, (const double2*)B_vals, B32);
+        if (npatch > 0) cast_values_kernel<<<grid_for(npatch, VB), VB, 0, s>>>(npatch, (const double2*)patch_vals, P32);
+        STRY(check_cuda(cudaGetLastError(), "cast values"));
+        OpArgs op32 = op64;
+        op32.E = E32; op32.B = B_vals ? B32 : nullptr; op32.patch_vals = P32;
+        Krylov<float> k;
+        k.method = method; k.op = op32; k.n = n; k.h = n / 2; k.S = S; k.precond = precond; k.nsys = nsys;
+        float2* r32 = (float2*)(ws + L.off_v[6]);
+        float2* d32 = (float2*)(ws + L.off_v[7]);
+        k.x = d32; k.r = r32; k.minv = (float2*)(ws + L.off_minv);
+        for (int q = 0; q < 6; q++) k.v[q] = (float2*)(ws + L.off_v[q]);
+        k.partial = partial; k.st = st; k.s = s;
+        if (precond) {
+            precond_setup_kernel<float><<<grid_for((n / 2) * (long long)S, VB), VB, 0, s>>>(op64, precond, k.minv);
+            STRY(check_cuda(cudaGetLastError(), "precond_setup"));
+        }
+        std::vector<SysState> ho(S);
+        int used = 0;
+        for (int outer = 0; outer < 60; outer++) {
             STRY(check_cuda(cudaMemcpyAsync(ho.data(), st_outer, sizeof(SysState) * S, cudaMemcpyDeviceToHost, s), "copy"));
             STRY(check_cuda(cudaStreamSynchronize(s), "sync"));
-            for (int k = 0; k < S; k++) {
-                if (ho[k].active) { ho[k].active = 0; ho[k].status = 1; }
-                ho[k].iters = inner_iters[k];
+            bool any = false;
+            for (int q = 0; q < S; q++) any |= ho[q].active != 0;
+            if (!any || used >= maxit) break;
+            to_f32_scaled_kernel<<<gv, VB, 0, s>>>(n, S, r64, st_outer, r32, scale);
+            STRY(check_cuda(cudaMemsetAsync(d32, 0, sizeof(float2) * nS, s), "memset d"));
+            inner_init_kernel<<<1, 64, 0, s>>>(st, st_outer, S, 1e-4);
+            k.maxit = std::max(1, maxit - used);
+            STRY(k.start());
+            STRY(k.run(16));
+            std::vector<SysState> hin(S);
+            STRY(check_cuda(cudaMemcpyAsync(hin.data(), st, sizeof(SysState) * S, cudaMemcpyDeviceToHost, s), "copy"));
+            STRY(check_cuda(cudaStreamSynchronize(s), "sync"));
+            int mx = 1;
+            for (int q = 0; q < S; q++) if (ho[q].active) mx = std::max(mx, hin[q].iters);
+            used += mx;
+            add_scaled_f32_kernel<<<gv, VB, 0, s>>>(n, S, d32, scale, st_outer, x64);
+            spmv_kernel<double><<<gv, VB, 0, s>>>(op64, x64, Ax, nullptr, DOT_NONE, nullptr);
+            residual_kernel<<<gv, VB, 0, s>>>(n, S, free_mask, b64, Ax, r64, partial);
+            // the inner state array is free now: reuse it to reduce ||b||^2, ||r||^2 of the new residual
+            reduce_update_kernel<<<S, VB, 0, s>>>(partial, (int)gv, S, 2, st, UPD_INIT, maxit, 1.0, S);
+            STRY(check_cuda(cudaGetLastError(), "refinement"));
+            std::vector<SysState> hr(S);
+            STRY(check_cuda(cudaMemcpyAsync(hr.data(), st, sizeof(SysState) * S, cudaMemcpyDeviceToHost, s), "copy"));
+            STRY(check_cuda(cudaStreamSynchronize(s), "sync"));
+            // a correction that did not lower the FP64 residual is reverted and the system stops
+            std::vector<double> rev(S, 0.0);
+            bool any_rev = false;
+            for (int q = 0; q < S; q++) {
+                if (!ho[q].active) continue;
+                ho[q].iters += hin[q].iters;
+                double prev = ho[q].rn2;
+                if (!std::isfinite(hr[q].rn2) || hr[q].rn2 >= prev) {
+                    rev[q] = -std::sqrt(prev);
+                    any_rev = true;
+                    ho[q].active = 0; ho[q].status = 2;
+                    continue;
+                }
+                ho[q].rn2 = hr[q].rn2;
+                if (ho[q].rn2 <= ho[q].tol2) { ho[q].active = 0; ho[q].status = 0; }
+                else if (ho[q].rn2 >= 0.98 * prev) { ho[q].active = 0; ho[q].status = 2; }
             }
-            STRY(check_cuda(cudaMemcpyAsync(st, ho.data(), sizeof(SysState) * S, cudaMemcpyHostToDevice, s), "copy"));
+            if (any_rev) {
+                STRY(check_cuda(cudaMemcpyAsync(scale, rev.data(), sizeof(double) * S, cudaMemcpyHostToDevice, s), "copy"));
+                add_scaled_f32_kernel<<<gv, VB, 0, s>>>(n, S, d32, scale, st_outer, x64);
+                STRY(check_cuda(cudaGetLastError(), "revert"));
+            }
+            STRY(check_cuda(cudaMemcpyAsync(st_outer, ho.data(), sizeof(SysState) * S, cudaMemcpyHostToDevice, s), "copy"));
         }
-        // final FP64 true residual
-        spmv_kernel<double><<<(unsigned)nb_rows, VB, 0, s>>>(op64, x64, Ax, nullptr);
-        residual_kernel<<<(unsigned)nb_rows, VB, 0, s>>>(n, S, free_mask, b64, Ax, r64, partial, nb_rows);
-        reduce_partials_kernel<<<S, VB, 0, s>>>(partial, (int)nb_rows, S, red, 2);
+        STRY(check_cuda(cudaMemcpyAsync(ho.data(), st_outer, sizeof(SysState) * S, cudaMemcpyDeviceToHost, s), "copy"));
+        STRY(check_cuda(cudaStreamSynchronize(s), "sync"));
+        for (int q = 0; q < S; q++) if (ho[q].active) { ho[q].active = 0; ho[q].status = 1; }
+        STRY(check_cuda(cudaMemcpyAsync(st, ho.data(), sizeof(SysState) * S, cudaMemcpyHostToDevice, s), "copy"));
+    }
+    {
+        // final FP64 true residual and solution copy-out
+        std::vector<SysState> hs(S);
+        STRY(check_cuda(cudaMemcpyAsync(hs.data(), st, sizeof(SysState) * S, cudaMemcpyDeviceToHost, s), "copy"));
+        spmv_kernel<double><<<gv, VB, 0, s>>>(op64, x64, Ax, nullptr, DOT_NONE, nullptr);
+        residual_kernel<<<gv, VB, 0, s>>>(n, S, free_mask, b64, Ax, r64, partial);
+        reduce_update_kernel<<<S, VB, 0, s>>>(partial, (int)gv, S, 2, st_outer, UPD_INIT, maxit, tol, S);
         unpad_copy_kernel<<<grid_for(n * (long long)nsys, VB), VB, 0, s>>>(n, nsys, S, x64, (double2*)x);
         STRY(check_cuda(cudaGetLastError(), "final residual"));
-        std::vector<SysState> hs(S);
-        std::vector<double2> hred(2 * S);
-        STRY(check_cuda(cudaMemcpyAsync(hs.data(), st, sizeof(SysState) * S, cudaMemcpyDeviceToHost, s), "copy"));
-        STRY(check_cuda(cudaMemcpyAsync(hred.data(), red, sizeof(double2) * 2 * S, cudaMemcpyDeviceToHost, s), "copy"));
+        std::vector<SysState> hf(S);
+        STRY(check_cuda(cudaMemcpyAsync(hf.data(), st_outer, sizeof(SysState) * S, cudaMemcpyDeviceToHost, s), "copy"));
         STRY(check_cuda(cudaStreamSynchronize(s), "sync"));
         bool all_ok = true;
-        for (int k = 0; k < nsys; k++) {
-            double bn = hred[k].x, rn = hred[S + k].x;
-            double rel = bn > 0 ? std::sqrt(rn / bn) : 0.0;
-            int stat = hs[k].status;
-            if (hs[k].active) stat = 1;
-            if (stat == 0 && rel > tol * 10) stat = 1;  // recurrence drifted from the true residual
-            if (status) status[k] = stat;
-            if (iters) iters[k] = hs[k].iters;
-            if (relres) relres[k] = rel;
+        for (int q = 0; q < nsys; q++) {
+            double rel = hf[q].bn2 > 0 ? std::sqrt(hf[q].rn2 / hf[q].bn2) : 0.0;
+            int stat = hs[q].active ? 1 : hs[q].status;
+            if (stat == 0 && rel > tol) stat = 1;  // the recurrence drifted from the true residual
+            if (status) status[q] = stat;
+            if (iters) iters[q] = hs[q].iters;
+            if (relres) relres[q] = rel;
             all_ok &= stat == 0;
         }
         if (!all_ok) {
-            set_error("emfem_cocg_solve: not every system reached the tolerance");
+            set_error("emfem_krylov_solve: not every system reached the tolerance");
             rc = EMFEM_ERR_NOT_CONVERGED;
         }
     }

@@ -19,7 +19,7 @@ import torch
 from scipy.sparse import csr_matrix
 
 from ._lib import Handle, check, lib, ptr, ERR_NOT_CONVERGED
-from .sweep import PRECISION, PRECOND
+from .sweep import METHOD, PRECISION, PRECOND
 
 
 @dataclass
@@ -89,7 +89,11 @@ class Solver:
 
 
 class SolverB200COCG(Solver):
-    """Device COCG for the complex-symmetric FEM systems, block-Jacobi on DOF pairs (i, i+n/2).
+    """Device Krylov solver (BiCGStab by default, COCG on request), block Jacobi on DOF pairs (i, i+n/2).
+
+    The reference's K is not complex-symmetric (its face-face mass block is asymmetric,
+    ``ASM/curlcurl.py:348-357``), so BiCGStab is the default; ``method="cocg"`` is exact only for
+    symmetric operators.
 
     ``solve(A, b)`` takes the already reduced system (SciPy CSR/CSC, complex) exactly as
     ``SolveRoutine.solve`` hands it to a solver.  ``reuse_factorization=True`` keeps the uploaded
@@ -102,16 +106,17 @@ class SolverB200COCG(Solver):
     released_gil = True
 
     def __init__(self, pre: str = "", tol: float = 1e-10, maxit: int = 50000, precond: str = "block_jacobi",
-                 precision: str = "fp64", device=None, raise_on_fail: bool = False):
+                 precision: str = "fp64", device=None, raise_on_fail: bool = False, method: str = "bicgstab"):
         super().__init__(pre)
         self.tol, self.maxit, self.precond, self.precision = tol, maxit, precond, precision
+        self.method = method
         self.device = device
         self.raise_on_fail = raise_on_fail
         self._cache = None
 
     def duplicate(self) -> "SolverB200COCG":
         return SolverB200COCG(self.pre, self.tol, self.maxit, self.precond, self.precision, self.device,
-                              self.raise_on_fail)
+                              self.raise_on_fail, self.method)
 
     def reset(self) -> None:
         self._cache = None
@@ -149,17 +154,17 @@ class SolverB200COCG(Solver):
             x = torch.zeros_like(rhs)
             prec = PRECISION[self.precision]
             sz = ctypes.c_size_t()
-            check(lib().emfem_cocg_workspace_size(n, c["nnz"], ns, prec, ctypes.byref(sz)), "emfem_cocg_workspace_size")
+            check(lib().emfem_krylov_workspace_size(n, c["nnz"], ns, prec, ctypes.byref(sz)), "emfem_krylov_workspace_size")
             ws = torch.empty(sz.value, dtype=torch.uint8, device=dev)
             status = (ctypes.c_int * ns)(); iters = (ctypes.c_int * ns)(); relres = (ctypes.c_double * ns)()
             k0 = (ctypes.c_double * ns)(*([0.0] * ns))
             h = Handle.get(dev)
-            st = lib().emfem_cocg_solve(h.h, n, c["nnz"], ptr(c["indptr"]), ptr(c["indices"]), ptr(c["vals"]), None,
+            st = lib().emfem_krylov_solve(h.h, METHOD[self.method], n, c["nnz"], ptr(c["indptr"]), ptr(c["indices"]), ptr(c["vals"]), None,
                                         ns, k0, 0, None, None, None, None, None, 0, None, ptr(c["mask"]),
                                         ptr(rhs), ptr(x), self.tol, self.maxit, PRECOND[self.precond], prec,
                                         ptr(ws), ws.numel(), status, iters, relres)
             if st not in (0, ERR_NOT_CONVERGED):
-                check(st, "emfem_cocg_solve")
+                check(st, "emfem_krylov_solve")
             out[:, c0:c0 + ns] = x.cpu().numpy()
             reports.extend(zip(status[:], iters[:], relres[:]))
         simtime = time.perf_counter() - t0
@@ -169,7 +174,7 @@ class SolverB200COCG(Solver):
         rep = SolveReport(solver=str(self), exit_code=0 if ok else 1, simtime=simtime, precon=self.precond,
                           aux={"iterations": str([r[1] for r in reports]),
                                "true relative residual": str([f"{r[2]:.3e}" for r in reports]),
-                               "precision": self.precision, "tolerance": str(self.tol)})
+                               "precision": self.precision, "tolerance": str(self.tol), "method": self.method})
         return (out if multi else out[:, 0]), rep
 
 

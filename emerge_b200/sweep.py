@@ -1,4 +1,4 @@
-"""Device-resident frequency sweep: assembly once, then batched COCG solves of
+"""Device-resident frequency sweep: assembly once, then batched Krylov solves of
 K_f = E − k0_f²·B + Σ_p γ_p(k0_f)·R̂_p with port excitations b_{f,p} = s_p(k0_f)·b̂_p.
 
 This is the GPU counterpart of ``Microwave3D.run_sweep`` → ``Assembler.assemble_freq_matrix`` →
@@ -30,6 +30,7 @@ from .ports import k0_of
 
 PRECOND = {"none": 0, "jacobi": 1, "block_jacobi": 2}
 PRECISION = {"fp64": 0, "mixed": 1}
+METHOD = {"cocg": 0, "bicgstab": 1}
 
 
 def _seg_from_keys(keys: np.ndarray):
@@ -150,15 +151,16 @@ class FrequencySweep:
 
     def workspace(self, nsys: int, precision: int) -> torch.Tensor:
         sz = ctypes.c_size_t()
-        check(lib().emfem_cocg_workspace_size(self.n, self.plan.nnz, nsys, precision, ctypes.byref(sz)),
-              "emfem_cocg_workspace_size")
+        check(lib().emfem_krylov_workspace_size(self.n, self.plan.nnz, nsys, precision, ctypes.byref(sz)),
+              "emfem_krylov_workspace_size")
         if self._ws is None or self._ws.numel() < sz.value:
             self._ws = torch.empty(sz.value, dtype=torch.uint8, device=self.device)
         return self._ws
 
     def solve(self, systems, tol: float = 1e-8, maxit: int = 20000, precond: str = "block_jacobi",
-              precision: str = "fp64", x0: torch.Tensor | None = None, raise_on_fail: bool = False) -> SolveResult:
-        """Solve the listed (frequency, port index) systems in one batched COCG call (<= 64)."""
+              precision: str = "fp64", method: str = "bicgstab", x0: torch.Tensor | None = None,
+              raise_on_fail: bool = False) -> SolveResult:
+        """Solve the listed (frequency, port index) systems in one batched Krylov call (<= 64)."""
         nsys = len(systems)
         assert 1 <= nsys <= 64
         freqs = [f for f, _ in systems]
@@ -176,7 +178,7 @@ class FrequencySweep:
         ga = (ctypes.c_double * len(gam))(*gam)
         h = Handle.get(self.device)
         t0 = time.perf_counter()
-        st = lib().emfem_cocg_solve(h.h, self.n, self.plan.nnz, ptr(self.plan.indptr), ptr(self.plan.indices),
+        st = lib().emfem_krylov_solve(h.h, METHOD[method], self.n, self.plan.nnz, ptr(self.plan.indptr), ptr(self.plan.indices),
                                     ptr(self.E), ptr(self.B), nsys, k0a,
                                     self.patch_rows.numel(), ptr(self.patch_rows), ptr(self.patch_rowptr),
                                     ptr(self.patch_cols), ptr(self.patch_vals), ptr(self.patch_port), self.n_ports, ga,
@@ -184,7 +186,7 @@ class FrequencySweep:
                                     ptr(ws), ws.numel(), status, iters, relres)
         dt = time.perf_counter() - t0
         if st not in (0, ERR_NOT_CONVERGED) or (raise_on_fail and st != 0):
-            check(st, "emfem_cocg_solve")
+            check(st, "emfem_krylov_solve")
         return SolveResult(x, np.array(status[:]), np.array(iters[:]), np.array(relres[:]), list(systems), dt)
 
     def apply(self, systems, x: torch.Tensor) -> torch.Tensor:

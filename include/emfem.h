@@ -121,34 +121,38 @@ int emfem_sweep_combine(emfem_handle h, int64_t nnz, const void *E_vals, const v
                         int64_t n_patch, const int32_t *patch_slot, const void *patch_vals,
                         double gamma_re, double gamma_im, void *K_vals);
 
-/* ---- batched COCG solver ---------------------------------------------------------------------
- * Solves nsys complex-symmetric systems A_s x_s = b_s on one CSR pattern, replacing the
- * per-frequency direct solve (SolverSuperLU, src/emerge/_emerge/solver.py:535-572, reached through
- * SolveRoutine.solve :1241-1326).  A_s = E - k0sq[s] * B + sum_p gamma[s, p] * R_p, where B may be
- * NULL (then A_s = E + ...), and the Robin terms R_p are given as a small row-compressed "patch"
- * (patch_rowptr over patch_rows, patch_cols, patch_vals, patch_port).  Rows/columns where
- * free_mask == 0 are eliminated exactly as SolveRoutine's submatrix A[ids, ids] (solution zero).
- * Vectors are (n, nsys) c128, DOF-major (entry (i, s) at i * nsys + s).  x is the initial guess on
- * entry (zero for the reference's behaviour) and the solution on exit.
- *   precond: 0 none, 1 point Jacobi, 2 block Jacobi on DOF pairs (i, i + n/2) — the first- and
- *            second-kind DOFs of one edge/face (elements/nedelec2.py:42-58).
- *   precision: 0 = FP64 COCG; 1 = FP32 inner COCG inside FP64 iterative refinement (FP64 true
- *            residual and solution update).
- * Host outputs per system: status (0 converged, 1 iteration cap, 2 breakdown), iters, relres
- * (FP64 true relative residual ||b - A x|| / ||b||).  workspace (device) must hold
- * emfem_cocg_workspace_size() bytes.  Synchronises the stream. */
-int emfem_cocg_workspace_size(int64_t n, int64_t nnz, int nsys, int precision, size_t *bytes);
-int emfem_cocg_solve(emfem_handle h, int64_t n, int64_t nnz, const int32_t *indptr, const int32_t *indices,
-                     const void *E_vals, const void *B_vals, int nsys, const double *k0sq,
-                     int64_t n_patch_rows, const int32_t *patch_rows, const int32_t *patch_rowptr,
-                     const int32_t *patch_cols, const void *patch_vals, const int32_t *patch_port,
-                     int n_ports, const double *gamma,
-                     const uint8_t *free_mask, const void *rhs, void *x,
-                     double tol, int maxit, int precond, int precision,
-                     void *workspace, size_t workspace_bytes,
-                     int *status, int *iters, double *relres);
+/* ---- batched Krylov solver ------------------------------------------------------------------
+ * Solves nsys systems A_s x_s = b_s on one CSR pattern, replacing the per-frequency direct solve
+ * (SolverSuperLU, src/emerge/_emerge/solver.py:535-572, reached through SolveRoutine.solve
+ * :1241-1326).  A_s = E - k0sq[s] * B + sum_p gamma[s, p] * R_p, where B may be NULL (then
+ * A_s = E + ...), and the Robin terms R_p are given as a small row-compressed "patch"
+ * (patch_rows, patch_rowptr (n_patch_rows + 1), patch_cols, patch_vals, patch_port).  Rows and
+ * columns where free_mask == 0 are eliminated exactly as SolveRoutine's submatrix A[ids, ids]
+ * (their solution entries are zero).  Vectors are (n, nsys) c128, DOF-major (entry (i, s) at
+ * i * nsys + s).  x holds the initial guess on entry (zero for the reference's behaviour) and the
+ * solution on exit.  k0sq (nsys) and gamma (nsys * n_ports complex) are host arrays.
+ *   method:    0 = COCG (complex-symmetric A only), 1 = right-preconditioned BiCGStab (general A;
+ *              the reference's mass matrix is not symmetric, so this is the default).
+ *   precond:   0 none, 1 point Jacobi, 2 block Jacobi on DOF pairs (i, i + n/2) — the first- and
+ *              second-kind DOFs of one edge/face (elements/nedelec2.py:42-58).
+ *   precision: 0 = FP64 Krylov; 1 = FP32 inner Krylov inside FP64 iterative refinement (FP64
+ *              residual, solution update and convergence test).
+ * Host outputs per system: status (0 converged, 1 iteration cap, 2 breakdown/stagnation), iters,
+ * relres (FP64 true relative residual ||b - A x|| / ||b|| over free DOFs).  workspace (device)
+ * must hold emfem_krylov_workspace_size() bytes.  Synchronises the stream.  Returns
+ * EMFEM_ERR_NOT_CONVERGED when any system missed the tolerance (outputs still filled). */
+int emfem_krylov_workspace_size(int64_t n, int64_t nnz, int nsys, int precision, size_t *bytes);
+int emfem_krylov_solve(emfem_handle h, int method, int64_t n, int64_t nnz, const int32_t *indptr,
+                       const int32_t *indices, const void *E_vals, const void *B_vals, int nsys,
+                       const double *k0sq, int64_t n_patch_rows, const int32_t *patch_rows,
+                       const int32_t *patch_rowptr, const int32_t *patch_cols, const void *patch_vals,
+                       const int32_t *patch_port, int n_ports, const double *gamma,
+                       const uint8_t *free_mask, const void *rhs, void *x, double tol, int maxit,
+                       int precond, int precision, void *workspace, size_t workspace_bytes,
+                       int *status, int *iters, double *relres);
 
-/* y_s = A_s x_s for the operator of emfem_cocg_solve (FP64), with eliminated rows/cols as there. */
+/* y_s = A_s x_s for the operator of emfem_krylov_solve (FP64), eliminated rows/cols as there;
+ * nsys a power of two <= 256; k0sq_dev and gamma_dev are device arrays. */
 int emfem_sweep_spmv(emfem_handle h, int64_t n, const int32_t *indptr, const int32_t *indices,
                      const void *E_vals, const void *B_vals, int nsys, const double *k0sq_dev,
                      int64_t n_patch_rows, const int32_t *patch_rows, const int32_t *patch_rowptr,

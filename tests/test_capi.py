@@ -32,5 +32,5 @@ def test_host_only_calls():
     buf = ctypes.create_string_buffer(64)
     assert L.emfem_last_error(buf, 64) == 0
     sz = ctypes.c_size_t()
-    assert L.emfem_cocg_workspace_size(1000, 20000, 3, 0, ctypes.byref(sz)) == 0 and sz.value > 0
-    assert L.emfem_cocg_workspace_size(1000, 20000, 65, 0, ctypes.byref(sz)) == _lib.ERR_INVALID_ARG
+    assert L.emfem_krylov_workspace_size(1000, 20000, 3, 0, ctypes.byref(sz)) == 0 and sz.value > 0
+    assert L.emfem_krylov_workspace_size(1000, 20000, 65, 0, ctypes.byref(sz)) == _lib.ERR_INVALID_ARG

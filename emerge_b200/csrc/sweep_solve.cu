@@ -1079,3 +1079,84 @@ done:
 }
 
 }  // extern "C"
+
+// ---- allocation-free variant of emfem_sweep_spmv ------------------------------------------------
+// Some callers cannot call cudaMalloc: applications that hand all device memory to their own pool
+// allocator up front (a raw cudaMalloc fails or fragments it), and latency-critical loops in which an
+// allocation's implicit device synchronisation is not acceptable.  This entry point computes exactly
+// what emfem_sweep_spmv computes, but keeps its only scratch — the row -> Robin-patch-row map, one int
+// per row — in the fixed array below instead of a stream-ordered allocation.  The array is part of
+// this library's device image: every GPU that loads the library holds its 16 MiB until the process
+// exits.  All calls share it and it keeps the last call's contents, so every call resets the rows it
+// uses before filling them, and calls that overlap on the GPU (different streams or threads) race.
+#include <mutex>
+
+namespace emfem {
+static __device__ __align__(256) int g_noalloc_patch_map[EMFEM_NOALLOC_MAX_ROWS];
+
+constexpr int NOALLOC_MAX_DEVICES = 64;
+static int* g_noalloc_addr[NOALLOC_MAX_DEVICES] = {nullptr};
+static std::mutex g_noalloc_mutex;
+
+// Device address of the static map on `device` (which must be current).  Resolved once per device
+// with cudaGetSymbolAddress: host code only holds a host-side stand-in for the symbol, which must
+// never be passed to a kernel.
+static int noalloc_scratch(int device, int** out) {
+    if (device < 0 || device >= NOALLOC_MAX_DEVICES) {
+        set_error("emfem_sweep_spmv_noalloc: device %d beyond the supported %d", device, NOALLOC_MAX_DEVICES);
+        return EMFEM_ERR_INVALID_ARG;
+    }
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    if (g_noalloc_addr[device] == nullptr) {
+        int* p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress((void**)&p, g_noalloc_patch_map);
+        if (e != cudaSuccess) {
+            set_error("emfem_sweep_spmv_noalloc: cudaGetSymbolAddress: %s", cudaGetErrorString(e));
+            return EMFEM_ERR_CUDA;
+        }
+        g_noalloc_addr[device] = p;
+    }
+    *out = g_noalloc_addr[device];
+    return EMFEM_OK;
+}
+}  // namespace emfem
+
+extern "C" int emfem_sweep_spmv_noalloc(emfem_handle h, int64_t n, const int32_t* indptr, const int32_t* indices,
+                                        const void* E_vals, const void* B_vals, int nsys, const double* k0sq_dev,
+                                        int64_t n_patch_rows, const int32_t* patch_rows, const int32_t* patch_rowptr,
+                                        const int32_t* patch_cols, const void* patch_vals, const int32_t* patch_port,
+                                        int n_ports, const double* gamma_dev, const uint8_t* free_mask,
+                                        const void* x, void* y) {
+    EMFEM_REQUIRE(h && indptr && indices && E_vals && k0sq_dev && free_mask && x && y && n > 0,
+                  "emfem_sweep_spmv_noalloc: bad argument");
+    EMFEM_REQUIRE(n <= EMFEM_NOALLOC_MAX_ROWS,
+                  "emfem_sweep_spmv_noalloc: %lld rows exceed the fixed scratch of %d rows; use emfem_sweep_spmv",
+                  (long long)n, EMFEM_NOALLOC_MAX_ROWS);
+    EMFEM_REQUIRE(nsys >= 1 && nsys <= 256 && (nsys & (nsys - 1)) == 0,
+                  "emfem_sweep_spmv_noalloc: nsys must be a power of two <= 256");
+    EMFEM_REQUIRE(n_patch_rows == 0 || (patch_rows && patch_rowptr && patch_cols && patch_vals && patch_port && gamma_dev),
+                  "emfem_sweep_spmv_noalloc: patch arrays missing");
+    int prev = 0;
+    EMFEM_CUDA(cudaGetDevice(&prev));
+    if (prev != h->h.device) EMFEM_CUDA(cudaSetDevice(h->h.device));
+    int* pmap = nullptr;
+    int rc = EMFEM_OK;
+    if (n_patch_rows > 0) {
+        rc = noalloc_scratch(h->h.device, &pmap);
+        if (rc == EMFEM_OK) rc = check_cuda(cudaMemsetAsync(pmap, 0xff, sizeof(int) * n, h->h.stream), "cudaMemsetAsync");
+        if (rc == EMFEM_OK) {
+            patch_map_kernel<<<grid_for(n_patch_rows, VB), VB, 0, h->h.stream>>>(n_patch_rows, patch_rows, pmap);
+            rc = check_cuda(cudaGetLastError(), "patch_map_kernel");
+        }
+    }
+    if (rc == EMFEM_OK) {
+        OpArgs a;
+        build_op(a, n, nsys, indptr, indices, E_vals, B_vals, k0sq_dev, pmap, patch_rowptr, patch_cols, patch_vals,
+                 patch_port, n_ports, gamma_dev, free_mask);
+        spmv_kernel<double><<<grid_for(n * nsys, VB), VB, 0, h->h.stream>>>(a, (const double2*)x, (double2*)y, nullptr,
+                                                                              DOT_NONE, nullptr);
+        rc = check_cuda(cudaGetLastError(), "spmv_kernel");
+    }
+    if (prev != h->h.device) cudaSetDevice(prev);
+    return rc;
+}

@@ -160,6 +160,25 @@ int emfem_sweep_spmv(emfem_handle h, int64_t n, const int32_t *indptr, const int
                      int n_ports, const double *gamma_dev, const uint8_t *free_mask,
                      const void *x, void *y);
 
+/* ---- allocation-free sweep SpMV ------------------------------------------------------------
+ * No counterpart in the reference.  The same y_s = A_s x_s as emfem_sweep_spmv, for callers that
+ * cannot call cudaMalloc: applications whose device memory is owned up front by their own pool
+ * allocator, and latency-critical loops that cannot afford an allocation's implicit device
+ * synchronisation.  Its only scratch (one int per row: the row -> Robin-patch-row map) lives in a
+ * fixed device array of EMFEM_NOALLOC_MAX_ROWS ints (16 MiB) inside the library, held by every GPU
+ * that loads the library until the process exits; larger n is rejected with EMFEM_ERR_INVALID_ARG.
+ * It calls no cudaMalloc/cudaFree.  The first call on a device resolves the array's device address
+ * (cudaGetSymbolAddress) once; make that first call before any stream capture.  All calls share the
+ * array (each call resets the rows it uses), so calls that overlap on the GPU race.  Arguments as
+ * emfem_sweep_spmv. */
+#define EMFEM_NOALLOC_MAX_ROWS 4194304
+int emfem_sweep_spmv_noalloc(emfem_handle h, int64_t n, const int32_t *indptr, const int32_t *indices,
+                             const void *E_vals, const void *B_vals, int nsys, const double *k0sq_dev,
+                             int64_t n_patch_rows, const int32_t *patch_rows, const int32_t *patch_rowptr,
+                             const int32_t *patch_cols, const void *patch_vals, const int32_t *patch_port,
+                             int n_ports, const double *gamma_dev, const uint8_t *free_mask,
+                             const void *x, void *y);
+
 #ifdef __cplusplus
 }
 #endif

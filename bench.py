@@ -202,6 +202,7 @@ def main():
     ap.add_argument("--sweep-maxit", type=int, default=3000)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--grid", type=int, default=40, help="cavity hex grid size (40 = the 384 000-tet workload)")
+    ap.add_argument("--variant", type=int, default=-1, help="assembly kernel variant (default: autotune)")
     args = ap.parse_args()
     ws, rank, local = dist_init(args.gpus)
     if args.impl == "reference":
@@ -232,6 +233,11 @@ def main():
     B = torch.empty(nnz, dtype=torch.complex128, device=dev)
     stream = torch.cuda.current_stream(dev)
 
+    if args.variant >= 0:
+        plan.set_variant(args.variant)
+        tuning = {"variant": args.variant, "ms": None}
+    else:
+        tuning = plan.tune(er, ur)
     for _ in range(args.warmup):
         plan.assemble(er, ur, E, B)
     torch.cuda.synchronize()
@@ -305,7 +311,7 @@ def main():
                     "api": "emerge_b200.assembly.tet_mass_stiffness_matrices (host numpy in, SciPy CSR out)"},
             "gpu_launches": 2 * args.steps,
             "clocks": clocks,
-            "plan_seconds": t_plan, "nnz": int(nnz),
+            "plan_seconds": t_plan, "nnz": int(nnz), "autotune": tuning,
             "sweep": sweep,
             "cpu_baseline": cb,
         }

@@ -15,6 +15,8 @@ Device-resident building blocks (torch tensors, used by the frequency sweep and 
 from __future__ import annotations
 
 import ctypes
+import json
+import os
 
 import numpy as np
 import torch
@@ -132,6 +134,63 @@ class CsrPlan:
         check(lib().emfem_plan_assemble(self._p, d.n_nodes, d.n_edges, ptr(d.nodes), ptr(d.tets), ptr(d.tet_to_edge),
                                         ptr(d.edge_lengths), ptr(ur), ptr(er), ptr(E), ptr(B)), "emfem_plan_assemble")
         return E, B
+
+    @property
+    def variant(self) -> int:
+        n, cur = ctypes.c_int(), ctypes.c_int()
+        check(lib().emfem_plan_variants(self._p, ctypes.byref(n), ctypes.byref(cur)), "emfem_plan_variants")
+        return cur.value
+
+    def set_variant(self, v: int) -> None:
+        check(lib().emfem_plan_set_variant(self._p, int(v)), "emfem_plan_set_variant")
+
+    def tune(self, er: torch.Tensor, ur: torch.Tensor, reps: int = 3, cache: str | None = None) -> dict:
+        """Autotune the assembly kernel variant (chunk capacity x CTA size) for this mesh on this GPU.
+
+        Times every available variant with CUDA events on the current stream (one warm-up launch,
+        then ``reps`` launches) and keeps the fastest.  Results are cached as JSON keyed by GPU name
+        and mesh size (``~/.cache/emerge_b200/autotune.json`` unless ``cache`` is given)."""
+        path = cache or os.path.join(os.path.expanduser("~"), ".cache", "emerge_b200", "autotune.json")
+        key = f"{torch.cuda.get_device_name(self.device)}|assemble|{self.dmesh.n_tets}|{self.nnz}"
+        try:
+            table = json.load(open(path))
+        except (OSError, ValueError):
+            table = {}
+        if key in table:
+            try:
+                self.set_variant(int(table[key]["variant"]))
+                return table[key]
+            except Exception:
+                pass
+        n = ctypes.c_int()
+        check(lib().emfem_plan_variants(self._p, ctypes.byref(n), None), "emfem_plan_variants")
+        E = torch.empty(self.nnz, dtype=torch.complex128, device=self.device)
+        B = torch.empty_like(E)
+        times = {}
+        stream = torch.cuda.current_stream(self.device)
+        for v in range(n.value):
+            try:
+                self.set_variant(v)
+            except Exception:
+                continue
+            self.assemble(er, ur, E, B)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(reps):
+                self.assemble(er, ur, E, B)
+            e1.record(stream)
+            e1.synchronize()
+            times[v] = e0.elapsed_time(e1) / reps
+        best = min(times, key=times.get)
+        self.set_variant(best)
+        entry = {"variant": best, "ms": times}
+        table[key] = entry
+        try:
+            os.makedirs(os.path.dirname(path), exist_ok=True)
+            json.dump(table, open(path, "w"), indent=1)
+        except OSError:
+            pass
+        return entry
 
     def find_slots(self, rows: torch.Tensor, cols: torch.Tensor) -> torch.Tensor:
         rows = rows.to(self.device, torch.int64).contiguous()

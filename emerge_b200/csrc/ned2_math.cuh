@@ -74,18 +74,22 @@ constexpr int INV_RANK = 118;     // vertex ranks packed as a double-encoded int
 constexpr int INV_NDOUBLE = 119;
 constexpr int INV_STRIDE = 120;   // per-tet record length in the array-of-structs buffer (960 B)
 
-// Orientation of the tet's local entities from the rank (0..3) of each vertex's global id.
+// Orientation of the tet's local entities from the rank (0..3) of each vertex's global id,
+// packed 2 bits per vertex (no per-thread arrays, so nothing spills to local memory).
 struct Orient {
-    int rank[4];
+    int code;
+    EMFEM_HD int rank(int v) const { return (code >> (2 * v)) & 3; }
     EMFEM_HD void edge(int e, int& a, int& b) const {
         int p = tet_edge_p(e), q = tet_edge_q(e);
-        if (rank[p] < rank[q]) { a = p; b = q; } else { a = q; b = p; }
+        bool keep = rank(p) < rank(q);
+        a = keep ? p : q;
+        b = keep ? q : p;
     }
     EMFEM_HD void face(int f, int& a, int& b, int& c) const {
         int v0 = tet_face_v(f, 0), v1 = tet_face_v(f, 1), v2 = tet_face_v(f, 2), t;
-        if (rank[v1] < rank[v0]) { t = v0; v0 = v1; v1 = t; }
-        if (rank[v2] < rank[v1]) { t = v1; v1 = v2; v2 = t; }
-        if (rank[v1] < rank[v0]) { t = v0; v0 = v1; v1 = t; }
+        if (rank(v1) < rank(v0)) { t = v0; v0 = v1; v1 = t; }
+        if (rank(v2) < rank(v1)) { t = v1; v1 = v2; v2 = t; }
+        if (rank(v1) < rank(v0)) { t = v0; v0 = v1; v1 = t; }
         a = v0; b = v1; c = v2;
     }
 };
@@ -101,8 +105,22 @@ EMFEM_HD int pack_rank(const int64_t ids[4]) {
 }
 EMFEM_HD Orient unpack_rank(int code) {
     Orient o;
-    for (int i = 0; i < 4; i++) o.rank[i] = (code >> (2 * i)) & 3;
+    o.code = code;
     return o;
+}
+
+// Volume coefficient of letters a..d (1..4 name vertices, 0 = absent) without arrays:
+// prod k_i! over the letter multiplicities, divided by (n + 3)!.
+EMFEM_HD double volume_coeff_closed(int a, int b, int c, int d) {
+    int l[4] = {a, b, c, d};
+    int n = (a > 0) + (b > 0) + (c > 0) + (d > 0);
+    double num = 1.0;
+    for (int v = 1; v <= 4; v++) {
+        int k = (l[0] == v) + (l[1] == v) + (l[2] == v) + (l[3] == v);
+        num *= k == 2 ? 2.0 : k == 3 ? 6.0 : k == 4 ? 24.0 : 1.0;
+    }
+    double den = n == 0 ? 6.0 : n == 1 ? 24.0 : n == 2 ? 120.0 : n == 3 ? 720.0 : 5040.0;
+    return num / den;
 }
 
 // det of [[1,p_j,q_j],[1,p_k,q_k],[1,p_l,q_l]]

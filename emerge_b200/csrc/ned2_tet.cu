@@ -65,15 +65,8 @@ __global__ void __launch_bounds__(128) tet_invariants_kernel(
 }
 
 __device__ __forceinline__ void load_vtab(double* sh) {
-    for (int i = threadIdx.x; i < 625; i += blockDim.x) {
-        int a = i / 125, b = (i / 25) % 5, c = (i / 5) % 5, d = i % 5;
-        int cnt[7] = {0, 0, 0, 0, 0, 0, 0};
-        cnt[a]++; cnt[b]++; cnt[c]++; cnt[d]++;
-        const double fact[10] = {1, 1, 2, 6, 24, 120, 720, 5040, 40320, 362880};
-        double num = 1; int n = 0;
-        for (int k = 1; k < 7; k++) { num *= fact[cnt[k]]; n += cnt[k]; }
-        sh[i] = num / fact[n + 3];
-    }
+    for (int i = threadIdx.x; i < 625; i += blockDim.x)
+        sh[i] = volume_coeff_closed(i / 125, (i / 25) % 5, (i / 5) % 5, i % 5);
 }
 
 // ---------------------------------------------------------------- per-element matrices
@@ -341,77 +334,144 @@ __global__ void export_indices_kernel(long long H, long long sum_m, const int* _
 
 // ---------------------------------------------------------------- fused numeric assembly
 // One CTA per chunk of consecutive entities of one kind (all edges or all faces) holding at most
-// CH_INC incidences.  Phase 1: one thread per (incidence, column entity) pair block, column-entity
-// major so that every warp evaluates the same edge/face block type; results staged in shared
-// memory.  Phase 2: one thread per output (X, k) sums its tets' staged blocks in ascending tet
-// order and writes the 4 E and 4 B CSR values of its column pair.
-constexpr int CH_INC = 64;
-constexpr int CH_THREADS = 320;
-constexpr int CH_SMEM = CH_INC * 10 * 8 * 16 + 625 * 8 + CH_INC * 16 + CH_INC * 4 + 16;
+// CH incidences.  Phase 0: the chunk's incidence records and the invariants of their tets are
+// copied to shared memory with coalesced loads.  Phase 1: one thread per (incidence, column entity)
+// pair block, column-entity major so every warp evaluates one edge/face block type; results staged
+// in shared memory.  Phase 2: one thread per output (X, k) sums its tets' staged blocks in
+// ascending tet order and writes the 4 E and 4 B CSR values of its column pair.
+constexpr int INV_SMEM_STRIDE = 121;  // odd stride in doubles: lanes of a warp hit distinct banks
 
-__global__ void __launch_bounds__(CH_THREADS) assemble_chunk_kernel(
+template <int CH, bool SINV>
+struct ChunkSmem {
+    static constexpr size_t stage = (size_t)CH * 10 * 8 * 16;
+    static constexpr size_t inv = SINV ? (size_t)CH * INV_SMEM_STRIDE * 8 : 0;
+    static constexpr size_t vtab = 625 * 8;
+    static constexpr size_t rec = (size_t)CH * 16;
+    static constexpr size_t code = (size_t)CH * 4;
+    static constexpr size_t off_inv = stage;
+    static constexpr size_t off_vtab = off_inv + inv;
+    static constexpr size_t off_rec = (off_vtab + vtab + 15) & ~(size_t)15;
+    static constexpr size_t off_code = off_rec + rec;
+    static constexpr size_t off_ent = off_code + code;              // (CH + 1) mptr, (CH + 1) inc_ptr
+    static constexpr size_t total = off_ent + (size_t)(2 * CH + 2) * 4;
+};
+
+template <int CH, int NT, int MINB, bool SINV>
+__global__ void __launch_bounds__(NT, MINB) assemble_chunk_kernel(
     const int* __restrict__ chunk_ptr, long long H, const int* __restrict__ mptr,
     const int* __restrict__ inc_ptr, const uint32_t* __restrict__ inc_code, const uint4* __restrict__ rec,
     const double* __restrict__ inv, double2* __restrict__ Ev, double2* __restrict__ Bv) {
+    typedef ChunkSmem<CH, SINV> L;
     extern __shared__ __align__(16) unsigned char smem[];
-    double2* stage = reinterpret_cast<double2*>(smem);                                  // [CH_INC][10][8]
-    double* vtab = reinterpret_cast<double*>(smem + CH_INC * 10 * 8 * 16);               // 625
-    uint4* srec = reinterpret_cast<uint4*>(smem + CH_INC * 10 * 8 * 16 + 625 * 8 + 8);   // CH_INC (16 B aligned)
-    uint32_t* scode = reinterpret_cast<uint32_t*>(srec + CH_INC);                         // CH_INC
+    double2* stage = reinterpret_cast<double2*>(smem);                 // [sy * 8 + q][CH]
+    double* sinv = reinterpret_cast<double*>(smem + L::off_inv);       // [CH][INV_SMEM_STRIDE]
+    double* vtab = reinterpret_cast<double*>(smem + L::off_vtab);      // 625
+    uint4* srec = reinterpret_cast<uint4*>(smem + L::off_rec);         // CH
+    uint32_t* scode = reinterpret_cast<uint32_t*>(smem + L::off_code); // CH
+    int* smptr = reinterpret_cast<int*>(smem + L::off_ent);             // chunk entities' mptr, X0..X1
+    int* sinc = smptr + CH + 1;                                          // chunk entities' inc_ptr - i0
     load_vtab(vtab);
     const int X0 = chunk_ptr[blockIdx.x], X1 = chunk_ptr[blockIdx.x + 1];
     const int i0 = inc_ptr[X0], ninc = inc_ptr[X1] - i0;
-    for (int li = threadIdx.x; li < ninc; li += CH_THREADS) {
+    const int nent = X1 - X0;  // <= CH: every entity has at least one incidence
+    for (int li = threadIdx.x; li < ninc; li += NT) {
         srec[li] = rec[i0 + li];
         scode[li] = inc_code[i0 + li];
+    }
+    for (int e = threadIdx.x; e <= nent; e += NT) {
+        smptr[e] = mptr[X0 + e];
+        sinc[e] = inc_ptr[X0 + e] - i0;
+    }
+    __syncthreads();
+    if (SINV) {
+        // one warp per incidence: lanes copy consecutive doubles of the tet's record
+        const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+        for (int li = warp; li < ninc; li += NT / 32) {
+            const double* src = inv + (long long)(scode[li] >> 4) * INV_STRIDE;
+            double* dst = sinv + li * INV_SMEM_STRIDE;
+#pragma unroll
+            for (int f = lane; f < INV_NDOUBLE; f += 32) dst[f] = src[f];
+        }
     }
     __syncthreads();
     VTab T{vtab};
     const int npad = (ninc + 31) & ~31;
-    for (int w = threadIdx.x; w < 10 * npad; w += CH_THREADS) {
+    for (int w = threadIdx.x; w < 10 * npad; w += NT) {
         int sy = w / npad, li = w - sy * npad;
         if (li >= ninc) continue;
-        uint4 r4 = srec[li];
-        int sx = (int)((r4.z >> 16) & 0xff);  // byte 10 of the record
-        long long t = scode[li] >> 4;
-        InvView I{inv + t * INV_STRIDE, 1};
+        int sx = (int)((srec[li].z >> 16) & 0xff);  // byte 10 of the record
+        InvView I = SINV ? InvView{sinv + li * INV_SMEM_STRIDE, 1}
+                         : InvView{inv + (long long)(scode[li] >> 4) * INV_STRIDE, 1};
         Orient o = unpack_rank((int)I.g(INV_RANK));
         cd d[4], f[4];
         pair_block(I, o, T, sx, sy, d, f);
-        double2* dst = stage + (li * 10 + sy) * 8;
 #pragma unroll
         for (int q = 0; q < 4; q++) {
-            dst[q] = make_double2(d[q].x, d[q].y);
-            dst[4 + q] = make_double2(f[q].x, f[q].y);
+            stage[(sy * 8 + q) * CH + li] = make_double2(d[q].x, d[q].y);
+            stage[(sy * 8 + 4 + q) * CH + li] = make_double2(f[q].x, f[q].y);
         }
     }
     __syncthreads();
-    const int m0 = mptr[X0], total = mptr[X1] - m0;
+    const int m0 = smptr[0], total = smptr[nent] - m0;
     const long long two_mH = 2LL * mptr[H];
-    for (int o = threadIdx.x; o < total; o += CH_THREADS) {
+    for (int o = threadIdx.x; o < total; o += NT) {
         int j = m0 + o;
-        int lo = X0, hi = X1;  // largest X in [X0, X1) with mptr[X] <= j
-        while (hi - lo > 1) { int mid = (lo + hi) >> 1; if (mptr[mid] <= j) lo = mid; else hi = mid; }
-        const int X = lo;
-        const int mb = mptr[X], k = j - mb, m = mptr[X + 1] - mb;
+        int lo = 0, hi = nent;  // largest e in [0, nent) with smptr[e] <= j
+        while (hi - lo > 1) { int mid = (lo + hi) >> 1; if (smptr[mid] <= j) lo = mid; else hi = mid; }
+        const int mb = smptr[lo], k = j - mb, m = smptr[lo + 1] - mb;
         double2 acc[8];
 #pragma unroll
         for (int q = 0; q < 8; q++) acc[q] = make_double2(0.0, 0.0);
-        for (int li = inc_ptr[X] - i0; li < inc_ptr[X + 1] - i0; li++) {
+        for (int li = sinc[lo]; li < sinc[lo + 1]; li++) {
             uint4 r4 = srec[li];
             uint32_t wds[4] = {r4.x, r4.y, r4.z, r4.w};
             int sy = -1;
 #pragma unroll
             for (int q = 0; q < 10; q++) if ((int)((wds[q >> 2] >> (8 * (q & 3))) & 0xff) == k) sy = q;
             if (sy < 0) continue;
-            const double2* src = stage + (li * 10 + sy) * 8;
 #pragma unroll
-            for (int q = 0; q < 8; q++) { acc[q].x += src[q].x; acc[q].y += src[q].y; }
+            for (int q = 0; q < 8; q++) {
+                double2 v = stage[(sy * 8 + q) * CH + li];
+                acc[q].x += v.x; acc[q].y += v.y;
+            }
         }
         long long b1 = 2LL * mb + k, b2 = two_mH + 2LL * mb + k;
         Ev[b1] = acc[0]; Ev[b1 + m] = acc[1]; Ev[b2] = acc[2]; Ev[b2 + m] = acc[3];
         Bv[b1] = acc[4]; Bv[b1 + m] = acc[5]; Bv[b2] = acc[6]; Bv[b2 + m] = acc[7];
     }
+}
+
+// Kernel variants: chunk capacity CH incidences, NT threads, min resident CTAs, invariants staged in
+// shared memory or read through L1.  The plan times them and keeps the fastest.
+struct AsmVariant { int ch; int nt; size_t smem; };
+#define EMFEM_ASM_VARIANTS(X)              \
+    X(0, 32, 160, 2, true)                 \
+    X(1, 32, 160, 4, false)                \
+    X(2, 64, 320, 1, true)                 \
+    X(3, 16, 128, 5, false)                \
+    X(4, 32, 160, 3, false)                \
+    X(5, 64, 320, 2, false)
+constexpr int N_ASM_VARIANTS = 6;
+#define EMFEM_V_ENTRY(i, ch, nt, mb, si) {ch, nt, ChunkSmem<ch, si>::total},
+static const AsmVariant ASM_VARIANTS[N_ASM_VARIANTS] = {EMFEM_ASM_VARIANTS(EMFEM_V_ENTRY)};
+
+static void launch_asm_variant(int v, unsigned grid, cudaStream_t s, const int* chunk_ptr, long long H, const int* mptr,
+                               const int* inc_ptr, const uint32_t* inc_code, const uint4* rec, const double* inv,
+                               double2* E, double2* B) {
+    switch (v) {
+#define EMFEM_V_LAUNCH(i, ch, nt, mb, si) \
+    case i: assemble_chunk_kernel<ch, nt, mb, si><<<grid, nt, ASM_VARIANTS[i].smem, s>>>(chunk_ptr, H, mptr, inc_ptr, inc_code, rec, inv, E, B); break;
+        EMFEM_ASM_VARIANTS(EMFEM_V_LAUNCH)
+    default: break;
+    }
+}
+
+static cudaError_t set_asm_smem_attributes() {
+    cudaError_t e = cudaSuccess;
+#define EMFEM_V_ATTR(i, ch, nt, mb, si) \
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(assemble_chunk_kernel<ch, nt, mb, si>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ASM_VARIANTS[i].smem);
+    EMFEM_ASM_VARIANTS(EMFEM_V_ATTR)
+    return e;
 }
 
 __global__ void find_slots_kernel(long long n, long long H, const int* __restrict__ mptr, const int* __restrict__ S,
@@ -447,14 +507,16 @@ struct emfem_plan_s {
     int* mptr = nullptr;           // H + 1
     int* S = nullptr;              // sum_m
     double* inv = nullptr;         // INV_STRIDE * nt (array of structs)
-    int* chunk_ptr = nullptr;      // n_chunks + 1 entity boundaries
-    int n_chunks = 0;
+    int* chunk_ptr[N_ASM_VARIANTS] = {nullptr};   // per variant: n_chunks + 1 entity boundaries
+    int n_chunks[N_ASM_VARIANTS] = {0};
+    int variant = 0;                                 // kernel variant used by emfem_plan_assemble
 };
 
 static void plan_free(emfem_plan p) {
     if (!p) return;
     cudaFree(p->inc_ptr); cudaFree(p->inc_code); cudaFree(p->rec);
-    cudaFree(p->mptr); cudaFree(p->S); cudaFree(p->inv); cudaFree(p->chunk_ptr);
+    cudaFree(p->mptr); cudaFree(p->S); cudaFree(p->inv);
+    for (int v = 0; v < N_ASM_VARIANTS; v++) cudaFree(p->chunk_ptr[v]);
     delete p;
 }
 
@@ -564,30 +626,39 @@ int emfem_plan_create(emfem_handle h, int64_t n_tets, int64_t n_edges, int64_t n
                                                       p->S, p->rec, h->h.dev_status);
     PTRY(check_cuda(cudaGetLastError(), "cols_fill_kernel"));
     {
-        // greedy chunks of whole entities of one kind with at most CH_INC incidences each
+        // greedy chunks of whole entities of one kind with at most CH incidences each, per variant
         std::vector<int> hptr(H + 1);
         PTRY(check_cuda(cudaMemcpyAsync(hptr.data(), p->inc_ptr, (H + 1) * sizeof(int), cudaMemcpyDeviceToHost, s), "copy"));
         PTRY(check_cuda(cudaStreamSynchronize(s), "sync"));
-        std::vector<int> cptr;
-        cptr.push_back(0);
-        int cur = 0;
-        for (long long X = 0; X < H; X++) {
-            int deg = hptr[X + 1] - hptr[X];
-            if (deg > CH_INC) {
-                set_error("emfem_plan_create: an edge or face is shared by %d tets (at most %d supported)", deg, CH_INC);
-                st = EMFEM_ERR_INVALID_ARG;
-                goto fail;
+        int maxdeg = 0;
+        for (long long X = 0; X < H; X++) maxdeg = std::max(maxdeg, hptr[X + 1] - hptr[X]);
+        p->variant = -1;
+        for (int v = 0; v < N_ASM_VARIANTS; v++) {
+            const int CH = ASM_VARIANTS[v].ch;
+            if (maxdeg > CH) continue;  // an entity must fit one chunk
+            std::vector<int> cptr;
+            cptr.push_back(0);
+            int cur = 0;
+            for (long long X = 0; X < H; X++) {
+                int deg = hptr[X + 1] - hptr[X];
+                bool kind_change = X == n_edges && X > cptr.back();
+                bool full = (cur + deg > CH || X - cptr.back() >= CH) && X > cptr.back();
+                if (full || kind_change) { cptr.push_back((int)X); cur = 0; }
+                cur += deg;
             }
-            bool kind_change = X == n_edges && X > cptr.back();
-            if ((cur + deg > CH_INC && X > cptr.back()) || kind_change) { cptr.push_back((int)X); cur = 0; }
-            cur += deg;
+            cptr.push_back((int)H);
+            p->n_chunks[v] = (int)cptr.size() - 1;
+            PTRY(check_cuda(cudaMalloc(&p->chunk_ptr[v], cptr.size() * sizeof(int)), "cudaMalloc(chunk_ptr)"));
+            PTRY(check_cuda(cudaMemcpyAsync(p->chunk_ptr[v], cptr.data(), cptr.size() * sizeof(int), cudaMemcpyHostToDevice, s), "copy"));
+            PTRY(check_cuda(cudaStreamSynchronize(s), "sync"));
+            if (p->variant < 0) p->variant = v;
         }
-        cptr.push_back((int)H);
-        p->n_chunks = (int)cptr.size() - 1;
-        PTRY(check_cuda(cudaMalloc(&p->chunk_ptr, cptr.size() * sizeof(int)), "cudaMalloc(chunk_ptr)"));
-        PTRY(check_cuda(cudaMemcpyAsync(p->chunk_ptr, cptr.data(), cptr.size() * sizeof(int), cudaMemcpyHostToDevice, s), "copy"));
-        PTRY(check_cuda(cudaFuncSetAttribute(assemble_chunk_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, CH_SMEM),
-                        "cudaFuncSetAttribute"));
+        if (p->variant < 0) {
+            set_error("emfem_plan_create: an edge or face is shared by %d tets (at most 64 supported)", maxdeg);
+            st = EMFEM_ERR_INVALID_ARG;
+            goto fail;
+        }
+        PTRY(check_cuda(set_asm_smem_attributes(), "cudaFuncSetAttribute"));
     }
     PTRY(check_cuda(cudaStreamSynchronize(s), "sync"));
     cudaFree(cnt); cudaFree(cursor); cudaFree(scratch); cudaFree(tmp); cudaFree(m);
@@ -633,10 +704,24 @@ int emfem_plan_assemble(emfem_plan p, int64_t n_nodes, int64_t n_edges, const do
                                                                 edge_lengths, (const double2*)ur, (const double2*)er,
                                                                 p->inv, p->h->dev_status);
     EMFEM_LAUNCH("tet_invariants_kernel");
-    assemble_chunk_kernel<<<p->n_chunks, CH_THREADS, CH_SMEM, s>>>(
-        p->chunk_ptr, p->H, p->mptr, p->inc_ptr, p->inc_code, (const uint4*)p->rec, p->inv,
-        (double2*)E_vals, (double2*)B_vals);
+    const int v = p->variant;
+    launch_asm_variant(v, (unsigned)p->n_chunks[v], s, p->chunk_ptr[v], p->H, p->mptr, p->inc_ptr, p->inc_code,
+                       (const uint4*)p->rec, p->inv, (double2*)E_vals, (double2*)B_vals);
     EMFEM_LAUNCH("assemble_chunk_kernel");
+    return EMFEM_OK;
+}
+
+int emfem_plan_variants(emfem_plan p, int* n_variants, int* current) {
+    EMFEM_REQUIRE(p, "emfem_plan_variants: null plan");
+    if (n_variants) *n_variants = N_ASM_VARIANTS;
+    if (current) *current = p->variant;
+    return EMFEM_OK;
+}
+
+int emfem_plan_set_variant(emfem_plan p, int variant) {
+    EMFEM_REQUIRE(p && variant >= 0 && variant < N_ASM_VARIANTS, "emfem_plan_set_variant: bad variant");
+    EMFEM_REQUIRE(p->chunk_ptr[variant] != nullptr, "emfem_plan_set_variant: variant %d cannot hold this mesh's incidences", variant);
+    p->variant = variant;
     return EMFEM_OK;
 }
 

@@ -94,6 +94,11 @@ int emfem_plan_export_csr(emfem_plan plan, int32_t *indptr, int32_t *indices);
 int emfem_plan_assemble(emfem_plan plan, int64_t n_nodes, int64_t n_edges, const double *nodes,
                         const int64_t *tets, const int64_t *tet_to_edge, const double *edge_lengths,
                         const void *ur, const void *er, void *E_vals, void *B_vals);
+/* Kernel variants of emfem_plan_assemble (chunk capacity x threads per CTA).  A project autotuner
+ * (emerge_b200.assembly.CsrPlan.tune) times them on the device and selects the fastest; variants
+ * whose chunk cannot hold the mesh's largest edge/face incidence are unavailable. */
+int emfem_plan_variants(emfem_plan plan, int *n_variants, int *current);
+int emfem_plan_set_variant(emfem_plan plan, int variant);
 /* CSR slot of each (row, col) pair (device int64 arrays of length n), -1 where absent. */
 int emfem_plan_find_slots(emfem_plan plan, int64_t n, const int64_t *rows, const int64_t *cols,
                           int32_t *slots);

@@ -200,10 +200,22 @@ class CsrPlan:
         check(lib().emfem_plan_find_slots(self._p, rows.numel(), ptr(rows), ptr(cols), ptr(out)), "emfem_plan_find_slots")
         return out
 
+    def host_pattern(self) -> tuple[np.ndarray, np.ndarray]:
+        """Host copy of (indptr, indices), downloaded once per plan (the pattern never changes)."""
+        if getattr(self, "_host_pattern", None) is None:
+            self._host_pattern = (self.indptr.cpu().numpy(), self.indices.cpu().numpy())
+        return self._host_pattern
+
     def to_scipy(self, vals: torch.Tensor) -> csr_matrix:
+        """SciPy CSR with fresh value storage and the (shared, read-only) cached pattern."""
         n = self.n_field
-        A = csr_matrix((vals.cpu().numpy(), self.indices.cpu().numpy(), self.indptr.cpu().numpy()), shape=(n, n))
+        indptr, indices = self.host_pattern()
+        A = csr_matrix((n, n), dtype=np.complex128)
+        A.data = vals.cpu().numpy()
+        A.indices = indices
+        A.indptr = indptr
         A.has_sorted_indices = True
+        A.has_canonical_format = True
         return A
 
 

@@ -343,7 +343,7 @@ constexpr int INV_SMEM_STRIDE = 121;  // odd stride in doubles: lanes of a warp 
 
 template <int CH, bool SINV>
 struct ChunkSmem {
-    static constexpr size_t stage = (size_t)CH * 10 * 8 * 16;
+    static constexpr size_t stage = (size_t)(CH + 1) * 10 * 8 * 16;
     static constexpr size_t inv = SINV ? (size_t)CH * INV_SMEM_STRIDE * 8 : 0;
     static constexpr size_t vtab = 625 * 8;
     static constexpr size_t rec = (size_t)CH * 16;
@@ -363,7 +363,7 @@ __global__ void __launch_bounds__(NT, MINB) assemble_chunk_kernel(
     const double* __restrict__ inv, double2* __restrict__ Ev, double2* __restrict__ Bv) {
     typedef ChunkSmem<CH, SINV> L;
     extern __shared__ __align__(16) unsigned char smem[];
-    double2* stage = reinterpret_cast<double2*>(smem);                 // [sy * 8 + q][CH]
+    double2* stage = reinterpret_cast<double2*>(smem);                 // [q][sy][CH + 1] (padded rows)
     double* sinv = reinterpret_cast<double*>(smem + L::off_inv);       // [CH][INV_SMEM_STRIDE]
     double* vtab = reinterpret_cast<double*>(smem + L::off_vtab);      // 625
     uint4* srec = reinterpret_cast<uint4*>(smem + L::off_rec);         // CH
@@ -407,8 +407,8 @@ __global__ void __launch_bounds__(NT, MINB) assemble_chunk_kernel(
         pair_block(I, o, T, sx, sy, d, f);
 #pragma unroll
         for (int q = 0; q < 4; q++) {
-            stage[(sy * 8 + q) * CH + li] = make_double2(d[q].x, d[q].y);
-            stage[(sy * 8 + 4 + q) * CH + li] = make_double2(f[q].x, f[q].y);
+            stage[(q * 10 + sy) * (CH + 1) + li] = make_double2(d[q].x, d[q].y);
+            stage[((4 + q) * 10 + sy) * (CH + 1) + li] = make_double2(f[q].x, f[q].y);
         }
     }
     __syncthreads();
@@ -431,7 +431,7 @@ __global__ void __launch_bounds__(NT, MINB) assemble_chunk_kernel(
             if (sy < 0) continue;
 #pragma unroll
             for (int q = 0; q < 8; q++) {
-                double2 v = stage[(sy * 8 + q) * CH + li];
+                double2 v = stage[(q * 10 + sy) * (CH + 1) + li];
                 acc[q].x += v.x; acc[q].y += v.y;
             }
         }

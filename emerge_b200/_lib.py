@@ -68,6 +68,8 @@ _SIGS = {
                           _dbl, _i32, _i32, _i32, _vp, ctypes.c_size_t, _i32p, _i32p, _dblp], _i32),
     "emfem_sweep_spmv": ([_vp, _i64, _vp, _vp, _vp, _vp, _i32, _vp, _i64, _vp, _vp, _vp, _vp, _vp, _i32, _vp,
                           _vp, _vp, _vp], _i32),
+    "emfem_port_overlap": ([_vp, _i64, _vp, _i64, _vp, _vp, _i64, _i64, _vp, _vp, _vp, _i32, _vp, _vp, _i32, _vp,
+                            _vp, _vp, _vp], _i32),
     "emfem_sweep_spmv_noalloc": ([_vp, _i64, _vp, _vp, _vp, _vp, _i32, _vp, _i64, _vp, _vp, _vp, _vp, _vp, _i32,
                                   _vp, _vp, _vp, _vp], _i32),
 }

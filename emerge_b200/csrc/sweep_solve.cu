@@ -93,6 +93,10 @@ __device__ __forceinline__ void block_store2(double2 v0, double2 v1, int ncomp, 
 }
 
 // y = A x for all systems, one thread per (row, system); optional dot-product epilogue (DotMode).
+// The operator values (E, B, Robin patch) are always FP64 and every row is accumulated in FP64;
+// R is the precision of the Krylov vectors only (FP32 in the mixed-precision inner solve), so the
+// inner iterations see the exact operator and only the vectors are rounded.  Rounding E and B to
+// FP32 separately would lose the cancellation in E - k0^2 B near resonances.
 template <typename R>
 __global__ void __launch_bounds__(VB) spmv_kernel(OpArgs a, const typename V2<R>::T* __restrict__ x,
                                                    typename V2<R>::T* __restrict__ y, double2* __restrict__ partial,
@@ -105,46 +109,47 @@ __global__ void __launch_bounds__(VB) spmv_kernel(OpArgs a, const typename V2<R>
     double2 c0 = make_double2(0.0, 0.0), c1 = c0;
     double c2 = 0.0;
     if (i < a.n) {
-        R yr = 0, yi = 0;
+        double yr = 0, yi = 0;
         if (a.mask[i]) {
-            const T* Ev = (const T*)a.E;
-            const T* Bv = (const T*)a.B;
-            R er = 0, ei = 0, br = 0, bi = 0;
+            const double2* Ev = (const double2*)a.E;
+            const double2* Bv = (const double2*)a.B;
+            double er = 0, ei = 0, br = 0, bi = 0;
             int jb = a.indptr[i], je = a.indptr[i + 1];
             for (int j = jb; j < je; j++) {
                 int c = a.indices[j];
                 T xv = x[(long long)c * S + s];
-                T e = Ev[j];
-                er += e.x * xv.x - e.y * xv.y;
-                ei += e.x * xv.y + e.y * xv.x;
+                double xr = xv.x, xi = xv.y;
+                double2 e = Ev[j];
+                er += e.x * xr - e.y * xi;
+                ei += e.x * xi + e.y * xr;
                 if (Bv) {
-                    T b = Bv[j];
-                    br += b.x * xv.x - b.y * xv.y;
-                    bi += b.x * xv.y + b.y * xv.x;
+                    double2 b = Bv[j];
+                    br += b.x * xr - b.y * xi;
+                    bi += b.x * xi + b.y * xr;
                 }
             }
-            R k2 = (R)a.k0sq[s];
+            double k2 = a.k0sq[s];
             yr = er - k2 * br;
             yi = ei - k2 * bi;
             int pr = a.patch_of_row ? a.patch_of_row[i] : -1;
             if (pr >= 0) {
-                const T* Pv = (const T*)a.patch_vals;
+                const double2* Pv = (const double2*)a.patch_vals;
                 for (int q = 0; q < a.n_ports; q++) {
-                    R pr_ = 0, pi_ = 0;
+                    double pr_ = 0, pi_ = 0;
                     for (int j = a.patch_rowptr[pr]; j < a.patch_rowptr[pr + 1]; j++) {
                         if (a.patch_port[j] != q) continue;
                         T xv = x[(long long)a.patch_cols[j] * S + s];
-                        T v = Pv[j];
+                        double2 v = Pv[j];
                         pr_ += v.x * xv.x - v.y * xv.y;
                         pi_ += v.x * xv.y + v.y * xv.x;
                     }
-                    R gr = (R)a.gamma[2 * (s * a.n_ports + q)], gi = (R)a.gamma[2 * (s * a.n_ports + q) + 1];
+                    double gr = a.gamma[2 * (s * a.n_ports + q)], gi = a.gamma[2 * (s * a.n_ports + q) + 1];
                     yr += gr * pr_ - gi * pi_;
                     yi += gr * pi_ + gi * pr_;
                 }
             }
         }
-        y[i * S + s] = mk2<R>(yr, yi);
+        y[i * S + s] = mk2<R>((R)yr, (R)yi);
         if (dotmode == DOT_XY) {
             T xi = x[i * S + s];
             c0 = make_double2((double)xi.x * yr - (double)xi.y * yi, (double)xi.x * yi + (double)xi.y * yr);
@@ -153,8 +158,8 @@ __global__ void __launch_bounds__(VB) spmv_kernel(OpArgs a, const typename V2<R>
             c0 = make_double2((double)wi.x * yr + (double)wi.y * yi, (double)wi.x * yi - (double)wi.y * yr);
         } else if (dotmode == DOT_CONJY_W_YY) {
             T wi = w[i * S + s];
-            c0 = make_double2((double)yr * wi.x + (double)yi * wi.y, (double)yr * wi.y - (double)yi * wi.x);
-            c1 = make_double2((double)yr * yr + (double)yi * yi, 0.0);
+            c0 = make_double2(yr * wi.x + yi * wi.y, yr * wi.y - yi * wi.x);
+            c1 = make_double2(yr * yr + yi * yi, 0.0);
             c2 = nrm2(wi);
         }
     }
@@ -669,7 +674,6 @@ struct Layout {
     size_t off_x, off_b, off_r64, off_Ax;                  // FP64 vectors (n, S)
     size_t off_v[8];                                       // Krylov vectors of the inner precision
     size_t off_minv;
-    size_t off_E32, off_B32, off_P32;                      // FP32 operator copies (mixed)
     size_t total;
 };
 
@@ -693,13 +697,7 @@ static Layout make_layout(long long n, long long nnz, long long npatch, int S, i
     L.off_Ax = o; o = align256(o + vec64);
     for (int k = 0; k < 8; k++) { L.off_v[k] = o; o = align256(o + vecw); }
     L.off_minv = o; o = align256(o + vecw * 2);  // (n/2) * S * 4 entries
-    if (precision) {
-        L.off_E32 = o; o = align256(o + sizeof(float2) * nnz);
-        L.off_B32 = o; o = align256(o + sizeof(float2) * nnz);
-        L.off_P32 = o; o = align256(o + sizeof(float2) * (npatch > 0 ? npatch : 1));
-    } else {
-        L.off_E32 = L.off_B32 = L.off_P32 = 0;
-    }
+    (void)nnz; (void)npatch;
     L.total = o;
     return L;
 }
@@ -963,15 +961,7 @@ int emfem_krylov_solve(emfem_handle hd, int method, int64_t n, int64_t nnz, cons
         STRY(k.start());
         STRY(k.run(16));
     } else {
-        float2* E32 = (float2*)(ws + L.off_E32);
-        float2* B32 = (float2*)(ws + L.off_B32);
-        float2* P32 = (float2*)(ws + L.off_P32);
-        cast_values_kernel<<<grid_for(nnz, VB), VB, 0, s>>>(nnz, (const double2*)E_vals, E32);
-        if (B_vals) cast_values_kernel<<<grid_for(nnz, VB), VB, 0, s>>>(nnz, (const double2*)B_vals, B32);
-        if (npatch > 0) cast_values_kernel<<<grid_for(npatch, VB), VB, 0, s>>>(npatch, (const double2*)patch_vals, P32);
-        STRY(check_cuda(cudaGetLastError(), "cast values"));
-        OpArgs op32 = op64;
-        op32.E = E32; op32.B = B_vals ? B32 : nullptr; op32.patch_vals = P32;
+        OpArgs op32 = op64;  // FP64 values, FP32 vectors (see spmv_kernel)
         Krylov<float> k;
         k.method = method; k.op = op32; k.n = n; k.h = n / 2; k.S = S; k.precond = precond; k.nsys = nsys;
         float2* r32 = (float2*)(ws + L.off_v[6]);

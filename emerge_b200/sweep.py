@@ -64,6 +64,23 @@ class SolveResult:
     seconds: float
 
 
+def sparam_corrections(S: np.ndarray, col: bool = True, single: bool = True, recip: bool = False) -> np.ndarray:
+    """The reference's S-matrix post-corrections, defaults as in its settings
+    (``MW/microwave_3d.py:1208-1225``, ``src/emerge/_emerge/settings.py:25-27``)."""
+    S = np.array(S, dtype=np.complex128)
+    N = S.shape[1]
+    if recip:
+        S = (S + S.T) / 2
+    if col:
+        for j in range(N):
+            S[:, j] = S[:, j] / max(1.0, float(np.sum(np.abs(S[:, j]) ** 2)))
+    if single:
+        for i in range(N):
+            for j in range(N):
+                S[i, j] = S[i, j] / max(1.0, abs(S[i, j]))
+    return S
+
+
 class FrequencySweep:
     def __init__(self, problem, device=None, assemble: bool = True):
         dev = torch.device("cuda", torch.cuda.current_device()) if device is None else torch.device(device)
@@ -132,6 +149,69 @@ class FrequencySweep:
         self.patch_cols = torch.from_numpy(u_cols.astype(np.int32)).to(dev)
         self.patch_port = torch.from_numpy(u_port.astype(np.int32)).to(dev)
         self.n_ports = nports
+
+    # ---------------------------------------------------------------- S-parameters
+    def _port_sp_data(self) -> list:
+        """Per port: owning tets, node ids, unit mode shape at the quadrature points and the TE weight
+        1/mean(diag ur) of the owning tet (``_compute_s_data``, ``MW/microwave_3d.py:1250-1303``)."""
+        if getattr(self, "_spdata", None) is not None:
+            return self._spdata
+        P, mesh, dev = self.problem, self.problem.mesh, self.device
+        dp = dunavant4()
+        out = []
+        for port in P.ports:
+            tid = np.asarray(port.tri_ids, dtype=np.int64)
+            tn = mesh.tris[:, tid]
+            owner = mesh.tri_to_tet[0, tid]
+            pts = np.einsum("cvs,vp->cps", mesh.nodes[:, tn], dp[1:4])               # (3, npts, ntri)
+            shape = port.shape_global(pts[0], pts[1], pts[2]).astype(np.complex128)
+            ur = P.ur[:, :, owner]
+            const = (1.0 / ((ur[0, 0] + ur[1, 1] + ur[2, 2]) / 3)).astype(np.complex128)
+            out.append(dict(n=len(tid),
+                            tri_tet=torch.from_numpy(np.ascontiguousarray(owner)).to(dev),
+                            tri_nodes=torch.from_numpy(np.ascontiguousarray(tn)).to(dev),
+                            shape=torch.from_numpy(np.ascontiguousarray(shape)).to(dev),
+                            const=torch.from_numpy(np.ascontiguousarray(const)).to(dev)))
+        self._spdata = out
+        return out
+
+    def port_overlaps(self, x: torch.Tensor) -> tuple[np.ndarray, np.ndarray]:
+        """(overlap (n_ports, nsys), mode_norm (n_ports,)) of the solutions x (N, nsys) on every port face."""
+        x = x.contiguous()
+        nsys = x.shape[1]
+        h = Handle.get(self.device)
+        d_m = self.dmesh
+        ov, nm = [], []
+        for d in self._port_sp_data():
+            work = torch.empty(d["n"] * (nsys + 1), dtype=torch.complex128, device=self.device)
+            o = torch.empty(nsys, dtype=torch.complex128, device=self.device)
+            m = torch.empty(1, dtype=torch.complex128, device=self.device)
+            check(lib().emfem_port_overlap(h.h, d_m.n_nodes, ptr(d_m.nodes), d_m.n_tets, ptr(d_m.tets),
+                                           ptr(d_m.tet_to_field), self.n, d["n"], ptr(d["tri_tet"]), ptr(d["tri_nodes"]),
+                                           ptr(self.dpts), self.dpts.shape[1], ptr(d["shape"]), ptr(d["const"]), nsys,
+                                           ptr(x), ptr(work), ptr(o), ptr(m)), "emfem_port_overlap")
+            ov.append(o.cpu().numpy())
+            nm.append(m.cpu().numpy()[0])
+        h.raise_on_device_status("emfem_port_overlap")
+        return np.array(ov), np.array(nm)
+
+    def sparams(self, res: SolveResult, corrections: bool = False) -> dict:
+        """S-parameters of solved systems: {frequency: (n_ports, n_ports) complex S} with the columns of
+        the excited ports filled (NaN elsewhere).  S[q, p] is field_power / mode_power / sqrt(P_p) of
+        the reference's ``_post_process`` (``MW/microwave_3d.py:1110-1247``); ``corrections`` applies its
+        default column-power and |S| <= 1 caps."""
+        ov, nm = self.port_overlaps(res.x)
+        P = self.problem
+        out: dict = {}
+        for s, (f, p) in enumerate(res.systems):
+            k0 = k0_of(f)
+            S = out.setdefault(f, np.full((len(P.ports), len(P.ports)), np.nan + 0j))
+            for q, port in enumerate(P.ports):
+                scale = port.qmode(k0) * port.polarization * port.amplitude()
+                S[q, p] = (ov[q, s] / (scale * nm[q]) - (1.0 if q == p else 0.0)) / np.sqrt(P.ports[p].power)
+        if corrections:
+            out = {f: sparam_corrections(S) for f, S in out.items()}
+        return out
 
     # ---------------------------------------------------------------- per-frequency data
     def k0sq(self, freqs) -> np.ndarray:

@@ -165,6 +165,22 @@ int emfem_sweep_spmv(emfem_handle h, int64_t n, const int32_t *indptr, const int
                      int n_ports, const double *gamma_dev, const uint8_t *free_mask,
                      const void *x, void *y);
 
+/* ---- S-parameter overlap integrals -------------------------------------------------------------
+ * For the port triangles (tri_nodes (3, n_tri) i64, their owning tets tri_tet (n_tri) i64) and nsys
+ * solutions x (n_field, nsys) c128, computes the port-mode overlap of every solution,
+ *   overlap[s] = sum_t c_t A_t sum_p W_p E_s(x_p) . conj(shape(x_p)),
+ * and the mode norm N = sum_t c_t A_t sum_p W_p |shape(x_p)|^2, with E interpolated in the owning
+ * tet as ned2_tet_interp does (src/emerge/_emerge/elements/ned2_interp.py:142-300) and the integrals
+ * of sparam_field_power / sparam_mode_power (src/emerge/_emerge/physics/microwave/sparam.py:71-138).
+ * S[q, p] = (overlap / (scale_q(k0) N) - [q == p]) / sqrt(P_p), scale = the mode's amplitude factor.
+ * shape: (3, npts, n_tri) c128 unit mode at the quadrature points; tri_const: (n_tri) c128 (TE:
+ * 1/mean(diag ur)); dpts (4, npts) with npts <= 16; work: device scratch of 16 n_tri (nsys + 1)
+ * bytes; overlap (nsys) and mode_norm (1) c128, device. */
+int emfem_port_overlap(emfem_handle h, int64_t n_nodes, const double *nodes, int64_t n_tets, const int64_t *tets,
+                       const int64_t *tet_to_field, int64_t n_field, int64_t n_tri, const int64_t *tri_tet,
+                       const int64_t *tri_nodes, const double *dpts, int npts, const void *shape,
+                       const void *tri_const, int nsys, const void *x, void *work, void *overlap, void *mode_norm);
+
 /* ---- allocation-free sweep SpMV ------------------------------------------------------------
  * No counterpart in the reference.  The same y_s = A_s x_s as emfem_sweep_spmv, for callers that
  * cannot call cudaMalloc: applications whose device memory is owned up front by their own pool

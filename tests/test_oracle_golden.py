@@ -86,3 +86,13 @@ def test_config1_pattern_and_solution_match_reference(golden):
     xs = oracle.solve_routine(K, pvs, sid)
     for x, gx in zip(xs, (g["x1"], g["x2"])):
         assert np.linalg.norm(x - gx) / np.linalg.norm(gx) <= 1e-10
+
+
+def test_sparam_oracle_matches_reference(golden):
+    """The S-parameter oracle, fed the reference's own SuperLU solutions, reproduces the reference's
+    raw S-matrix (sparam_field_power / sparam_mode_power with ned2_tet_interp)."""
+    from oracle import sparams as osp
+    g = golden("config1")
+    P = problems.waveguide()
+    S = osp.sparams(P, {0: g["x1"], 1: g["x2"]}, k0_of(float(g["f"])), oracle.dunavant4())
+    assert np.abs(S - g["S"]).max() <= 1e-12

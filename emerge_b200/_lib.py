@@ -70,6 +70,10 @@ _SIGS = {
                           _vp, _vp, _vp], _i32),
     "emfem_port_overlap": ([_vp, _i64, _vp, _i64, _vp, _vp, _i64, _i64, _vp, _vp, _vp, _i32, _vp, _vp, _i32, _vp,
                             _vp, _vp, _vp], _i32),
+    "emfem_mesh_connect_create": ([_vp, _i64, _i64, _vp, ctypes.POINTER(_vp)], _i32),
+    "emfem_mesh_connect_info": ([_vp, ctypes.POINTER(_i64), ctypes.POINTER(_i64)], _i32),
+    "emfem_mesh_connect_export": ([_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp], _i32),
+    "emfem_mesh_connect_destroy": ([_vp], _i32),
     "emfem_sweep_spmv_noalloc": ([_vp, _i64, _vp, _vp, _vp, _vp, _i32, _vp, _i64, _vp, _vp, _vp, _vp, _vp, _i32,
                                   _vp, _vp, _vp, _vp], _i32),
 }

@@ -206,12 +206,24 @@ class CsrPlan:
             self._host_pattern = (self.indptr.cpu().numpy(), self.indices.cpu().numpy())
         return self._host_pattern
 
+    def download(self, vals: torch.Tensor) -> np.ndarray:
+        """Device values -> a fresh host array.  The copy goes through a pinned staging buffer owned
+        by the plan (pageable device-to-host copies run at a few GB/s) and then a multi-threaded
+        host copy into new memory, so every call returns storage the caller owns."""
+        if getattr(self, "_stage", None) is None or self._stage.numel() < vals.numel():
+            self._stage = torch.empty(vals.numel(), dtype=vals.dtype, pin_memory=True)
+        stage = self._stage[:vals.numel()]
+        stage.copy_(vals)
+        out = torch.empty(vals.numel(), dtype=vals.dtype)
+        out.copy_(stage)
+        return out.numpy()
+
     def to_scipy(self, vals: torch.Tensor) -> csr_matrix:
         """SciPy CSR with fresh value storage and the (shared, read-only) cached pattern."""
         n = self.n_field
         indptr, indices = self.host_pattern()
         A = csr_matrix((n, n), dtype=np.complex128)
-        A.data = vals.cpu().numpy()
+        A.data = self.download(vals)
         A.indices = indices
         A.indptr = indptr
         A.has_sorted_indices = True

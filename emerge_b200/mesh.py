@@ -10,7 +10,7 @@ The hot path consumes a mesh exactly as EMerge's ``Mesh3D._pre_update`` lays it 
   tet's own vertex order (``mesh3d.py:427``);
 * ``tet_to_tri`` (4, N_t): local triples (1,2,3),(1,3,4),(1,4,2),(2,3,4) (``mesh3d.py:431``);
 * ``tri_to_edge`` (3, N_f): (i1,i2),(i2,i3),(i1,i3) of the sorted triple (``mesh3d.py:476-480``);
-* ``tri_to_tet`` (2, N_f): tets in order of first appearance, padded with -1 (``mesh3d.py:437-447``);
+* ``tri_to_tet`` (2, N_f): tets in order of first appearance, padded with -1234 (``mesh3d.py:27,437-447``);
 * ``edge_lengths`` (N_e,): Euclidean lengths (``mesh3d.py:497``).
 
 gmsh is not part of this package. :func:`box_tet_mesh` builds the synthetic meshes used by the
@@ -25,7 +25,7 @@ import itertools
 
 import numpy as np
 
-MISSING_ID = -1
+MISSING_ID = -1234          # Mesh3D's _MISSING_ID (mesh3d.py:27)
 
 # local vertex pairs / triples, 0-based, in the order Mesh3D uses
 TET_EDGE_PAIRS = ((0, 1), (0, 2), (0, 3), (1, 2), (3, 1), (2, 3))

@@ -38,6 +38,7 @@ extern "C" {
 
 typedef struct emfem_handle_s *emfem_handle;
 typedef struct emfem_plan_s *emfem_plan;
+typedef struct emfem_conn_s *emfem_conn;
 
 /* ---- library / handle ------------------------------------------------------------------- */
 int emfem_version(void);
@@ -180,6 +181,29 @@ int emfem_port_overlap(emfem_handle h, int64_t n_nodes, const double *nodes, int
                        const int64_t *tet_to_field, int64_t n_field, int64_t n_tri, const int64_t *tri_tet,
                        const int64_t *tri_nodes, const double *dpts, int npts, const void *shape,
                        const void *tri_const, int nsys, const void *x, void *work, void *overlap, void *mode_norm);
+
+/* ---- mesh connectivity ---------------------------------------------------------------------
+ * Replaces the connectivity part of Mesh3D._pre_update (src/emerge/_emerge/mesh3d.py:385-497):
+ * the unique sorted edge / triangle node lists in lexicographic order (:386-406), tet_to_edge with
+ * local pairs (1,2),(1,3),(1,4),(2,3),(4,2),(3,4) (:427), tet_to_tri with local triples
+ * (1,2,3),(1,3,4),(1,4,2),(2,3,4) (:431), tri_to_tet with the tets in ascending order, padded with
+ * EMFEM_MISSING_ID (:27, :437-447), tri_to_edge as (i1,i2),(i2,i3),(i1,i3) of the sorted triple (:470-481) and
+ * edge_lengths (:497).  Ids are identical to the reference's.
+ * create: tets (4, n_tets) i64, device; checks node ids are in range and distinct per tet
+ * (EMFEM_ERR_DEVICE_CHECK otherwise), builds the per-node edge / triangle buckets and synchronises
+ * the stream once to learn the counts.  info: the counts, host.  export: writes, all device,
+ * edges (2, n_edges) i64, tris (3, n_tris) i64, tet_to_edge (6, n_tets), tet_to_tri (4, n_tets),
+ * tri_to_edge (3, n_tris), tri_to_tet (2, n_tris) i64 and edge_lengths (n_edges) f64 from nodes
+ * (3, n_nodes) f64; `tets` must be the array given to create.  A triangle shared by more than two
+ * tets (a non-manifold mesh, which the reference rejects) keeps the two smallest tet ids and sets
+ * EMFEM_DEV_CAPACITY. */
+#define EMFEM_MISSING_ID (-1234)  /* Mesh3D's _MISSING_ID (mesh3d.py:27) */
+int emfem_mesh_connect_create(emfem_handle h, int64_t n_nodes, int64_t n_tets, const int64_t *tets, emfem_conn *c);
+int emfem_mesh_connect_info(emfem_conn c, int64_t *n_edges, int64_t *n_tris);
+int emfem_mesh_connect_export(emfem_conn c, const double *nodes, const int64_t *tets, int64_t *edges, int64_t *tris,
+                              int64_t *tet_to_edge, int64_t *tet_to_tri, int64_t *tri_to_edge, int64_t *tri_to_tet,
+                              double *edge_lengths);
+int emfem_mesh_connect_destroy(emfem_conn c);
 
 /* ---- allocation-free sweep SpMV ------------------------------------------------------------
  * No counterpart in the reference.  The same y_s = A_s x_s as emfem_sweep_spmv, for callers that

@@ -20,6 +20,14 @@ Fixtures
     ``SolveRoutine.solve`` submatrix path ``:1266-1313``) and the raw S-matrix from the reference's
     ``sparam_field_power``/``sparam_mode_power`` (``MW/sparam.py:71-138``).
 
+``mesh_conn.npz``      two meshes (a shuffled-local-order box and a box with randomly permuted node ids
+    and tet order, gmsh-style non-contiguous node tags) through the reference's own
+    ``Mesh3D._pre_update`` (``src/emerge/_emerge/mesh3d.py:326-497``), fed by a gmsh stand-in that
+    serves the nodes and tets and reports no surface/edge entities: edges, tris, tet_to_edge,
+    tet_to_tri, tri_to_edge, tri_to_tet and edge_lengths.
+
+Fixtures can be generated one at a time: ``python tests/golden/make_golden.py mesh_conn``.
+
 ``ASM/`` = ``src/emerge/_emerge/physics/microwave/assembly/``; ``MW/`` = ``src/emerge/_emerge/physics/microwave/``.
 """
 from __future__ import annotations
@@ -193,10 +201,62 @@ def config1():
     print(f"config1: nnz={E.nnz} K.nnz={Kmat.nnz} solve={len(solve_ids)} S=\n{S}\n|S|={np.abs(S)}")
 
 
+def _reference_mesh3d(nodes, tets, tag_stride=3, tag_offset=7):
+    """Run Mesh3D._pre_update on (nodes, tets) through a gmsh stand-in (gmsh node tags are
+    tag_offset + tag_stride * (i + 1), tet tags 1..N_t; no 1-D/2-D elements or entities)."""
+    import importlib
+    gm = sys.modules["gmsh"]
+    nn = nodes.shape[1]
+    node_tags = (np.arange(1, nn + 1, dtype=np.uint64) * tag_stride + tag_offset)
+    empty = np.array([], dtype=np.uint64)
+
+    class _MeshNS:
+        @staticmethod
+        def get_nodes(*args):
+            return node_tags, np.ascontiguousarray(nodes.T).ravel(), None
+
+        @staticmethod
+        def get_elements(dim, tag=-1):
+            if dim == 3:
+                return [4], [np.arange(1, tets.shape[1] + 1, dtype=np.uint64)], [node_tags[tets.T.ravel()]]
+            return [], [empty], [empty]
+
+    gm.model = types.SimpleNamespace(mesh=_MeshNS, get_entities=lambda dim=-1: [])
+    M = importlib.import_module("emerge._emerge.mesh3d").Mesh3D()
+    M._pre_update()
+    return M
+
+
+def mesh_conn():
+    out = {}
+    nodes, tets = box_tet_mesh(4, 3, 3, 1.0e-2, 0.8e-2, 0.9e-2, jitter=0.15, seed=21, shuffle_local=True)
+    cases = {"a": (nodes, tets)}
+    rng = np.random.default_rng(77)
+    nodes, tets = box_tet_mesh(5, 4, 3, 2.0e-2, 1.0e-2, 1.5e-2, jitter=0.1, seed=22, shuffle_local=True)
+    perm = rng.permutation(nodes.shape[1])          # new id of old node i = perm[i]
+    nodes_p = np.empty_like(nodes)
+    nodes_p[:, perm] = nodes
+    tets_p = perm[tets][:, rng.permutation(tets.shape[1])]
+    cases["b"] = (nodes_p, tets_p)
+    for key, (nd, tt) in cases.items():
+        M = _reference_mesh3d(nd, tt)
+        out[key + "_nodes"] = nd
+        out[key + "_tets"] = np.asarray(M.tets, dtype=np.int64)
+        for name in ("edges", "tris", "tet_to_edge", "tet_to_tri", "tri_to_edge", "tri_to_tet"):
+            out[key + "_" + name] = np.asarray(getattr(M, name), dtype=np.int64)
+        out[key + "_edge_lengths"] = np.asarray(M.edge_lengths, dtype=np.float64)
+    np.savez_compressed(os.path.join(HERE, "mesh_conn.npz"), **out)
+
+
 if __name__ == "__main__":
-    m, f = element_small()
-    robin_small(m, f)
-    config1()
+    which = sys.argv[1:] or ["element_small", "config1", "mesh_conn"]
+    if "element_small" in which:
+        m, f = element_small()
+        robin_small(m, f)
+    if "config1" in which:
+        config1()
+    if "mesh_conn" in which:
+        mesh_conn()
     for fn in sorted(os.listdir(HERE)):
         if fn.endswith(".npz"):
             print(fn, os.path.getsize(os.path.join(HERE, fn)))

@@ -96,3 +96,21 @@ def test_sparam_oracle_matches_reference(golden):
     P = problems.waveguide()
     S = osp.sparams(P, {0: g["x1"], 1: g["x2"]}, k0_of(float(g["f"])), oracle.dunavant4())
     assert np.abs(S - g["S"]).max() <= 1e-12
+
+
+CONN_KEYS = ("edges", "tris", "tet_to_edge", "tet_to_tri", "tri_to_edge", "tri_to_tet")
+
+
+@pytest.mark.parametrize("case", ["a", "b"])
+def test_connectivity_oracle_and_host_mesh_match_reference(golden, case):
+    """oracle.connectivity and the host TetMesh reproduce Mesh3D._pre_update's arrays exactly."""
+    from oracle import connectivity as oc
+    g = golden("mesh_conn")
+    nodes, tets = g[case + "_nodes"], g[case + "_tets"]
+    o = oc.connectivity(nodes, tets)
+    m = TetMesh(nodes, tets)
+    for k in CONN_KEYS:
+        assert np.array_equal(o[k], g[case + "_" + k]), k
+        assert np.array_equal(getattr(m, k), g[case + "_" + k]), k
+    assert np.array_equal(o["edge_lengths"], g[case + "_edge_lengths"])
+    assert np.abs(m.edge_lengths - g[case + "_edge_lengths"]).max() <= 1e-15

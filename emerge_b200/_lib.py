@@ -65,7 +65,7 @@ _SIGS = {
     "emfem_krylov_workspace_size": ([_i64, _i64, _i32, _i32, ctypes.POINTER(ctypes.c_size_t)], _i32),
     "emfem_krylov_solve": ([_vp, _i32, _i64, _i64, _vp, _vp, _vp, _vp, _i32, _dblp,
                           _i64, _vp, _vp, _vp, _vp, _vp, _i32, _dblp, _vp, _vp, _vp,
-                          _dbl, _i32, _i32, _i32, _vp, ctypes.c_size_t, _i32p, _i32p, _dblp], _i32),
+                          _dbl, _i32, _i32, _i32, _vp, ctypes.c_size_t, _i32p, _i32p, _dblp, _vp], _i32),
     "emfem_sweep_spmv": ([_vp, _i64, _vp, _vp, _vp, _vp, _i32, _vp, _i64, _vp, _vp, _vp, _vp, _vp, _i32, _vp,
                           _vp, _vp, _vp], _i32),
     "emfem_port_overlap": ([_vp, _i64, _vp, _i64, _vp, _vp, _i64, _i64, _vp, _vp, _vp, _i32, _vp, _vp, _i32, _vp,
@@ -74,6 +74,23 @@ _SIGS = {
     "emfem_mesh_connect_info": ([_vp, ctypes.POINTER(_i64), ctypes.POINTER(_i64)], _i32),
     "emfem_mesh_connect_export": ([_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp], _i32),
     "emfem_mesh_connect_destroy": ([_vp], _i32),
+    "emfem_aux_create": ([_vp, _i64, _i64, _i64, _vp, _vp, _vp, _vp, ctypes.POINTER(_vp)], _i32),
+    "emfem_aux_info": ([_vp, ctypes.POINTER(_i64), ctypes.POINTER(_i64), ctypes.POINTER(_i64)], _i32),
+    "emfem_aux_export": ([_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp], _i32),
+    "emfem_aux_set_operator": ([_vp, _i64, _vp, _vp, _vp, _vp, _i64, _vp, _vp, _vp, _vp, _vp, _i32, _vp, _vp, _vp],
+                               _i32),
+    "emfem_aux_reserve": ([_vp, _i32], _i32),
+    "emfem_aux_set_network": ([_vp, _vp], _i32),
+    "emfem_aux_destroy": ([_vp], _i32),
+    "emfem_aux_dinv": ([_vp, _i32, _vp, _vp, _vp], _i32),
+    "emfem_aux_restrict": ([_vp, _i32, _vp, _vp, _vp], _i32),
+    "emfem_aux_prolong": ([_vp, _i32, _vp, _vp, _vp, _i32], _i32),
+    "emfem_mpnn_nparams": ([], _i32),
+    "emfem_mpnn_workspace_floats": ([_vp, _i32, ctypes.POINTER(_i64), ctypes.POINTER(_i64)], _i32),
+    "emfem_mpnn_forward": ([_vp, _i32, _vp, _vp, _vp, _vp], _i32),
+    "emfem_mpnn_backward": ([_vp, _i32, _vp, _vp, _vp, _vp, _vp, _vp], _i32),
+    "emfem_adam_step": ([_vp, _i64, _vp, _vp, _vp, _vp, ctypes.c_float, ctypes.c_float, ctypes.c_float,
+                         ctypes.c_float, ctypes.c_float, _i32], _i32),
     "emfem_sweep_spmv_noalloc": ([_vp, _i64, _vp, _vp, _vp, _vp, _i32, _vp, _i64, _vp, _vp, _vp, _vp, _vp, _i32,
                                   _vp, _vp, _vp, _vp], _i32),
 }

@@ -67,6 +67,44 @@ __device__ __forceinline__ void flag(int* st, int bit) { atomicOr(st, bit); }
 size_t scan_scratch_ints(long long n);
 int exclusive_scan_i32(Handle* h, const int* in, int* out, long long n, int* scratch);
 
+// patch row map (sweep_solve.cu): pmap[rows[k]] = k for the Robin patch rows
+void launch_patch_map(long long np, const int* rows, int* pmap, cudaStream_t s);
+
 }  // namespace emfem
 
 struct emfem_handle_s { emfem::Handle h; };
+
+// Auxiliary nodal space (aux_space.cu); the Krylov solver reads it directly.
+struct emfem_aux_s {
+    emfem::Handle* h = nullptr;
+    long long nn = 0, ne = 0, nf = 0, n = 0, na = 0, nnz_gt = 0, nnz_inc = 0;
+    int* gcol = nullptr;        // G rows, ELL [n][6]
+    double* gval = nullptr;
+    int* gt_ptr = nullptr;      // G^T, CSR [na + 1]
+    int* gt_row = nullptr;
+    double* gt_val = nullptr;
+    int* inc_ptr = nullptr;     // vertex-edge incidence graph, CSR [na + 1]
+    int* inc = nullptr;
+    float* inv_deg = nullptr;   // [na]
+    uint8_t* atype = nullptr;   // [na] 0 vertex, 1 edge
+    uint8_t* amask = nullptr;   // [na] usable (support entirely on free DOFs)
+    double2* dE = nullptr;      // [na] diag(G^T E G)
+    double2* dB = nullptr;      // [na] diag(G^T B G)
+    double2* dR = nullptr;      // [EMFEM_MAX_PORTS][na] diag(G^T R_p G)
+    int nports = 0;
+    bool have_operator = false;
+    float* params = nullptr;    // [EMFEM_MPNN_NPARAMS], caller-owned device memory
+    void* kbuf = nullptr;       // solve-time buffers (emfem_aux_reserve)
+    size_t kbuf_bytes = 0;
+};
+
+namespace emfem {
+template <typename T>
+int aux_correct(const emfem_aux_s* a, int S, bool learned, const T* dinv, const T* v, const uint8_t* mask, T* z,
+                cudaStream_t s);
+template <typename T>
+int aux_setup_dinv(const emfem_aux_s* a, int S, int nsys, const double* k0sq, const double* gamma, T* dinv,
+                   cudaStream_t s);
+size_t aux_solve_bytes(const emfem_aux_s* a, int S);
+void* aux_dinv_buffer(const emfem_aux_s* a, int S);
+}  // namespace emfem

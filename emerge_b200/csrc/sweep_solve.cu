@@ -626,6 +626,10 @@ __global__ void patch_map_kernel(long long np, const int* rows, int* patch_of_ro
     if (g < np) patch_of_row[rows[g]] = (int)g;
 }
 
+void launch_patch_map(long long np, const int* rows, int* pmap, cudaStream_t s) {
+    patch_map_kernel<<<grid_for(np, VB), VB, 0, s>>>(np, rows, pmap);
+}
+
 __global__ void pad_copy_kernel(long long n, int nsys, int S, const double2* __restrict__ src, double2* __restrict__ dst) {
     long long g = (long long)blockIdx.x * VB + threadIdx.x;
     if (g >= n * S) return;
@@ -716,6 +720,10 @@ struct Krylov {
     double2* partial = nullptr;
     SysState* st = nullptr;
     cudaStream_t s = nullptr;
+    // auxiliary-space correction (precond 3: aux Jacobi, 4: learned network); BiCGStab only
+    const emfem_aux_s* aux = nullptr;
+    T* adinv = nullptr;
+    int bj() const { return precond >= 3 ? 2 : precond; }
 
     unsigned nb_all() const { return grid_for(n * (long long)S, VB); }
     unsigned nb_pair() const { return grid_for(h * (long long)S, VB); }
@@ -748,10 +756,12 @@ struct Krylov {
             cocg_pupdate_kernel<R><<<nb_all(), VB, 0, s>>>(n, S, st, z, p);
         } else {
             T *rh = v[0], *p = v[1], *vv = v[2], *ph = v[3], *sh = v[4], *t = v[5];
-            bicg_p_kernel<R><<<nb_pair(), VB, 0, s>>>(h, S, precond, st, r, p, vv, ph, minv, rh);
+            bicg_p_kernel<R><<<nb_pair(), VB, 0, s>>>(h, S, bj(), st, r, p, vv, ph, minv, rh);
+            if (aux) EMFEM_TRY(aux_correct<T>(aux, S, precond == 4, adinv, p, op.mask, ph, s));
             spmv_kernel<R><<<nb_all(), VB, 0, s>>>(op, ph, vv, partial, DOT_CONJW_Y, rh);
             reduce(1, nb_all(), UPD_BICG_ALPHA);
-            bicg_s_kernel<R><<<nb_pair(), VB, 0, s>>>(h, S, precond, st, r, vv, sh, minv);
+            bicg_s_kernel<R><<<nb_pair(), VB, 0, s>>>(h, S, bj(), st, r, vv, sh, minv);
+            if (aux) EMFEM_TRY(aux_correct<T>(aux, S, precond == 4, adinv, r, op.mask, sh, s));
             spmv_kernel<R><<<nb_all(), VB, 0, s>>>(op, sh, t, partial, DOT_CONJY_W_YY, r);
             reduce(3, nb_all(), UPD_BICG_OMEGA);
             bicg_x_kernel<R><<<nb_all(), VB, 0, s>>>(n, S, st, x, r, ph, sh, t, rh, partial);
@@ -865,13 +875,17 @@ int emfem_krylov_solve(emfem_handle hd, int method, int64_t n, int64_t nnz, cons
                        const int32_t* patch_cols, const void* patch_vals, const int32_t* patch_port,
                        int n_ports, const double* gamma, const uint8_t* free_mask, const void* rhs, void* x,
                        double tol, int maxit, int precond, int precision, void* workspace, size_t workspace_bytes,
-                       int* status, int* iters, double* relres) {
+                       int* status, int* iters, double* relres, emfem_aux aux) {
     EMFEM_REQUIRE(hd && indptr && indices && E_vals && k0sq && free_mask && rhs && x && workspace,
                   "emfem_krylov_solve: null argument");
     EMFEM_REQUIRE(method == 0 || method == 1, "emfem_krylov_solve: method must be 0 (COCG) or 1 (BiCGStab)");
     EMFEM_REQUIRE(n > 0 && (n % 2) == 0, "emfem_krylov_solve: n must be even (DOF pairs i, i + n/2)");
     EMFEM_REQUIRE(nsys >= 1 && nsys <= 64, "emfem_krylov_solve: 1 <= nsys <= 64");
-    EMFEM_REQUIRE(precond >= 0 && precond <= 2 && (precision == 0 || precision == 1), "emfem_krylov_solve: bad option");
+    EMFEM_REQUIRE(precond >= 0 && precond <= 4 && (precision == 0 || precision == 1), "emfem_krylov_solve: bad option");
+    EMFEM_REQUIRE(precond < 3 || (aux && method == 1 && aux->n == n && aux->have_operator && aux->nports == n_ports),
+                  "emfem_krylov_solve: precond 3/4 need BiCGStab and an aux space of this field with its operator "
+                  "set (emfem_aux_set_operator, same ports)");
+    EMFEM_REQUIRE(precond != 4 || aux->params, "emfem_krylov_solve: precond 4 needs network parameters (emfem_aux_set_network)");
     EMFEM_REQUIRE(n_ports >= 0 && n_ports <= 8, "emfem_krylov_solve: at most 8 ports");
     EMFEM_REQUIRE(n_patch_rows == 0 || (patch_rows && patch_rowptr && patch_cols && patch_vals && patch_port && gamma),
                   "emfem_krylov_solve: patch arrays missing");
@@ -885,6 +899,8 @@ int emfem_krylov_solve(emfem_handle hd, int method, int64_t n, int64_t nnz, cons
         npatch = last;
     }
     EMFEM_REQUIRE(npatch <= nnz, "emfem_krylov_solve: more patch entries than nnz");
+    EMFEM_REQUIRE(precond < 3 || aux->kbuf_bytes >= aux_solve_bytes(aux, S),
+                  "emfem_krylov_solve: call emfem_aux_reserve with at least nsys systems first");
     Layout L = make_layout(n, nnz, npatch, S, n_ports, precision);
     size_t need = make_layout(n, nnz, nnz, S, 8, precision).total;
     if (workspace_bytes < need) {
@@ -952,8 +968,13 @@ int emfem_krylov_solve(emfem_handle hd, int method, int64_t n, int64_t nnz, cons
         for (int q = 0; q < 7; q++) k.v[q] = (double2*)(ws + L.off_v[q]);
         k.partial = partial; k.st = st; k.s = s;
         if (precond) {
-            precond_setup_kernel<double><<<grid_for((n / 2) * (long long)S, VB), VB, 0, s>>>(op64, precond, k.minv);
+            precond_setup_kernel<double><<<grid_for((n / 2) * (long long)S, VB), VB, 0, s>>>(op64, k.bj(), k.minv);
             STRY(check_cuda(cudaGetLastError(), "precond_setup"));
+        }
+        if (precond >= 3) {
+            k.aux = aux;
+            k.adinv = (double2*)aux_dinv_buffer(aux, S);
+            STRY(aux_setup_dinv<double2>(aux, S, nsys, k0dev, gdev, k.adinv, s));
         }
         // the recurrence tolerance is half the requested one so the FP64 true residual meets it
         reduce_update_kernel<<<S, VB, 0, s>>>(partial, (int)gv, S, 2, st, UPD_INIT, maxit, 0.5 * tol, nsys);
@@ -970,8 +991,13 @@ int emfem_krylov_solve(emfem_handle hd, int method, int64_t n, int64_t nnz, cons
         for (int q = 0; q < 6; q++) k.v[q] = (float2*)(ws + L.off_v[q]);
         k.partial = partial; k.st = st; k.s = s;
         if (precond) {
-            precond_setup_kernel<float><<<grid_for((n / 2) * (long long)S, VB), VB, 0, s>>>(op64, precond, k.minv);
+            precond_setup_kernel<float><<<grid_for((n / 2) * (long long)S, VB), VB, 0, s>>>(op64, k.bj(), k.minv);
             STRY(check_cuda(cudaGetLastError(), "precond_setup"));
+        }
+        if (precond >= 3) {
+            k.aux = aux;
+            k.adinv = (float2*)aux_dinv_buffer(aux, S);
+            STRY(aux_setup_dinv<float2>(aux, S, nsys, k0dev, gdev, k.adinv, s));
         }
         std::vector<SysState> ho(S);
         int used = 0;

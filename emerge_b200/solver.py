@@ -162,7 +162,7 @@ class SolverB200COCG(Solver):
             st = lib().emfem_krylov_solve(h.h, METHOD[self.method], n, c["nnz"], ptr(c["indptr"]), ptr(c["indices"]), ptr(c["vals"]), None,
                                         ns, k0, 0, None, None, None, None, None, 0, None, ptr(c["mask"]),
                                         ptr(rhs), ptr(x), self.tol, self.maxit, PRECOND[self.precond], prec,
-                                        ptr(ws), ws.numel(), status, iters, relres)
+                                        ptr(ws), ws.numel(), status, iters, relres, None)
             if st not in (0, ERR_NOT_CONVERGED):
                 check(st, "emfem_krylov_solve")
             out[:, c0:c0 + ns] = x.cpu().numpy()

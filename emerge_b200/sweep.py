@@ -28,7 +28,7 @@ from ._lib import Handle, check, lib, ptr, ERR_NOT_CONVERGED
 from .assembly import CsrPlan, DeviceMesh, dunavant4, tri_robin_device
 from .ports import k0_of
 
-PRECOND = {"none": 0, "jacobi": 1, "block_jacobi": 2}
+PRECOND = {"none": 0, "jacobi": 1, "block_jacobi": 2, "aux": 3, "learned": 4}
 PRECISION = {"fp64": 0, "mixed": 1}
 METHOD = {"cocg": 0, "bicgstab": 1}
 
@@ -100,6 +100,21 @@ class FrequencySweep:
         mask[problem.pec_ids] = 0
         self.mask = torch.from_numpy(mask).to(dev)
         self._ws = None
+        self._aux = None
+        self.network = None
+
+    def aux_space(self):
+        """The auxiliary nodal space of this mesh with this operator's diagonals (built once)."""
+        if self._aux is None:
+            from .auxspace import AuxSpace
+            self._aux = AuxSpace(self.problem.mesh, self.device)
+            self._aux.set_operator(self)
+        return self._aux
+
+    def set_network(self, net) -> None:
+        """Use this trained :class:`auxspace.Network` for ``precond="learned"``."""
+        self.network = net
+        self.aux_space().set_network(net.params if net is not None else None)
 
     def assemble(self):
         self.E, self.B = self.plan.assemble(self.er, self.ur, self.E, self.B)
@@ -256,6 +271,13 @@ class FrequencySweep:
         relres = (ctypes.c_double * nsys)()
         k0a = (ctypes.c_double * nsys)(*k0)
         ga = (ctypes.c_double * len(gam))(*gam)
+        aux = None
+        if PRECOND[precond] >= 3:
+            if precond == "learned" and self.network is None:
+                raise ValueError("precond='learned' needs a trained network (FrequencySweep.set_network)")
+            a = self.aux_space()
+            a.reserve(nsys)
+            aux = a.handle
         h = Handle.get(self.device)
         t0 = time.perf_counter()
         st = lib().emfem_krylov_solve(h.h, METHOD[method], self.n, self.plan.nnz, ptr(self.plan.indptr), ptr(self.plan.indices),
@@ -263,7 +285,7 @@ class FrequencySweep:
                                     self.patch_rows.numel(), ptr(self.patch_rows), ptr(self.patch_rowptr),
                                     ptr(self.patch_cols), ptr(self.patch_vals), ptr(self.patch_port), self.n_ports, ga,
                                     ptr(self.mask), ptr(b), ptr(x), tol, maxit, PRECOND[precond], prec,
-                                    ptr(ws), ws.numel(), status, iters, relres)
+                                    ptr(ws), ws.numel(), status, iters, relres, aux)
         dt = time.perf_counter() - t0
         if st not in (0, ERR_NOT_CONVERGED) or (raise_on_fail and st != 0):
             check(st, "emfem_krylov_solve")
@@ -276,11 +298,17 @@ class FrequencySweep:
         k0 = torch.from_numpy(self.k0sq(freqs)).to(self.device)
         g = self.gammas(freqs)
         gam = torch.from_numpy(np.ascontiguousarray(np.stack([g.real, g.imag], axis=-1).reshape(-1))).to(self.device)
+        S = 1 << (nsys - 1).bit_length()          # the kernel takes a power-of-two batch
+        if S != nsys:
+            pad = S - nsys
+            x = torch.cat([x, torch.zeros((x.shape[0], pad), dtype=x.dtype, device=x.device)], dim=1)
+            k0 = torch.cat([k0, k0[-1:].repeat(pad)])
+            gam = torch.cat([gam, gam[-2 * self.n_ports:].repeat(pad)]) if self.n_ports else gam
         y = torch.empty_like(x)
         h = Handle.get(self.device)
         check(lib().emfem_sweep_spmv(h.h, self.n, ptr(self.plan.indptr), ptr(self.plan.indices), ptr(self.E),
-                                     ptr(self.B), nsys, ptr(k0), self.patch_rows.numel(), ptr(self.patch_rows),
+                                     ptr(self.B), S, ptr(k0), self.patch_rows.numel(), ptr(self.patch_rows),
                                      ptr(self.patch_rowptr), ptr(self.patch_cols), ptr(self.patch_vals),
                                      ptr(self.patch_port), self.n_ports, ptr(gam), ptr(self.mask), ptr(x.contiguous()),
                                      ptr(y)), "emfem_sweep_spmv")
-        return y
+        return y[:, :nsys] if S != nsys else y

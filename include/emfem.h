@@ -36,8 +36,15 @@ extern "C" {
 #define EMFEM_DEV_CAPACITY 8
 #define EMFEM_DEV_BREAKDOWN 16
 
+/* Limits and sizes of the auxiliary-space preconditioner (emfem_aux_*, emfem_mpnn_*). */
+#define EMFEM_MAX_PORTS 8
+#define EMFEM_MPNN_CHANNELS 32   /* complex channels = 64 real */
+#define EMFEM_MPNN_LAYERS 4
+#define EMFEM_MPNN_NPARAMS (2 * 32 + 4 * 4 * 32 * 32 + 2 * 32)
+
 typedef struct emfem_handle_s *emfem_handle;
 typedef struct emfem_plan_s *emfem_plan;
+typedef struct emfem_aux_s *emfem_aux;
 typedef struct emfem_conn_s *emfem_conn;
 
 /* ---- library / handle ------------------------------------------------------------------- */
@@ -140,7 +147,12 @@ int emfem_sweep_combine(emfem_handle h, int64_t nnz, const void *E_vals, const v
  *   method:    0 = COCG (complex-symmetric A only), 1 = right-preconditioned BiCGStab (general A;
  *              the reference's mass matrix is not symmetric, so this is the default).
  *   precond:   0 none, 1 point Jacobi, 2 block Jacobi on DOF pairs (i, i + n/2) — the first- and
- *              second-kind DOFs of one edge/face (elements/nedelec2.py:42-58).
+ *              second-kind DOFs of one edge/face (elements/nedelec2.py:42-58); 3 block Jacobi plus
+ *              the auxiliary-space (discrete-gradient) correction with aux-space Jacobi, 4 block
+ *              Jacobi plus the correction through the learned network.  3 and 4 need method 1 and
+ *              `aux` (emfem_aux_create / _set_operator with the same ports / _reserve, and for 4
+ *              _set_network); `aux` is ignored (may be NULL) for precond 0-2.  The reference has no
+ *              preconditioner: it factorises directly.
  *   precision: 0 = FP64 Krylov; 1 = FP32 inner Krylov inside FP64 iterative refinement (FP64
  *              residual, solution update and convergence test).
  * Host outputs per system: status (0 converged, 1 iteration cap, 2 breakdown/stagnation), iters,
@@ -155,7 +167,7 @@ int emfem_krylov_solve(emfem_handle h, int method, int64_t n, int64_t nnz, const
                        const int32_t *patch_port, int n_ports, const double *gamma,
                        const uint8_t *free_mask, const void *rhs, void *x, double tol, int maxit,
                        int precond, int precision, void *workspace, size_t workspace_bytes,
-                       int *status, int *iters, double *relres);
+                       int *status, int *iters, double *relres, emfem_aux aux);
 
 /* y_s = A_s x_s for the operator of emfem_krylov_solve (FP64), eliminated rows/cols as there;
  * nsys a power of two <= 256; k0sq_dev and gamma_dev are device arrays. */
@@ -204,6 +216,63 @@ int emfem_mesh_connect_export(emfem_conn c, const double *nodes, const int64_t *
                               int64_t *tet_to_edge, int64_t *tet_to_tri, int64_t *tri_to_edge, int64_t *tri_to_tet,
                               double *edge_lengths);
 int emfem_mesh_connect_destroy(emfem_conn c);
+
+/* ---- auxiliary nodal space and learned preconditioner -----------------------------------------
+ * No counterpart in the reference (it factorises every system directly, solver.py:535-572).
+ * The aux space has one node per mesh vertex (aux id v) and per mesh edge (aux id n_nodes + e); G
+ * (n_field x n_aux) is the exact discrete gradient of the second-order nodal functions L_v and
+ * L_a L_b in the reference's Nedelec-2 basis (elements/ned2_interp.py:248-295), built per entity
+ * from edges (2, n_edges), tris (3, n_tris), tri_to_edge (3, n_tris) and edge_lengths (device,
+ * Mesh3D layouts).  The preconditioner of precond 3/4 is M r = BJ r + G N(D_a^-1 G^T r) with
+ * D_a = diag(G^T A_s G) per system and N the identity (3) or the network (4).
+ * create: builds G (ELL, 6 per row), G^T (CSR) and the vertex-edge incidence graph; synchronises.
+ * info: n_aux, nnz of G^T and of the graph.  export: device copies (any pointer may be NULL):
+ *   gcol (n_field, 6) i32 (-1 = empty), gval (n_field, 6) f64, G^T ptr/row/val, graph ptr/nbr.
+ * set_operator: the operator of emfem_krylov_solve (same arguments) -> diag(G^T E G), diag(G^T B G),
+ *   diag(G^T R_p G) and the aux mask (1 where every DOF touched is free).  diag_out (optional,
+ *   device): (2 + n_ports) * n_aux c128 [dE | dB | dR_0 ..]; mask_out (optional, device) n_aux u8.
+ * reserve: allocates the solve-time buffers for up to nsys systems (call before emfem_krylov_solve).
+ * set_network: device float params (EMFEM_MPNN_NPARAMS, layout below) used by precond 4; the
+ *   caller keeps them alive.
+ * dinv: dinv (n_aux, nsys) c128 = 1 / (dE - k0sq_s dB + sum_p gamma_{s,p} dR_p), 0 off the mask;
+ *   k0sq_dev (nsys) and gamma_dev (nsys * n_ports complex) device.
+ * restrict: x = dinv .* (G^T v) (dinv NULL: no scaling), v (n_field, nsys), x (n_aux, nsys) c128.
+ * prolong: z (+)= G za on rows with free_mask (NULL: all rows), c128. */
+int emfem_aux_create(emfem_handle h, int64_t n_nodes, int64_t n_edges, int64_t n_tris, const int64_t *edges,
+                     const int64_t *tris, const int64_t *tri_to_edge, const double *edge_lengths, emfem_aux *aux);
+int emfem_aux_info(emfem_aux aux, int64_t *n_aux, int64_t *nnz_gt, int64_t *nnz_graph);
+int emfem_aux_export(emfem_aux aux, int32_t *gcol, double *gval, int32_t *gt_ptr, int32_t *gt_row, double *gt_val,
+                     int32_t *graph_ptr, int32_t *graph_nbr);
+int emfem_aux_set_operator(emfem_aux aux, int64_t n, const int32_t *indptr, const int32_t *indices,
+                           const void *E_vals, const void *B_vals, int64_t n_patch_rows, const int32_t *patch_rows,
+                           const int32_t *patch_rowptr, const int32_t *patch_cols, const void *patch_vals,
+                           const int32_t *patch_port, int n_ports, const uint8_t *free_mask, void *diag_out,
+                           uint8_t *mask_out);
+int emfem_aux_reserve(emfem_aux aux, int nsys);
+int emfem_aux_set_network(emfem_aux aux, const float *params);
+int emfem_aux_destroy(emfem_aux aux);
+int emfem_aux_dinv(emfem_aux aux, int nsys, const double *k0sq_dev, const double *gamma_dev, void *dinv);
+int emfem_aux_restrict(emfem_aux aux, int nsys, const void *dinv, const void *v, void *x);
+int emfem_aux_prolong(emfem_aux aux, int nsys, const void *za, const uint8_t *free_mask, void *z, int accumulate);
+
+/* The network (training and inference kernels).  Aux-space vectors x, za are (n_aux, nsys) c64
+ * (FP32 complex); activations are FP32.  With t = 0 for vertex and 1 for edge aux nodes, N(y) the
+ * incidence-graph neighbours and real weights:
+ *   H_0 = x w_in[t];  H_{l+1,y} = H_{l,y} W_l[t_y] + (1/|N(y)|) sum_{j in N(y)} H_{l,j} U_l[t_y];
+ *   za_y = x_y + H_{4,y} . w_out[t_y]           (linear in x, so M stays a fixed linear operator)
+ * params (float): w_in[2][32] | (W_l[2][32][32] | U_l[2][32][32]) for l = 0..3 | w_out[2][32].
+ * workspace_floats: sizes of act (forward output, all layers) and scratch (backward).
+ * forward: za and act.  backward: grad (EMFEM_MPNN_NPARAMS floats, overwritten) of a real loss L
+ *   given dza = dL/dRe(za) + i dL/dIm(za) (c64), from the act of the forward of the same x; the
+ *   sums over nodes are fixed-order.  adam_step: one Adam update (bias-corrected, L2 weight decay
+ *   added to the gradient) of params with moments m, v (device, n floats); step >= 1. */
+int emfem_mpnn_nparams(void);
+int emfem_mpnn_workspace_floats(emfem_aux aux, int nsys, int64_t *activation_floats, int64_t *scratch_floats);
+int emfem_mpnn_forward(emfem_aux aux, int nsys, const float *params, const void *x, float *act, void *za);
+int emfem_mpnn_backward(emfem_aux aux, int nsys, const float *params, const void *x, const float *act,
+                        const void *dza, float *grad, float *scratch);
+int emfem_adam_step(emfem_handle h, int64_t n, float *params, const float *grad, float *m, float *v, float lr,
+                    float beta1, float beta2, float eps, float weight_decay, int step);
 
 /* ---- allocation-free sweep SpMV ------------------------------------------------------------
  * No counterpart in the reference.  The same y_s = A_s x_s as emfem_sweep_spmv, for callers that

@@ -97,7 +97,7 @@ def test_undersized_workspace_and_bad_options(cuda, prob):
     args = lambda nsys, wsb: (h.h, 1, sw.n, sw.plan.nnz, ptr(sw.plan.indptr), ptr(sw.plan.indices), ptr(sw.E),
                               ptr(sw.B), nsys, k0, sw.patch_rows.numel(), ptr(sw.patch_rows), ptr(sw.patch_rowptr),
                               ptr(sw.patch_cols), ptr(sw.patch_vals), ptr(sw.patch_port), sw.n_ports, gam,
-                              ptr(sw.mask), ptr(b), ptr(x), 1e-8, 100, 2, 0, ptr(ws), wsb, st, it, rr)
+                              ptr(sw.mask), ptr(b), ptr(x), 1e-8, 100, 2, 0, ptr(ws), wsb, st, it, rr, None)
     assert lib().emfem_krylov_solve(*args(1, ws.numel())) == _lib.ERR_WORKSPACE
     assert "workspace" in _lib.last_error()
     assert lib().emfem_krylov_solve(*args(65, ws.numel())) == _lib.ERR_INVALID_ARG

@@ -352,9 +352,9 @@ __global__ void __launch_bounds__(AB) mpnn_layer_kernel(long long na, int S, int
         sWout[k / NN_C][k % NN_C] = P[nn_off_wout() + k];
     }
     __syncthreads();
-    long long w = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     int lane = threadIdx.x & 31;
-    if (w >= na * S) return;
+    long long nw = (long long)gridDim.x * (blockDim.x >> 5);
+    for (long long w = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < na * S; w += nw) {
     long long y = w / S;
     int s = (int)(w % S);
     int t = atype[y];
@@ -402,6 +402,14 @@ __global__ void __launch_bounds__(AB) mpnn_layer_kernel(long long na, int S, int
             za[w] = r;
         }
     }
+    }
+}
+
+// persistent grid for the warp-per-row network kernels: the weights are staged once per block
+static unsigned warp_grid(long long rows) {
+    long long blocks = (rows + (AB / 32) - 1) / (AB / 32);
+    long long cap = 148LL * 8;
+    return (unsigned)(blocks < cap ? (blocks > 0 ? blocks : 1) : cap);
 }
 
 // Hstore non-null: every layer's output is kept (training); else layers alternate H0/H1 and the
@@ -410,7 +418,7 @@ template <typename TX>
 int mpnn_forward(const emfem_aux_s* a, int S, const float* P, const TX* x, float2* H0, float2* H1, float2* Hstore,
                  TX* za, cudaStream_t s) {
     long long na = a->na;
-    unsigned grid = grid_for(na * S * 32, AB);
+    unsigned grid = warp_grid(na * S);
     const float2* hin = nullptr;
     for (int l = 0; l < NN_L; l++) {
         float2* hout = Hstore ? Hstore + (size_t)l * na * S * NN_C : ((l % 2 == 0) ? H0 : H1);
@@ -441,22 +449,23 @@ __global__ void __launch_bounds__(AB) mpnn_bwd_dm_kernel(long long na, int S, in
         sU[t][r][c] = P[nn_off_U(layer) + k];
     }
     __syncthreads();
-    long long w = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     int lane = threadIdx.x & 31;
-    if (w >= na * S) return;
-    long long y = w / S;
-    int t = atype[y];
-    float2 d = dOut[w * NN_C + lane];
-    float2 o = make_float2(0.f, 0.f);
+    long long nw = (long long)gridDim.x * (blockDim.x >> 5);
+    for (long long w = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < na * S; w += nw) {
+        long long y = w / S;
+        int t = atype[y];
+        float2 d = dOut[w * NN_C + lane];
+        float2 o = make_float2(0.f, 0.f);
 #pragma unroll 8
-    for (int c = 0; c < NN_C; c++) {
-        float dx = __shfl_sync(0xffffffffu, d.x, c), dy = __shfl_sync(0xffffffffu, d.y, c);
-        float u = sU[t][lane][c];
-        o.x += u * dx;
-        o.y += u * dy;
+        for (int c = 0; c < NN_C; c++) {
+            float dx = __shfl_sync(0xffffffffu, d.x, c), dy = __shfl_sync(0xffffffffu, d.y, c);
+            float u = sU[t][lane][c];
+            o.x += u * dx;
+            o.y += u * dy;
+        }
+        float idg = inv_deg[y];
+        dM[w * NN_C + lane] = make_float2(o.x * idg, o.y * idg);
     }
-    float idg = inv_deg[y];
-    dM[w * NN_C + lane] = make_float2(o.x * idg, o.y * idg);
 }
 
 __global__ void __launch_bounds__(AB) mpnn_bwd_din_kernel(long long na, int S, int layer, const float* __restrict__ P,
@@ -470,27 +479,28 @@ __global__ void __launch_bounds__(AB) mpnn_bwd_din_kernel(long long na, int S, i
         sW[t][r][c] = P[nn_off_W(layer) + k];
     }
     __syncthreads();
-    long long w = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     int lane = threadIdx.x & 31;
-    if (w >= na * S) return;
-    long long y = w / S;
-    int s = (int)(w % S);
-    int t = atype[y];
-    float2 d = dOut[w * NN_C + lane];
-    float2 o = make_float2(0.f, 0.f);
+    long long nw = (long long)gridDim.x * (blockDim.x >> 5);
+    for (long long w = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < na * S; w += nw) {
+        long long y = w / S;
+        int s = (int)(w % S);
+        int t = atype[y];
+        float2 d = dOut[w * NN_C + lane];
+        float2 o = make_float2(0.f, 0.f);
 #pragma unroll 8
-    for (int c = 0; c < NN_C; c++) {
-        float dx = __shfl_sync(0xffffffffu, d.x, c), dy = __shfl_sync(0xffffffffu, d.y, c);
-        float wv = sW[t][lane][c];
-        o.x += wv * dx;
-        o.y += wv * dy;
+        for (int c = 0; c < NN_C; c++) {
+            float dx = __shfl_sync(0xffffffffu, d.x, c), dy = __shfl_sync(0xffffffffu, d.y, c);
+            float wv = sW[t][lane][c];
+            o.x += wv * dx;
+            o.y += wv * dy;
+        }
+        for (int k = nptr[y]; k < nptr[y + 1]; k++) {
+            float2 m = dM[((long long)nbr[k] * S + s) * NN_C + lane];
+            o.x += m.x;
+            o.y += m.y;
+        }
+        dIn[w * NN_C + lane] = o;
     }
-    for (int k = nptr[y]; k < nptr[y + 1]; k++) {
-        float2 m = dM[((long long)nbr[k] * S + s) * NN_C + lane];
-        o.x += m.x;
-        o.y += m.y;
-    }
-    dIn[w * NN_C + lane] = o;
 }
 
 template <typename TX>
@@ -924,7 +934,7 @@ int emfem_mpnn_backward(emfem_aux a, int nsys, const float* params, const void* 
     float2* dIn = dM + actn;
     float* partial = (float*)(dIn + actn);
     const float2* A = (const float2*)act;
-    unsigned gw = grid_for(rows * 32, AB);
+    unsigned gw = warp_grid(rows);
     mpnn_bwd_out_kernel<float2><<<grid_for(rows * NN_C, AB), AB, 0, s>>>(na, nsys, params, a->atype,
                                                                          (const float2*)dza, dOut);
     // w_out gradient from dza and the last layer's output, before dOut is overwritten

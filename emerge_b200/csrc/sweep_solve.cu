@@ -728,7 +728,10 @@ struct Krylov {
     unsigned nb_all() const { return grid_for(n * (long long)S, VB); }
     unsigned nb_pair() const { return grid_for(h * (long long)S, VB); }
 
-    double restart_eps = sizeof(R) == 8 ? 1e-9 : 1e-4;
+    // restart BiCGStab's shadow residual only when (r_hat, r) is at the rounding level of the
+    // vectors' precision (the dots accumulate in FP64); a looser FP32 threshold restarts so often
+    // that the Krylov memory is lost
+    double restart_eps = sizeof(R) == 8 ? 1e-9 : 1e-6;
     void reduce(int ncomp, unsigned nblocks, int mode) {
         reduce_update_kernel<<<S, VB, 0, s>>>(partial, (int)nblocks, S, ncomp, st, mode, maxit, restart_eps, nsys);
     }

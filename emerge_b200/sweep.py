@@ -62,6 +62,7 @@ class SolveResult:
     relres: np.ndarray
     systems: list
     seconds: float
+    fallbacks: int = 0       # systems re-solved by a fallback method
 
 
 def sparam_corrections(S: np.ndarray, col: bool = True, single: bool = True, recip: bool = False) -> np.ndarray:
@@ -252,10 +253,43 @@ class FrequencySweep:
             self._ws = torch.empty(sz.value, dtype=torch.uint8, device=self.device)
         return self._ws
 
+    FALLBACK = {("learned", "mixed"): [("learned", "fp64"), ("aux", "fp64"), ("block_jacobi", "fp64")],
+                ("learned", "fp64"): [("aux", "fp64"), ("block_jacobi", "fp64")],
+                ("aux", "mixed"): [("aux", "fp64"), ("block_jacobi", "fp64")],
+                ("aux", "fp64"): [("block_jacobi", "fp64")],
+                ("block_jacobi", "mixed"): [("block_jacobi", "fp64")]}
+
     def solve(self, systems, tol: float = 1e-8, maxit: int = 20000, precond: str = "block_jacobi",
               precision: str = "fp64", method: str = "bicgstab", x0: torch.Tensor | None = None,
-              raise_on_fail: bool = False) -> SolveResult:
-        """Solve the listed (frequency, port index) systems in one batched Krylov call (<= 64)."""
+              raise_on_fail: bool = False, fallback: bool = False) -> SolveResult:
+        """Solve the listed (frequency, port index) systems in one batched Krylov call (<= 64).
+
+        With ``fallback``, systems that miss the tolerance are solved again, warm-started from where
+        they stopped, by the next entry of ``FALLBACK[(precond, precision)]`` (learned -> aux-space
+        Jacobi -> plain block Jacobi, mixed -> FP64); the FP64 true residual decides.  ``iters`` and
+        ``seconds`` then include every attempt, and ``fallbacks`` counts the systems re-solved."""
+        res = self._solve(systems, tol, maxit, precond, precision, method, x0, raise_on_fail and not fallback)
+        if not fallback:
+            return res
+        for pc, pr in self.FALLBACK.get((precond, precision), []):
+            bad = np.flatnonzero(res.status != 0)
+            if len(bad) == 0:
+                break
+            if pc == "learned" and self.network is None:
+                continue
+            sub = [systems[j] for j in bad]
+            r2 = self._solve(sub, tol, maxit, pc, pr, method, res.x[:, bad].contiguous(), False)
+            res.x[:, bad] = r2.x
+            res.status[bad] = r2.status
+            res.iters[bad] += r2.iters
+            res.relres[bad] = r2.relres
+            res.seconds += r2.seconds
+            res.fallbacks += len(bad)
+        if raise_on_fail and (res.status != 0).any():
+            raise RuntimeError(f"not converged after fallbacks: status {res.status}")
+        return res
+
+    def _solve(self, systems, tol, maxit, precond, precision, method, x0, raise_on_fail) -> SolveResult:
         nsys = len(systems)
         assert 1 <= nsys <= 64
         freqs = [f for f, _ in systems]

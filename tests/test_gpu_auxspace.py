@@ -142,4 +142,12 @@ def test_training_reduces_correction_loss_and_learned_solve_converges(guide, gol
     for j, key in enumerate(("x1", "x2")):
         gx = g[key]
         assert np.linalg.norm(x[:, j] - gx) / np.linalg.norm(gx) <= 1e-8
+    # what the trained preconditioner gains over the method without it (plain block Jacobi) at a
+    # frequency outside the training set: the same systems to 1e-8 in a fraction of the iterations
+    held_sys = [(10.5e9, 0), (10.5e9, 1)]
+    plain = sw.solve(held_sys, tol=1e-8, maxit=40000, precond="block_jacobi")
+    learned = sw.solve(held_sys, tol=1e-8, maxit=40000, precond="learned", fallback=True)
+    assert (plain.status == 0).all() and (learned.status == 0).all()
+    assert learned.fallbacks == 0
+    assert learned.iters.max() * 4 < plain.iters.max(), (learned.iters, plain.iters)
     sw.set_network(None)

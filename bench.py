@@ -210,9 +210,12 @@ def train_network(P, train_freqs, steps: int = 300) -> tuple:
     held = make_pairs(sw, [(float(0.5 * (train_freqs[0] + train_freqs[1])), 0)], snapshots=(16, 64))
     t_pairs = time.perf_counter() - t0
     net = Network(aux, seed=0)
-    rep = train(net, sw, pairs, heldout=held, steps=steps, batch=8, lr=2e-3)
+    val = [(float(0.5 * (train_freqs[2] + train_freqs[3])), q) for q in range(len(P.ports))]
+    rep = train(net, sw, pairs, heldout=held, steps=steps, batch=8, lr=2e-3, validate=val)
     torch.cuda.synchronize()
     return net, {"pairs": rep.pairs, "pair_seconds": t_pairs, "steps": rep.steps, "train_seconds": rep.seconds,
+                 "validation_iters_aux_jacobi": rep.validation_iters_aux,
+                 "validation_iters_learned": rep.validation_iters_learned, "accepted": rep.accepted,
                  "loss_first": rep.loss_first, "loss_last": rep.loss_last,
                  "heldout_loss_aux_jacobi": rep.loss_jacobi_heldout, "heldout_loss_learned": rep.loss_learned_heldout,
                  "objective": "mean ||G za - e||^2 / ||e||^2 over (residual, correction) pairs"}

@@ -13,7 +13,7 @@ from __future__ import annotations
 
 import numpy as np
 
-from .assembly import assemble_robin_bc_excited, dunavant4, tet_mass_stiffness_matrices
+from .assembly import assemble_robin_bc, assemble_robin_bc_excited, dunavant4, tet_mass_stiffness_matrices
 from .ports import k0_of
 
 
@@ -48,7 +48,7 @@ class Assembler:
         self.cached_matrices = None
 
     def assemble_freq_matrix(self, field, er: np.ndarray, ur: np.ndarray, ports, pec_tris: np.ndarray,
-                             frequency: float, cache_matrices: bool = False, device=None) -> SimJob:
+                             frequency: float, cache_matrices: bool = False, device=None, robin_bcs=()) -> SimJob:
         K0 = k0_of(frequency)
         if cache_matrices and self.cached_matrices is not None:
             E, B = self.cached_matrices
@@ -59,7 +59,7 @@ class Assembler:
         b = np.zeros(E.shape[0], dtype=np.complex128)
         port_vectors = {p.port_number: np.zeros(E.shape[0], dtype=np.complex128) for p in ports}
         pec_ids = field.pec_dofs(pec_tris) if len(pec_tris) else np.zeros(0, dtype=np.int64)
-        if len(ports):
+        if len(ports) or len(robin_bcs):
             dpts = dunavant4()
             Bempty = field.empty_tri_matrix()
             for p in ports:
@@ -67,6 +67,9 @@ class Assembler:
                                                         lambda x, y, z, p=p: p.get_Uinc(x, y, z, K0),
                                                         p.get_gamma(K0), dpts, device=device)
                 port_vectors[p.port_number] += b_p
+            # non-excited Robin boundaries (absorbing, surface impedance): ASM/assembler.py:338-339
+            for bc in robin_bcs:
+                Bempty = assemble_robin_bc(field, Bempty, bc.tri_ids, bc.get_gamma(K0), device=device)
             K = K + field.generate_csr(Bempty)
         job = SimJob(K, b, K0 * 299792458 / (2 * np.pi), True)
         job.port_vectors = port_vectors

@@ -220,6 +220,9 @@ class TrainReport:
     loss_jacobi_heldout: float = float("nan")
     loss_learned_heldout: float = float("nan")
     history: list = field(default_factory=list)
+    validation_iters_aux: int = -1        # total iterations on the validation systems, aux Jacobi
+    validation_iters_learned: int = -1    # same with the trained network
+    accepted: bool = True                 # False: the network was reset to the aux Jacobi (w_out = 0)
 
 
 def make_pairs(sweep, systems, snapshots=(8, 24, 64), tol: float = 1e-10, maxit: int = 20000):
@@ -263,8 +266,14 @@ def _loss_and_grad(net: Network, aux: AuxSpace, sweep, batch, need_grad: bool = 
 
 
 def train(net: Network, sweep, pairs, heldout=None, steps: int = 200, batch: int = 8, lr: float = 1e-3,
-          seed: int = 0, log_every: int = 20) -> TrainReport:
-    """Adam on the correction loss over random minibatches of pairs (all on the GPU)."""
+          seed: int = 0, log_every: int = 20, validate=None, tol: float = 1e-8, margin: float = 1.05) -> TrainReport:
+    """Adam on the correction loss over random minibatches of pairs (all on the GPU).
+
+    With ``validate`` (a list of held-out (frequency, port) systems), the trained network is solved
+    against the aux-space Jacobi it started from; if it needs more than ``margin`` times the
+    iterations, its output weights are reset to zero, which makes it exactly the aux-space Jacobi,
+    and ``accepted`` is False.  The correction loss does not always predict Krylov iterations on
+    these indefinite systems, so this keeps a training run from ever slowing the solve down."""
     aux = net.aux
     rng = np.random.default_rng(seed)
     rep = TrainReport(pairs=len(pairs))
@@ -285,4 +294,14 @@ def train(net: Network, sweep, pairs, heldout=None, steps: int = 200, batch: int
         jac = Network(aux, init="jacobi")
         rep.loss_jacobi_heldout = float(np.mean([_loss_and_grad(jac, aux, sweep, [p], False)[0] for p in heldout]))
         rep.loss_learned_heldout = float(np.mean([_loss_and_grad(net, aux, sweep, [p], False)[0] for p in heldout]))
+    if validate:
+        prev = sweep.network
+        rep.validation_iters_aux = int(sweep.solve(validate, tol=tol, maxit=40000, precond="aux").iters.sum())
+        sweep.set_network(net)
+        r = sweep.solve(validate, tol=tol, maxit=40000, precond="learned")
+        rep.validation_iters_learned = int(r.iters.sum()) if (r.status == 0).all() else 1 << 30
+        sweep.set_network(prev)
+        if rep.validation_iters_learned > margin * rep.validation_iters_aux:
+            net.params[-2 * CHANNELS:] = 0.0
+            rep.accepted = False
     return rep

@@ -285,7 +285,19 @@ __global__ void aux_restrict_kernel(long long na, int S, const int* __restrict__
     long long y = g / S;
     int s = (int)(g % S);
     double ar = 0, ai = 0;
-    for (int k = gt_ptr[y]; k < gt_ptr[y + 1]; k++) {
+    int k = gt_ptr[y], ke = gt_ptr[y + 1];
+    for (; k + 4 <= ke; k += 4) {        // loads of four entries in flight, summed in order
+        int rr[4];
+        double gv[4];
+        TV vv[4];
+#pragma unroll
+        for (int u = 0; u < 4; u++) { rr[u] = gt_row[k + u]; gv[u] = gt_val[k + u]; }
+#pragma unroll
+        for (int u = 0; u < 4; u++) vv[u] = v[(long long)rr[u] * S + s];
+#pragma unroll
+        for (int u = 0; u < 4; u++) { ar += gv[u] * (double)vv[u].x; ai += gv[u] * (double)vv[u].y; }
+    }
+    for (; k < ke; k++) {
         double gv = gt_val[k];
         TV vv = v[(long long)gt_row[k] * S + s];
         ar += gv * (double)vv.x;

@@ -115,7 +115,33 @@ __global__ void __launch_bounds__(VB) spmv_kernel(OpArgs a, const typename V2<R>
             const double2* Bv = (const double2*)a.B;
             double er = 0, ei = 0, br = 0, bi = 0;
             int jb = a.indptr[i], je = a.indptr[i + 1];
-            for (int j = jb; j < je; j++) {
+            int j = jb;
+            // four entries' loads are issued before their products are summed (in column order, so
+            // the sums are the same as the one-at-a-time loop): the row walk is latency-bound
+            for (; j + 4 <= je; j += 4) {
+                int cc[4];
+                T xv[4];
+                double2 e[4], b[4];
+#pragma unroll
+                for (int u = 0; u < 4; u++) cc[u] = a.indices[j + u];
+#pragma unroll
+                for (int u = 0; u < 4; u++) {
+                    xv[u] = x[(long long)cc[u] * S + s];
+                    e[u] = Ev[j + u];
+                    b[u] = Bv ? Bv[j + u] : make_double2(0.0, 0.0);
+                }
+#pragma unroll
+                for (int u = 0; u < 4; u++) {
+                    double xr = xv[u].x, xi = xv[u].y;
+                    er += e[u].x * xr - e[u].y * xi;
+                    ei += e[u].x * xi + e[u].y * xr;
+                    if (Bv) {
+                        br += b[u].x * xr - b[u].y * xi;
+                        bi += b[u].x * xi + b[u].y * xr;
+                    }
+                }
+            }
+            for (; j < je; j++) {
                 int c = a.indices[j];
                 T xv = x[(long long)c * S + s];
                 double xr = xv.x, xi = xv.y;

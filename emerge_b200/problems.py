@@ -10,7 +10,7 @@ configurations (no public dataset is involved; meshes come from :func:`mesh.box_
 """
 from __future__ import annotations
 
-from dataclasses import dataclass
+from dataclasses import dataclass, field
 
 import numpy as np
 
@@ -30,6 +30,7 @@ class Problem:
     pec_tris: np.ndarray
     freqs: np.ndarray
     dims: tuple
+    robin: list = field(default_factory=list)   # non-excited Robin boundaries (boundaries.py)
 
     @property
     def pec_ids(self) -> np.ndarray:

@@ -128,7 +128,10 @@ class FrequencySweep:
         N = self.n
         blocks_all, meta_rows, meta_cols, meta_port = [], [], [], []
         self.bhat = []
-        nports = len(P.ports)
+        robin = list(getattr(P, "robin", []) or [])
+        nports = len(P.ports) + len(robin)
+        if nports > 8:
+            raise ValueError("at most 8 ports + Robin boundaries per sweep")
         off = 0
         for q, port in enumerate(P.ports):
             tid = np.asarray(port.tri_ids, dtype=np.int64)
@@ -151,6 +154,17 @@ class FrequencySweep:
             bh[torch.from_numpy(ud).to(dev)] = vals
             self.bhat.append(bh)
             off += len(rows)
+        # non-excited Robin boundaries: R̂ with γ = 1 (no excitation), as extra patch "ports"
+        for r, bc in enumerate(robin):
+            q = len(P.ports) + r
+            tid = np.asarray(bc.tri_ids, dtype=np.int64)
+            tn = mesh.tris[:, tid]
+            blocks, _ = tri_robin_device(self.dmesh, torch.from_numpy(np.ascontiguousarray(tn)).to(dev), 1.0)
+            t2f = fld.tri_to_field[:, tid]
+            blocks_all.append(blocks.reshape(-1))
+            meta_rows.append(np.repeat(t2f.T, 8, axis=1).ravel())
+            meta_cols.append(np.tile(t2f.T, (1, 8)).ravel())
+            meta_port.append(np.full(8 * 8 * len(tid), q))
         rows = np.concatenate(meta_rows); cols = np.concatenate(meta_cols); port = np.concatenate(meta_port)
         src = torch.cat(blocks_all)
         keys = (rows * nports + port) * N + cols
@@ -234,8 +248,9 @@ class FrequencySweep:
         return np.array([k0_of(f) ** 2 for f in freqs])
 
     def gammas(self, freqs) -> np.ndarray:
-        """(nsys, n_ports) complex γ of every port at every frequency."""
-        return np.array([[complex(p.get_gamma(k0_of(f))) for p in self.problem.ports] for f in freqs])
+        """(nsys, n_ports) complex γ of every port, then every non-excited Robin boundary, at every frequency."""
+        bcs = list(self.problem.ports) + list(getattr(self.problem, "robin", []) or [])
+        return np.array([[complex(p.get_gamma(k0_of(f))) for p in bcs] for f in freqs])
 
     def rhs(self, systems) -> torch.Tensor:
         """(N, nsys) right-hand sides b + port_vector[p] (``MW/simjob.py:88-92``, b = 0)."""

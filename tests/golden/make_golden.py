@@ -26,6 +26,11 @@ Fixtures
     serves the nodes and tets and reports no surface/edge entities: edges, tris, tet_to_edge,
     tet_to_tri, tri_to_edge, tri_to_tet and edge_lengths.
 
+``robin_gamma.npz``    γ(k0) of the reference's ``AbsorbingBoundary`` (order 1, and order 2 types A-E:
+    ``MW/microwave_bc.py:282-346``) and ``SurfaceImpedance`` (bulk conductor, finite thickness,
+    roughness, user impedance function: ``:1243-1343``) over 2-40 GHz, the objects built without their
+    geometry (only the attributes ``get_gamma`` reads are set).
+
 Fixtures can be generated one at a time: ``python tests/golden/make_golden.py mesh_conn``.
 
 ``ASM/`` = ``src/emerge/_emerge/physics/microwave/assembly/``; ``MW/`` = ``src/emerge/_emerge/physics/microwave/``.
@@ -248,8 +253,54 @@ def mesh_conn():
     np.savez_compressed(os.path.join(HERE, "mesh_conn.npz"), **out)
 
 
+def robin_gamma():
+    class _Scalar:
+        def __init__(self, v):
+            self.v = v
+
+        def scalar(self, f):
+            return self.v
+
+    class _Mat:
+        def __init__(self, er, ur, cond):
+            self.er, self.ur, self.cond = _Scalar(er), _Scalar(ur), _Scalar(cond)
+
+    freqs = np.array([2e9, 5.5e9, 10e9, 24e9, 40e9])
+    k0s = 2 * np.pi * freqs / K.C0
+    out = {"k0": k0s}
+    abc = object.__new__(R.bc.AbsorbingBoundary)
+    abc.o2coeffs = {'A': (1.0, -0.5), 'B': (1.00023, -0.51555), 'C': (1.03084, -0.73631),
+                    'D': (1.06103, -0.84883), 'E': (1.12500, -1.00000)}
+    abc.order = 1
+    abc.abctype = 'B'
+    out["abc1"] = np.array([abc.get_gamma(k) for k in k0s])
+    abc.order = 2
+    for t in "ABCDE":
+        abc.abctype = t
+        out["abc2_" + t] = np.array([abc.get_gamma(k) for k in k0s])
+    cases = [dict(sigma=5.8e7, thickness=None, sr=0.0, mur=1.0, er=1.0),
+             dict(sigma=3.5e7, thickness=2e-6, sr=0.0, mur=1.0, er=1.0),
+             dict(sigma=5.8e7, thickness=None, sr=1.2e-6, mur=1.0, er=1.0),
+             dict(sigma=1.0e6, thickness=5e-7, sr=3e-7, mur=1.5, er=2.0)]
+    for i, c in enumerate(cases):
+        si = object.__new__(R.bc.SurfaceImpedance)
+        si._Zf = None
+        si.sigma = c["sigma"]
+        si.thickness = c["thickness"]
+        si._sr = c["sr"]
+        si._sr_model = 'Hammerstad-Jensen'
+        si._material = _Mat(c["er"], c["mur"], c["sigma"])
+        out[f"surf{i}"] = np.array([si.get_gamma(k) for k in k0s])
+        out[f"surf{i}_params"] = np.array([c["sigma"], -1.0 if c["thickness"] is None else c["thickness"], c["sr"],
+                                           c["mur"], c["er"]])
+    si = object.__new__(R.bc.SurfaceImpedance)
+    si._Zf = lambda f: (0.02 + 1e-12 * f) + 1j * (0.01 + 3e-12 * f)
+    out["surf_fn"] = np.array([si.get_gamma(k) for k in k0s])
+    np.savez_compressed(os.path.join(HERE, "robin_gamma.npz"), **out)
+
+
 if __name__ == "__main__":
-    which = sys.argv[1:] or ["element_small", "config1", "mesh_conn"]
+    which = sys.argv[1:] or ["element_small", "config1", "mesh_conn", "robin_gamma"]
     if "element_small" in which:
         m, f = element_small()
         robin_small(m, f)
@@ -257,6 +308,8 @@ if __name__ == "__main__":
         config1()
     if "mesh_conn" in which:
         mesh_conn()
+    if "robin_gamma" in which:
+        robin_gamma()
     for fn in sorted(os.listdir(HERE)):
         if fn.endswith(".npz"):
             print(fn, os.path.getsize(os.path.join(HERE, fn)))

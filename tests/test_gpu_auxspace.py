@@ -126,13 +126,18 @@ def test_network_forward_backward_vs_oracle(guide):
 def test_training_reduces_correction_loss_and_learned_solve_converges(guide, golden):
     P, sw = guide
     aux = sw.aux_space()
-    train_sys = [(f, q) for f in (8.5e9, 9.5e9, 11e9) for q in (0, 1)]
-    pairs = make_pairs(sw, train_sys, snapshots=(8, 32))
-    held = make_pairs(sw, [(10.5e9, 0)], snapshots=(16,))
+    train_sys = [(f, q) for f in np.linspace(8.125e9, 11.875e9, 9) for q in (0, 1)]
+    pairs = make_pairs(sw, train_sys, snapshots=(4, 16, 48, 128))
+    held = make_pairs(sw, [(10.5e9, 0)], snapshots=(16, 64))
     net = Network(aux, seed=0)
-    rep = train(net, sw, pairs, heldout=held, steps=60, batch=4, lr=2e-3)
+    rep = train(net, sw, pairs, heldout=held, steps=300, batch=8, lr=2e-3, validate=[(9.3e9, 0), (9.3e9, 1)])
     assert rep.loss_last < rep.loss_first
-    assert rep.loss_learned_heldout <= rep.loss_jacobi_heldout * 1.001, rep
+    # the training objective generalises to held-out pairs ...
+    assert rep.loss_learned_heldout < rep.loss_jacobi_heldout, rep
+    # ... and validation keeps the solve no slower than the aux Jacobi the network started from
+    assert rep.validation_iters_aux > 0 and rep.validation_iters_learned > 0
+    if not rep.accepted:
+        assert float(net.params[-64:].abs().max()) == 0.0
     sw.set_network(net)
     g = golden("config1")
     f = float(g["f"])

@@ -86,3 +86,46 @@ def test_solver_plugin_through_solve_routine(cuda, golden):
         assert rep.exit_code == 0, rep.aux
         gx = g[key]
         assert np.linalg.norm(x - gx) / np.linalg.norm(gx) <= 1e-10
+
+
+@pytest.mark.parametrize("kind", ["abc", "surface"])
+def test_sweep_with_robin_boundaries_matches_superlu(cuda, kind):
+    """Non-excited Robin boundaries in the device sweep (an absorbing boundary in place of the
+    second port; a conducting surface-impedance wall in place of a PEC wall) vs the oracle's
+    assembly with assemble_robin_bc and SuperLU."""
+    from emerge_b200.boundaries import AbsorbingBoundary, SurfaceImpedance
+    P = problems.waveguide()
+    m = P.mesh
+    a, b, l = P.dims
+    if kind == "abc":
+        P.robin = [AbsorbingBoundary(P.ports[1].tri_ids)]
+        P.ports = P.ports[:1]
+    else:
+        wall = m.tris_on_plane(1, b)
+        P.pec_tris = np.setdiff1d(P.pec_tris, wall)
+        P.robin = [SurfaceImpedance(wall, sigma=1.0e5, roughness=1e-6)]
+    sw = FrequencySweep(P)
+    f = 10e9
+    sysl = [(f, q) for q in range(len(P.ports))]
+    res = sw.solve(sysl, tol=1e-12, maxit=60000, precond="aux")
+    assert (res.status == 0).all(), (res.status, res.iters, res.relres)
+    k0 = k0_of(f)
+    E, B = oracle.tet_mass_stiffness_matrices(P.field, P.er, P.ur)
+    K = (E - B * k0 ** 2).tocsr()
+    Bm = P.field.empty_tri_matrix()
+    pvs = []
+    for p in P.ports:
+        Bm, bp = oracle.assemble_robin_bc_excited(P.field, Bm, p.tri_ids, lambda x, y, z, p=p: p.get_Uinc(x, y, z, k0),
+                                                  p.get_gamma(k0), oracle.dunavant4())
+        pvs.append(bp)
+    for bc in P.robin:
+        Bm = oracle.assemble_robin_bc(P.field, Bm, bc.tri_ids, bc.get_gamma(k0))
+    K = K + P.field.generate_csr(Bm)
+    xs = oracle.solve_routine(K, pvs, P.solve_ids)
+    x = res.x.cpu().numpy()
+    for j in range(len(P.ports)):
+        assert np.linalg.norm(x[:, j] - xs[j]) / np.linalg.norm(xs[j]) <= 1e-10
+    # the drop-in assembler with the same boundaries gives the same K
+    job = Assembler().assemble_freq_matrix(P.field, P.er, P.ur, P.ports, P.pec_tris, f, robin_bcs=P.robin)
+    d = (job.A - K).tocsr()
+    assert (abs(d).max() if d.nnz else 0.0) <= 1e-12 * abs(K).max()

@@ -216,6 +216,8 @@ def train_network(P, train_freqs, steps: int = 300) -> tuple:
     return net, {"pairs": rep.pairs, "pair_seconds": t_pairs, "steps": rep.steps, "train_seconds": rep.seconds,
                  "validation_iters_aux_jacobi": rep.validation_iters_aux,
                  "validation_iters_learned": rep.validation_iters_learned, "accepted": rep.accepted,
+                 "output_scale": rep.output_scale,
+                 "validation_iters_by_output_scale": {str(k): v for k, v in rep.validation_by_scale.items()},
                  "loss_first": rep.loss_first, "loss_last": rep.loss_last,
                  "heldout_loss_aux_jacobi": rep.loss_jacobi_heldout, "heldout_loss_learned": rep.loss_learned_heldout,
                  "objective": "mean ||G za - e||^2 / ||e||^2 over (residual, correction) pairs"}

@@ -221,7 +221,9 @@ class TrainReport:
     loss_learned_heldout: float = float("nan")
     history: list = field(default_factory=list)
     validation_iters_aux: int = -1        # total iterations on the validation systems, aux Jacobi
-    validation_iters_learned: int = -1    # same with the trained network
+    validation_iters_learned: int = -1    # same with the kept network
+    validation_by_scale: dict = field(default_factory=dict)   # output scale -> validation iterations
+    output_scale: float = 1.0             # factor applied to w_out after validation
     accepted: bool = True                 # False: the network was reset to the aux Jacobi (w_out = 0)
 
 
@@ -266,14 +268,16 @@ def _loss_and_grad(net: Network, aux: AuxSpace, sweep, batch, need_grad: bool = 
 
 
 def train(net: Network, sweep, pairs, heldout=None, steps: int = 200, batch: int = 8, lr: float = 1e-3,
-          seed: int = 0, log_every: int = 20, validate=None, tol: float = 1e-8, margin: float = 1.05) -> TrainReport:
+          seed: int = 0, log_every: int = 20, validate=None, tol: float = 1e-8,
+          scales=(1.0, 0.5, 0.25)) -> TrainReport:
     """Adam on the correction loss over random minibatches of pairs (all on the GPU).
 
-    With ``validate`` (a list of held-out (frequency, port) systems), the trained network is solved
-    against the aux-space Jacobi it started from; if it needs more than ``margin`` times the
-    iterations, its output weights are reset to zero, which makes it exactly the aux-space Jacobi,
-    and ``accepted`` is False.  The correction loss does not always predict Krylov iterations on
-    these indefinite systems, so this keeps a training run from ever slowing the solve down."""
+    With ``validate`` (a list of held-out (frequency, port) systems), the learned term is scaled by
+    each factor in ``scales`` (its output weights w_out times the factor) and by 0, which is
+    exactly the aux-space Jacobi the network started from.  Each variant solves the validation systems,
+    and the variant with the fewest iterations is kept.  ``accepted`` is False when that variant is 0.
+    The correction loss does not always predict Krylov iterations on these indefinite systems, so
+    this selection keeps a training run from ever slowing the solve down."""
     aux = net.aux
     rng = np.random.default_rng(seed)
     rep = TrainReport(pairs=len(pairs))
@@ -297,11 +301,17 @@ def train(net: Network, sweep, pairs, heldout=None, steps: int = 200, batch: int
     if validate:
         prev = sweep.network
         rep.validation_iters_aux = int(sweep.solve(validate, tol=tol, maxit=40000, precond="aux").iters.sum())
+        rep.validation_by_scale[0.0] = rep.validation_iters_aux
+        w_out = net.params[-2 * CHANNELS:].clone()
         sweep.set_network(net)
-        r = sweep.solve(validate, tol=tol, maxit=40000, precond="learned")
-        rep.validation_iters_learned = int(r.iters.sum()) if (r.status == 0).all() else 1 << 30
+        for a in scales:
+            net.params[-2 * CHANNELS:] = w_out * a
+            r = sweep.solve(validate, tol=tol, maxit=40000, precond="learned")
+            rep.validation_by_scale[float(a)] = int(r.iters.sum()) if (r.status == 0).all() else 1 << 30
         sweep.set_network(prev)
-        if rep.validation_iters_learned > margin * rep.validation_iters_aux:
-            net.params[-2 * CHANNELS:] = 0.0
-            rep.accepted = False
+        best = min(rep.validation_by_scale, key=lambda k: (rep.validation_by_scale[k], k))
+        net.params[-2 * CHANNELS:] = w_out * best
+        rep.output_scale = best
+        rep.accepted = best > 0.0
+        rep.validation_iters_learned = rep.validation_by_scale[best]
     return rep

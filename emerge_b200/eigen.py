@@ -1,0 +1,87 @@
+"""Eigenmodes of the Nédélec-2 operator with device inner solves.
+
+Replaces the reference's eigenmode path: ``Assembler.assemble_eig_matrix`` (``ASM/assembler.py:431-600``:
+E, B with PEC elimination) solved by shift-invert ARPACK, ``eigs(A, k, M=B, sigma=k_t², which="LM")``
+(``SolverARPACK.eig``, ``src/emerge/_emerge/solver.py:820-833``).  The reference factorises
+A − σB inside SciPy; here ARPACK (SciPy, on the host, as in the reference) is given the inverse as an
+operator whose every application is a device BiCGStab solve of (E − σB) y = x, preconditioned by the
+auxiliary-space correction (σ plays the role of k0²), and the mass products B x run on the device too.
+Only closed (PEC) cavities are handled: the reference adds Robin terms to B (``:512-538``), which
+this path does not.
+
+``ASM/`` = ``src/emerge/_emerge/physics/microwave/assembly/``.
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass
+
+import numpy as np
+import torch
+from scipy.sparse.linalg import LinearOperator, eigs
+
+from ._lib import Handle, check, lib, ptr
+from .constants import C0
+
+__all__ = ["EigenResult", "eigenmodes"]
+
+
+@dataclass
+class EigenResult:
+    k0sq: np.ndarray          # eigenvalues λ = k0², sorted by distance to σ
+    freqs: np.ndarray         # resonance frequencies (Hz) of the real part of λ
+    modes: np.ndarray         # (N, nmodes) complex, zero on PEC DOFs
+    inner_solves: int
+    inner_iters: int
+
+
+def eigenmodes(sweep, nmodes: int = 4, target_k0: float = 1.0, tol: float = 1e-10, maxit: int = 40000,
+               precond: str = "aux", arpack_tol: float = 0.0) -> EigenResult:
+    """The ``nmodes`` eigenpairs of E x = λ B x nearest σ = target_k0² on the free DOFs of a
+    closed-cavity ``FrequencySweep`` (no ports, no Robin boundaries)."""
+    if sweep.n_ports:
+        raise ValueError("eigenmodes: closed cavities only (the sweep has ports or Robin boundaries)")
+    dev = sweep.device
+    free = torch.nonzero(sweep.mask, as_tuple=False).reshape(-1)
+    nf = free.numel()
+    N = sweep.n
+    sigma = float(target_k0) ** 2
+    stats = {"solves": 0, "iters": 0}
+    h = Handle.get(dev)
+    one = torch.zeros(1, dtype=torch.float64, device=dev)
+    nog = torch.zeros(2, dtype=torch.float64, device=dev)
+
+    def full(xf: np.ndarray) -> torch.Tensor:
+        x = torch.zeros((N, 1), dtype=torch.complex128, device=dev)
+        x[free, 0] = torch.from_numpy(np.ascontiguousarray(xf, dtype=np.complex128)).to(dev)
+        return x
+
+    def mass(xf):
+        x = full(xf)
+        y = torch.empty_like(x)
+        # y = B x through the sweep SpMV with B as its first operator and no second one
+        check(lib().emfem_sweep_spmv(h.h, N, ptr(sweep.plan.indptr), ptr(sweep.plan.indices), ptr(sweep.B), None, 1,
+                                     ptr(one), 0, None, None, None, None, None, 0, ptr(nog), ptr(sweep.mask),
+                                     ptr(x), ptr(y)), "emfem_sweep_spmv")
+        return y[free, 0].cpu().numpy()
+
+    def opinv(xf):
+        res = sweep.solve_rhs([sigma], full(xf), tol=tol, maxit=maxit, precond=precond)
+        stats["solves"] += 1
+        stats["iters"] += int(res.iters.sum())
+        if (res.status != 0).any():
+            raise RuntimeError(f"eigenmodes: inner solve at sigma={sigma:.6g} did not converge "
+                               f"(relres {res.relres.max():.2e} after {res.iters.max()} iterations)")
+        return res.x[free, 0].cpu().numpy()
+
+    def stiff(xf):
+        raise RuntimeError("not used in shift-invert mode")
+
+    A = LinearOperator((nf, nf), matvec=stiff, dtype=np.complex128)
+    M = LinearOperator((nf, nf), matvec=mass, dtype=np.complex128)
+    OPinv = LinearOperator((nf, nf), matvec=opinv, dtype=np.complex128)
+    vals, vecs = eigs(A, k=nmodes, M=M, sigma=sigma, which="LM", OPinv=OPinv, tol=arpack_tol)
+    order = np.argsort(np.abs(vals - sigma))
+    vals, vecs = vals[order], vecs[:, order]
+    modes = np.zeros((N, nmodes), dtype=np.complex128)
+    modes[free.cpu().numpy()] = vecs
+    return EigenResult(vals, np.sqrt(np.abs(vals.real)) * C0 / (2 * np.pi), modes, stats["solves"], stats["iters"])

@@ -86,3 +86,15 @@ def cavity(n=40, L=0.1, seed=0, jitter=0.1, nblocks=8, nfreq=101, fmin=2e9, fmax
                             mesh.tris_on_plane(1, L), mesh.tris_on_plane(2, L)])
     return Problem("cavity", mesh, fld, er, identity_tensors(nt), ports, walls,
                    np.linspace(fmin, fmax, nfreq), (L, L, L))
+
+
+def pec_cavity(nx=8, ny=4, nz=12, a=22.86e-3, b=10.16e-3, d=30e-3, seed=0, jitter=0.1) -> Problem:
+    """Air-filled rectangular box with PEC on all six faces and no ports (eigenmode workload)."""
+    nodes, tets = box_tet_mesh(nx, ny, nz, a, b, d, jitter=jitter, seed=seed)
+    mesh = TetMesh(nodes, tets)
+    fld = Nedelec2(mesh)
+    nt = mesh.n_tets
+    walls = np.concatenate([mesh.tris_on_plane(ax, v) for ax, v in ((0, 0.0), (0, a), (1, 0.0), (1, b),
+                                                                      (2, 0.0), (2, d))])
+    return Problem("pec_cavity", mesh, fld, identity_tensors(nt), identity_tensors(nt), [], walls,
+                   np.zeros(0), (a, b, d))

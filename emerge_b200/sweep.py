@@ -165,6 +165,15 @@ class FrequencySweep:
             meta_rows.append(np.repeat(t2f.T, 8, axis=1).ravel())
             meta_cols.append(np.tile(t2f.T, (1, 8)).ravel())
             meta_port.append(np.full(8 * 8 * len(tid), q))
+        if not meta_rows:                     # no ports and no Robin boundaries (a closed cavity)
+            i32 = dict(dtype=torch.int32, device=dev)
+            self.patch_vals = torch.zeros(0, dtype=torch.complex128, device=dev)
+            self.patch_rows = torch.zeros(0, **i32)
+            self.patch_rowptr = torch.zeros(1, **i32)
+            self.patch_cols = torch.zeros(0, **i32)
+            self.patch_port = torch.zeros(0, **i32)
+            self.n_ports = 0
+            return
         rows = np.concatenate(meta_rows); cols = np.concatenate(meta_cols); port = np.concatenate(meta_port)
         src = torch.cat(blocks_all)
         keys = (rows * nports + port) * N + cols
@@ -305,13 +314,24 @@ class FrequencySweep:
         return res
 
     def _solve(self, systems, tol, maxit, precond, precision, method, x0, raise_on_fail) -> SolveResult:
-        nsys = len(systems)
-        assert 1 <= nsys <= 64
         freqs = [f for f, _ in systems]
-        k0 = self.k0sq(freqs)
-        g = self.gammas(freqs)
+        return self.solve_rhs(self.k0sq(freqs), self.rhs(systems), self.gammas(freqs), tol=tol, maxit=maxit,
+                              precond=precond, precision=precision, method=method, x0=x0,
+                              raise_on_fail=raise_on_fail, systems=systems)
+
+    def solve_rhs(self, k0sq, b: torch.Tensor, gammas=None, tol: float = 1e-8, maxit: int = 20000,
+                  precond: str = "block_jacobi", precision: str = "fp64", method: str = "bicgstab",
+                  x0: torch.Tensor | None = None, raise_on_fail: bool = False, systems=None) -> SolveResult:
+        """(E - k0sq_s B + sum_p gammas[s, p] R_p) x_s = b_s for arbitrary right-hand sides b (N, nsys)
+        on the free DOFs (gammas default 0: the Robin terms drop out)."""
+        b = b.to(device=self.device, dtype=torch.complex128).contiguous()
+        nsys = b.shape[1]
+        assert 1 <= nsys <= 64
+        k0 = np.asarray(k0sq, dtype=np.float64).reshape(-1)
+        g = np.zeros((nsys, self.n_ports), dtype=np.complex128) if gammas is None else np.asarray(gammas)
         gam = np.ascontiguousarray(np.stack([g.real, g.imag], axis=-1).reshape(-1))
-        b = self.rhs(systems)
+        if gam.size == 0:
+            gam = np.zeros(2)
         x = torch.zeros_like(b) if x0 is None else x0.clone().contiguous()
         prec = PRECISION[precision]
         ws = self.workspace(nsys, prec)
@@ -338,7 +358,8 @@ class FrequencySweep:
         dt = time.perf_counter() - t0
         if st not in (0, ERR_NOT_CONVERGED) or (raise_on_fail and st != 0):
             check(st, "emfem_krylov_solve")
-        return SolveResult(x, np.array(status[:]), np.array(iters[:]), np.array(relres[:]), list(systems), dt)
+        return SolveResult(x, np.array(status[:]), np.array(iters[:]), np.array(relres[:]),
+                           list(systems) if systems is not None else [], dt)
 
     def apply(self, systems, x: torch.Tensor) -> torch.Tensor:
         """y = K_f x for each system (FP64; PEC rows/cols eliminated)."""

@@ -29,6 +29,8 @@ sys.path.insert(0, ROOT)
 METRIC = "Nedelec-2 tets assembled/s"
 UNIT = "tets/s"
 L2_BYTES = 126 * 2 ** 20
+# assemble_chunk_kernel DRAM traffic per tet, ncu capture at 82 944 tets: (686 + 178) MB / 82 944
+ASM_TRAFFIC_PER_TET = (686e6 + 178e6) / 82944
 
 
 def peaks():
@@ -420,7 +422,11 @@ def main():
             "vs_baseline": None, "dtype": "c128", "data": "synthetic",
             "config": workload_config(P),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                         "frac": achieved / hbm, "traffic": None, "peak_kind": peak_kind,
+                         "frac": achieved / hbm, "traffic": ASM_TRAFFIC_PER_TET * nt,
+                         "traffic_note": "bytes per launch of assemble_chunk_kernel: dram read+write per tet from the "
+                                         "ncu capture at 82 944 tets (profiles/assemble_chunk_kernel_cavity24.md) "
+                                         "scaled by tets; the invariants kernel adds ~1.4 KB/tet",
+                         "peak_kind": peak_kind,
                          "alg_bytes_per_tet": alg_bytes_per_tet, "kernels": "tet_invariants_kernel+assemble_kernel"},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
                     "api": "emerge_b200.assembly.tet_mass_stiffness_matrices (host numpy in, SciPy CSR out)"},

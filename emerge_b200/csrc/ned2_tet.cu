@@ -356,7 +356,10 @@ struct ChunkSmem {
     static constexpr size_t total = off_ent + (size_t)(2 * CH + 2) * 4;
 };
 
-template <int CH, int NT, int MINB, bool SINV>
+// LM (incidence-major): consecutive threads take the 6 edge columns, then the 4 face columns, of one
+// incidence before the next, so a warp's invariant loads fall on a few tets' records (few L1
+// wavefronts).  Otherwise consecutive threads take one column of 32 incidences (32 records).
+template <int CH, int NT, int MINB, bool SINV, bool LM>
 __global__ void __launch_bounds__(NT, MINB) assemble_chunk_kernel(
     const int* __restrict__ chunk_ptr, long long H, const int* __restrict__ mptr,
     const int* __restrict__ inc_ptr, const uint32_t* __restrict__ inc_code, const uint4* __restrict__ rec,
@@ -396,9 +399,16 @@ __global__ void __launch_bounds__(NT, MINB) assemble_chunk_kernel(
     __syncthreads();
     VTab T{vtab};
     const int npad = (ninc + 31) & ~31;
-    for (int w = threadIdx.x; w < 10 * npad; w += NT) {
-        int sy = w / npad, li = w - sy * npad;
-        if (li >= ninc) continue;
+    const int nwork = LM ? 10 * ninc : 10 * npad;
+    for (int w = threadIdx.x; w < nwork; w += NT) {
+        int sy, li;
+        if (LM) {
+            if (w < 6 * ninc) { li = w / 6; sy = w - 6 * li; }
+            else { int u = w - 6 * ninc; li = u >> 2; sy = 6 + (u & 3); }
+        } else {
+            sy = w / npad; li = w - sy * npad;
+            if (li >= ninc) continue;
+        }
         int sx = (int)((srec[li].z >> 16) & 0xff);  // byte 10 of the record
         InvView I = SINV ? InvView{sinv + li * INV_SMEM_STRIDE, 1}
                          : InvView{inv + (long long)(scode[li] >> 4) * INV_STRIDE, 1};
@@ -445,22 +455,30 @@ __global__ void __launch_bounds__(NT, MINB) assemble_chunk_kernel(
 // shared memory or read through L1.  The plan times them and keeps the fastest.
 struct AsmVariant { int ch; int nt; size_t smem; };
 #define EMFEM_ASM_VARIANTS(X)              \
-    X(0, 32, 160, 2, true)                 \
-    X(1, 32, 160, 4, false)                \
-    X(2, 64, 320, 1, true)                 \
-    X(3, 16, 128, 5, false)                \
-    X(4, 32, 160, 3, false)                \
-    X(5, 64, 320, 2, false)
-constexpr int N_ASM_VARIANTS = 6;
-#define EMFEM_V_ENTRY(i, ch, nt, mb, si) {ch, nt, ChunkSmem<ch, si>::total},
+    X(0, 32, 160, 2, true, false)          \
+    X(1, 32, 160, 4, false, false)         \
+    X(2, 64, 320, 1, true, false)          \
+    X(3, 16, 128, 5, false, false)         \
+    X(4, 32, 160, 3, false, false)         \
+    X(5, 64, 320, 2, false, false)         \
+    X(6, 64, 320, 2, false, true)          \
+    X(7, 32, 160, 4, false, true)          \
+    X(8, 32, 160, 3, false, true)          \
+    X(9, 64, 320, 1, true, true)           \
+    X(10, 64, 256, 2, false, true)         \
+    X(11, 32, 128, 4, false, true)         \
+    X(12, 64, 192, 3, false, true)
+constexpr int N_ASM_VARIANTS = 13;
+constexpr int DEFAULT_ASM_VARIANT = 6;
+#define EMFEM_V_ENTRY(i, ch, nt, mb, si, lm) {ch, nt, ChunkSmem<ch, si>::total},
 static const AsmVariant ASM_VARIANTS[N_ASM_VARIANTS] = {EMFEM_ASM_VARIANTS(EMFEM_V_ENTRY)};
 
 static void launch_asm_variant(int v, unsigned grid, cudaStream_t s, const int* chunk_ptr, long long H, const int* mptr,
                                const int* inc_ptr, const uint32_t* inc_code, const uint4* rec, const double* inv,
                                double2* E, double2* B) {
     switch (v) {
-#define EMFEM_V_LAUNCH(i, ch, nt, mb, si) \
-    case i: assemble_chunk_kernel<ch, nt, mb, si><<<grid, nt, ASM_VARIANTS[i].smem, s>>>(chunk_ptr, H, mptr, inc_ptr, inc_code, rec, inv, E, B); break;
+#define EMFEM_V_LAUNCH(i, ch, nt, mb, si, lm) \
+    case i: assemble_chunk_kernel<ch, nt, mb, si, lm><<<grid, nt, ASM_VARIANTS[i].smem, s>>>(chunk_ptr, H, mptr, inc_ptr, inc_code, rec, inv, E, B); break;
         EMFEM_ASM_VARIANTS(EMFEM_V_LAUNCH)
     default: break;
     }
@@ -468,8 +486,8 @@ static void launch_asm_variant(int v, unsigned grid, cudaStream_t s, const int* 
 
 static cudaError_t set_asm_smem_attributes() {
     cudaError_t e = cudaSuccess;
-#define EMFEM_V_ATTR(i, ch, nt, mb, si) \
-    if (e == cudaSuccess) e = cudaFuncSetAttribute(assemble_chunk_kernel<ch, nt, mb, si>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ASM_VARIANTS[i].smem);
+#define EMFEM_V_ATTR(i, ch, nt, mb, si, lm) \
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(assemble_chunk_kernel<ch, nt, mb, si, lm>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ASM_VARIANTS[i].smem);
     EMFEM_ASM_VARIANTS(EMFEM_V_ATTR)
     return e;
 }
@@ -653,6 +671,8 @@ int emfem_plan_create(emfem_handle h, int64_t n_tets, int64_t n_edges, int64_t n
             PTRY(check_cuda(cudaStreamSynchronize(s), "sync"));
             if (p->variant < 0) p->variant = v;
         }
+        // default: the incidence-major 64/320 variant (fastest measured on B200) when it fits
+        if (p->variant >= 0 && p->n_chunks[DEFAULT_ASM_VARIANT] > 0) p->variant = DEFAULT_ASM_VARIANT;
         if (p->variant < 0) {
             set_error("emfem_plan_create: an edge or face is shared by %d tets (at most 64 supported)", maxdeg);
             st = EMFEM_ERR_INVALID_ARG;

@@ -34,6 +34,11 @@ __device__ __forceinline__ T mk2(R x, R y) { T v; v.x = x; v.y = y; return v; }
 
 constexpr int VB = 256;  // threads per block for vector/SpMV kernels
 
+// relative tolerance of each FP32 inner solve in the mixed-precision refinement (compile-time)
+#ifndef EMFEM_INNER_TOL
+#define EMFEM_INNER_TOL 1e-4
+#endif
+
 struct OpArgs {
     long long n;
     int S;                          // padded systems (power of two, divides VB)
@@ -1038,7 +1043,7 @@ int emfem_krylov_solve(emfem_handle hd, int method, int64_t n, int64_t nnz, cons
             if (!any || used >= maxit) break;
             to_f32_scaled_kernel<<<gv, VB, 0, s>>>(n, S, r64, st_outer, r32, scale);
             STRY(check_cuda(cudaMemsetAsync(d32, 0, sizeof(float2) * nS, s), "memset d"));
-            inner_init_kernel<<<1, 64, 0, s>>>(st, st_outer, S, 1e-4);
+            inner_init_kernel<<<1, 64, 0, s>>>(st, st_outer, S, EMFEM_INNER_TOL);
             k.maxit = std::max(1, maxit - used);
             STRY(k.start());
             STRY(k.run(16));

@@ -109,3 +109,47 @@ def test_iteration_cap_reports_not_converged(cuda, prob):
     assert (res.status == 1).all()
     assert (res.iters <= 4).all()
     assert np.isfinite(res.relres).all() and (res.relres > 1e-12).all()
+
+
+def test_aux_preconditioner_misuse_is_rejected(cuda, prob):
+    """The aux-space and learned preconditioners refuse to run without their set-up, and a bad
+    edge list is caught by the device check, all as status codes."""
+    sw = FrequencySweep(prob)
+    b = sw.rhs([(10e9, 0)])
+    x = torch.zeros_like(b)
+    sz = ctypes.c_size_t()
+    lib().emfem_krylov_workspace_size(sw.n, sw.plan.nnz, 1, 0, ctypes.byref(sz))
+    ws = torch.empty(sz.value, dtype=torch.uint8, device=b.device)
+    st, it, rr = (ctypes.c_int * 1)(), (ctypes.c_int * 1)(), (ctypes.c_double * 1)()
+    k0 = (ctypes.c_double * 1)(sw.k0sq([10e9])[0])
+    g = sw.gammas([10e9])
+    gam = (ctypes.c_double * 4)(*np.stack([g.real, g.imag], -1).ravel())
+    h = Handle.get()
+
+    def call(precond, method, aux):
+        return lib().emfem_krylov_solve(h.h, method, sw.n, sw.plan.nnz, ptr(sw.plan.indptr), ptr(sw.plan.indices),
+                                        ptr(sw.E), ptr(sw.B), 1, k0, sw.patch_rows.numel(), ptr(sw.patch_rows),
+                                        ptr(sw.patch_rowptr), ptr(sw.patch_cols), ptr(sw.patch_vals),
+                                        ptr(sw.patch_port), sw.n_ports, gam, ptr(sw.mask), ptr(b), ptr(x), 1e-8, 50,
+                                        precond, 0, ptr(ws), ws.numel(), st, it, rr, aux)
+
+    assert call(3, 1, None) == _lib.ERR_INVALID_ARG              # no aux space
+    from emerge_b200.auxspace import AuxSpace
+    aux = AuxSpace(prob.mesh)
+    assert call(3, 1, aux.handle) == _lib.ERR_INVALID_ARG        # no operator set yet
+    aux.set_operator(sw)
+    assert call(3, 1, aux.handle) == _lib.ERR_INVALID_ARG        # buffers not reserved
+    aux.reserve(1)
+    assert call(3, 0, aux.handle) == _lib.ERR_INVALID_ARG        # COCG with the aux correction
+    assert call(4, 1, aux.handle) == _lib.ERR_INVALID_ARG        # learned without parameters
+    assert call(3, 1, aux.handle) in (0, _lib.ERR_NOT_CONVERGED)  # properly set up: runs
+    # an edge with an out-of-range node id is caught by the device check
+    bad = prob.mesh.edges.copy()
+    bad[1, 3] = prob.mesh.n_nodes + 7
+
+    class M:
+        nodes, edges, tris = prob.mesh.nodes, bad, prob.mesh.tris
+        tri_to_edge, edge_lengths = prob.mesh.tri_to_edge, prob.mesh.edge_lengths
+    with pytest.raises(EmfemError):
+        AuxSpace(M)
+    AuxSpace(prob.mesh)                                           # the handle stays usable

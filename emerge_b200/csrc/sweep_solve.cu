@@ -121,6 +121,54 @@ __global__ void __launch_bounds__(VB) spmv_kernel(OpArgs a, const typename V2<R>
             double er = 0, ei = 0, br = 0, bi = 0;
             int jb = a.indptr[i], je = a.indptr[i + 1];
             int j = jb;
+            if (S >= 32) {
+                // a warp holds 32 systems of one row: it stages 32 consecutive (column, E, B) entries
+                // with one coalesced load per lane and reads them back as shared-memory broadcasts;
+                // the products are summed in column order as below
+                __shared__ int s_c[VB / 32][32];
+                __shared__ double2 s_e[VB / 32][32], s_b[VB / 32][32];
+                const int wl = threadIdx.x >> 5, lane = threadIdx.x & 31;
+                for (int base = jb; base < je; base += 32) {
+                    int jj = base + lane;
+                    if (jj < je) {
+                        s_c[wl][lane] = a.indices[jj];
+                        s_e[wl][lane] = Ev[jj];
+                        s_b[wl][lane] = Bv ? Bv[jj] : make_double2(0.0, 0.0);
+                    }
+                    __syncwarp();
+                    const int cnt = min(32, je - base);
+                    int u = 0;
+                    for (; u + 4 <= cnt; u += 4) {
+                        T xv[4];
+#pragma unroll
+                        for (int t = 0; t < 4; t++) xv[t] = x[(long long)s_c[wl][u + t] * S + s];
+#pragma unroll
+                        for (int t = 0; t < 4; t++) {
+                            double2 e = s_e[wl][u + t], b = s_b[wl][u + t];
+                            double xr = xv[t].x, xi = xv[t].y;
+                            er += e.x * xr - e.y * xi;
+                            ei += e.x * xi + e.y * xr;
+                            if (Bv) {
+                                br += b.x * xr - b.y * xi;
+                                bi += b.x * xi + b.y * xr;
+                            }
+                        }
+                    }
+                    for (; u < cnt; u++) {
+                        T xv = x[(long long)s_c[wl][u] * S + s];
+                        double2 e = s_e[wl][u], b = s_b[wl][u];
+                        double xr = xv.x, xi = xv.y;
+                        er += e.x * xr - e.y * xi;
+                        ei += e.x * xi + e.y * xr;
+                        if (Bv) {
+                            br += b.x * xr - b.y * xi;
+                            bi += b.x * xi + b.y * xr;
+                        }
+                    }
+                    __syncwarp();
+                }
+                j = je;
+            }
             // four entries' loads are issued before their products are summed (in column order, so
             // the sums are the same as the one-at-a-time loop): the row walk is latency-bound
             for (; j + 4 <= je; j += 4) {

@@ -13,7 +13,8 @@ from __future__ import annotations
 
 import numpy as np
 
-from .assembly import assemble_robin_bc, assemble_robin_bc_excited, dunavant4, tet_mass_stiffness_matrices
+from .assembly import (abc_order_2_matrix, assemble_robin_bc, assemble_robin_bc_excited, dunavant4,
+                       tet_mass_stiffness_matrices)
 from .ports import k0_of
 
 
@@ -70,6 +71,8 @@ class Assembler:
             # non-excited Robin boundaries (absorbing, surface impedance): ASM/assembler.py:338-339
             for bc in robin_bcs:
                 Bempty = assemble_robin_bc(field, Bempty, bc.tri_ids, bc.get_gamma(K0), device=device)
+                if getattr(bc, "order", 1) == 2:        # second-order ABC correction (ASM/assembler.py:342-347)
+                    Bempty = Bempty + abc_order_2_matrix(field, bc.tri_ids, bc.get_gamma2(K0), device=device)
             K = K + field.generate_csr(Bempty)
         job = SimJob(K, b, K0 * 299792458 / (2 * np.pi), True)
         job.port_vectors = port_vectors

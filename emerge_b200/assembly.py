@@ -26,7 +26,8 @@ from . import _lib
 from ._lib import Handle, check, lib, ptr
 
 __all__ = ["DeviceMesh", "CsrPlan", "tet_mass_stiffness_matrices", "_matrix_builder",
-           "assemble_robin_bc", "assemble_robin_bc_excited", "tri_robin_device", "dunavant4"]
+           "assemble_robin_bc", "assemble_robin_bc_excited", "tri_robin_device", "dunavant4",
+           "tri_abc2_device", "abc_order_2_matrix"]
 
 
 def _device(device=None) -> torch.device:
@@ -346,3 +347,30 @@ def assemble_robin_bc(field, Bmat: np.ndarray, surf_triangle_indices, gamma, dev
     """Robin matrix blocks without excitation (``ASM/robinbc.py:465-473``); ``Bmat`` updated in place."""
     _robin_host(field, Bmat, surf_triangle_indices, gamma, None, None, device)
     return Bmat
+
+
+def tri_abc2_device(dmesh: DeviceMesh, tri_nodes: torch.Tensor, cf: complex) -> torch.Tensor:
+    """Second-order ABC correction blocks (n_sel, 64) of the triangles tri_nodes (3, n_sel)."""
+    dev = dmesh.device
+    tri_nodes = tri_nodes.to(dev, torch.int64).contiguous()
+    ns = tri_nodes.shape[1]
+    blocks = torch.empty((ns, 64), dtype=torch.complex128, device=dev)
+    h = Handle.get(dev)
+    c = complex(cf)
+    check(lib().emfem_ned2_tri_abc2(h.h, dmesh.n_nodes, ptr(dmesh.nodes), ns, ptr(tri_nodes), c.real, c.imag,
+                                    ptr(blocks)), "emfem_ned2_tri_abc2")
+    h.raise_on_device_status("emfem_ned2_tri_abc2")
+    return blocks
+
+
+def abc_order_2_matrix(field, surf_triangle_indices, coeff, device=None) -> np.ndarray:
+    """The reference's ``abc_order_2_matrix`` (``ASM/robin_abc_order2.py:350-373``): the flat
+    (N_f·64,) array with the listed triangles' second-order ABC blocks, computed on the GPU."""
+    dev = _device(device)
+    dm, _ = _plan_for(field, dev)
+    tid = np.asarray(surf_triangle_indices, dtype=np.int64)
+    out = np.zeros(field.mesh.n_tris * 64, dtype=np.complex128)
+    if len(tid):
+        blocks = tri_abc2_device(dm, _to_dev(field.mesh.tris[:, tid], torch.int64, dev), coeff).cpu().numpy()
+        np.add.at(out.reshape(-1, 64), tid, blocks)
+    return out

@@ -5,8 +5,9 @@ Every Robin boundary enters the system as γ(k0) · R̂ with R̂ the triangle ma
 only γ differs), so the frequency sweep treats them as extra non-excited "ports".
 
 * :class:`AbsorbingBoundary` — ``MW/microwave_bc.py:282-346``: γ = j k0 (order 1), or j k0 c0 with the
-  order-2 coefficient table when ``order == 2``.  The order-2 correction matrix
-  (``abc_order_2_matrix``, ``ASM/robin_abc_order2.py:192-373``) is not built, so order 2 is rejected.
+  order-2 coefficient table (the reference's default, ``order=2``, type B) plus the tangential
+  correction matrix ``abc_order_2_matrix`` scaled by j c2 / k0 (``ASM/assembler.py:342-347``,
+  ``ASM/robin_abc_order2.py:192-373``; device kernel ``emfem_ned2_tri_abc2``).
 * :class:`SurfaceImpedance` — ``MW/microwave_bc.py:1243-1343``: γ = j k0 Z0 / Z_s with the skin-depth
   surface impedance of a conductor σ, optional finite thickness (coth) and Hammerstad–Jensen roughness,
   or a user impedance function Z_s(f).
@@ -32,16 +33,19 @@ ABC_O2_COEFFS = {"A": (1.0, -0.5), "B": (1.00023, -0.51555), "C": (1.03084, -0.7
 @dataclass
 class AbsorbingBoundary:
     tri_ids: np.ndarray
-    order: int = 1
+    order: int = 2
     abctype: str = "B"
 
     def __post_init__(self):
         if self.order not in (1, 2):
             raise ValueError("AbsorbingBoundary: order must be 1 or 2")
-        if self.order == 2:
-            raise NotImplementedError("AbsorbingBoundary order 2 needs the second-order correction matrix, "
-                                      "which this package does not build; use order=1")
+        if self.abctype not in ABC_O2_COEFFS:
+            raise ValueError("AbsorbingBoundary: abctype must be one of A-E")
         self.tri_ids = np.asarray(self.tri_ids, dtype=np.int64)
+
+    def get_gamma2(self, k0: float) -> complex:
+        """Coefficient of the second-order correction matrix, j c2 / k0 (0 for order 1)."""
+        return 1j * ABC_O2_COEFFS[self.abctype][1] / k0 if self.order == 2 else 0.0
 
     def get_beta(self, k0: float) -> float:
         return k0

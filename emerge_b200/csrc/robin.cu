@@ -179,3 +179,99 @@ extern "C" int emfem_ned2_tri_robin(emfem_handle h, int64_t n_nodes, const doubl
     EMFEM_LAUNCH("tri_robin_kernel");
     return EMFEM_OK;
 }
+
+// ---- second-order absorbing boundary correction ------------------------------------------------
+// Restates abc_order_2_terms (ASM/robin_abc_order2.py:192-327): per triangle, in its plane frame
+// (x along the first edge, z the normal), cf * L_i L_j * (int curl_t N_i curl_t N_j - int div_t N_i div_t N_j) * |A|
+// over the 6-point rule that module carries (8-digit weights and points, :190-193).  The triangle's
+// nodes are in sorted order, so its edges are (0,1), (1,2), (0,2) (Mesh3D tri_to_edge order).
+__constant__ double ABC2_DPTS[4][6] = {
+    {0.22338159, 0.22338159, 0.22338159, 0.10995174, 0.10995174, 0.10995174},
+    {0.10810302, 0.44594849, 0.44594849, 0.81684757, 0.09157621, 0.09157621},
+    {0.44594849, 0.44594849, 0.10810302, 0.09157621, 0.09157621, 0.81684757},
+    {0.44594849, 0.10810302, 0.44594849, 0.09157621, 0.81684757, 0.09157621}};
+
+__global__ void tri_abc2_kernel(long long n_nodes, const double* __restrict__ nodes, long long n_sel,
+                                const int64_t* __restrict__ tri_nodes, double cf_re, double cf_im,
+                                double2* __restrict__ blocks, int* status) {
+    long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n_sel) return;
+    double v[3][3];
+    for (int k = 0; k < 3; k++) {
+        long long id = tri_nodes[k * n_sel + t];
+        if (id < 0 || id >= n_nodes) { flag(status, DEV_BAD_INDEX); return; }
+        for (int d = 0; d < 3; d++) v[d][k] = nodes[d * n_nodes + id];
+    }
+    double e1[3], e2[3], z[3], xh[3], yh[3];
+    for (int d = 0; d < 3; d++) { e1[d] = v[d][1] - v[d][0]; e2[d] = v[d][2] - v[d][0]; }
+    z[0] = e1[1] * e2[2] - e1[2] * e2[1]; z[1] = e1[2] * e2[0] - e1[0] * e2[2]; z[2] = e1[0] * e2[1] - e1[1] * e2[0];
+    double nz = sqrt(z[0] * z[0] + z[1] * z[1] + z[2] * z[2]), ne = sqrt(e1[0] * e1[0] + e1[1] * e1[1] + e1[2] * e1[2]);
+    if (!(nz > 0) || !(ne > 0)) { flag(status, DEV_DEGENERATE); return; }
+    for (int d = 0; d < 3; d++) { z[d] /= nz; xh[d] = e1[d] / ne; }
+    yh[0] = z[1] * xh[2] - z[2] * xh[1]; yh[1] = z[2] * xh[0] - z[0] * xh[2]; yh[2] = z[0] * xh[1] - z[1] * xh[0];
+    double ny = sqrt(yh[0] * yh[0] + yh[1] * yh[1] + yh[2] * yh[2]);
+    for (int d = 0; d < 3; d++) yh[d] /= ny;
+    double xp[3], yp[3];
+    for (int k = 0; k < 3; k++) {
+        double r0 = v[0][k] - v[0][0], r1 = v[1][k] - v[1][0], r2 = v[2][k] - v[2][0];
+        xp[k] = xh[0] * r0 + xh[1] * r1 + xh[2] * r2;
+        yp[k] = yh[0] * r0 + yh[1] * r1 + yh[2] * r2;
+    }
+    double D[3][3];
+    for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++) D[i][j] = sqrt((xp[i] - xp[j]) * (xp[i] - xp[j]) + (yp[i] - yp[j]) * (yp[i] - yp[j]));
+    double a[3] = {xp[1] * yp[2] - yp[1] * xp[2], xp[2] * yp[0] - yp[2] * xp[0], xp[0] * yp[1] - yp[0] * xp[1]};
+    double b[3] = {yp[1] - yp[2], yp[2] - yp[0], yp[0] - yp[1]};
+    double c[3] = {xp[2] - xp[1], xp[0] - xp[2], xp[1] - xp[0]};
+    double sA = 0.5 * ((xp[0] - xp[2]) * (yp[1] - yp[0]) - (xp[0] - xp[1]) * (yp[2] - yp[0]));
+    double A = fabs(sA), sg = sA > 0 ? 1.0 : (sA < 0 ? -1.0 : 0.0);
+    if (!(A > 0)) { flag(status, DEV_DEGENERATE); return; }
+    for (int k = 0; k < 3; k++) { a[k] = a[k] * sg / (2 * A); b[k] = b[k] * sg / (2 * A); c[k] = c[k] * sg / (2 * A); }
+    // curl_t and div_t of the 8 DOFs [e1 x3, f1, e2 x3, f2] at the 6 points
+    double cu[8][6], dv[8][6];
+    const int EI[3] = {0, 1, 0}, EJ[3] = {1, 2, 2};
+    for (int p = 0; p < 6; p++) {
+        double x = xp[0] * ABC2_DPTS[1][p] + xp[1] * ABC2_DPTS[2][p] + xp[2] * ABC2_DPTS[3][p];
+        double y = yp[0] * ABC2_DPTS[1][p] + yp[1] * ABC2_DPTS[2][p] + yp[2] * ABC2_DPTS[3][p];
+        for (int k = 0; k < 3; k++) {
+            int i = EI[k], j = EJ[k];
+            double a1 = a[i], b1 = b[i], c1 = c[i], a2 = a[j], b2 = b[j], c2 = c[j];
+            double L1 = a1 + b1 * x + c1 * y, L2 = a2 + b2 * x + c2 * y;
+            cu[k][p] = -3 * a1 * b1 * c2 + 3 * a1 * b2 * c1 - 3 * b1 * b1 * c2 * x + 3 * b1 * b2 * c1 * x
+                       - 3 * b1 * c1 * c2 * y + 3 * b2 * c1 * c1 * y;
+            cu[k + 4][p] = -3 * a2 * b1 * c2 + 3 * a2 * b2 * c1 - 3 * b1 * b2 * c2 * x - 3 * b1 * c2 * c2 * y
+                           + 3 * b2 * b2 * c1 * x + 3 * b2 * c1 * c2 * y;
+            dv[k][p] = b1 * (b1 * L2 - b2 * L1) + c1 * (c1 * L2 - c2 * L1);
+            dv[k + 4][p] = b2 * (b1 * L2 - b2 * L1) + c2 * (c1 * L2 - c2 * L1);
+        }
+        double L1 = a[0] + b[0] * x + c[0] * y, L2 = a[1] + b[1] * x + c[1] * y, L3 = a[2] + b[2] * x + c[2] * y;
+        cu[3][p] = -b[1] * (c[0] * L3 - c[2] * L1) + c[1] * (b[0] * L3 - b[2] * L1) + 2 * (b[0] * c[2] - b[2] * c[0]) * L2;
+        cu[7][p] = b[2] * (c[0] * L2 - c[1] * L1) - c[2] * (b[0] * L2 - b[1] * L1) - 2 * (b[0] * c[1] - b[1] * c[0]) * L3;
+        dv[3][p] = -b[1] * (b[0] * L3 - b[2] * L1) - c[1] * (c[0] * L3 - c[2] * L1);
+        dv[7][p] = b[2] * (b[0] * L2 - b[1] * L1) + c[2] * (c[0] * L2 - c[1] * L1);
+    }
+    double Lr[8];
+    for (int k = 0; k < 3; k++) Lr[k] = Lr[k + 4] = D[EI[k]][EJ[k]];
+    Lr[3] = D[0][2];
+    Lr[7] = D[0][1];
+    for (int r = 0; r < 8; r++)
+        for (int q = 0; q < 8; q++) {
+            double sc = 0, sd = 0;
+            for (int p = 0; p < 6; p++) {
+                sc += cu[r][p] * cu[q][p] * ABC2_DPTS[0][p];
+                sd += dv[r][p] * dv[q][p] * ABC2_DPTS[0][p];
+            }
+            double m = Lr[r] * Lr[q] * (sc - sd) * A;
+            blocks[t * 64 + r * 8 + q] = make_double2(cf_re * m, cf_im * m);
+        }
+}
+
+extern "C" int emfem_ned2_tri_abc2(emfem_handle h, int64_t n_nodes, const double* nodes, int64_t n_sel,
+                                   const int64_t* tri_nodes, double cf_re, double cf_im, void* blocks) {
+    EMFEM_REQUIRE(h && nodes && tri_nodes && blocks && n_sel >= 0 && n_nodes > 0, "emfem_ned2_tri_abc2: bad argument");
+    if (n_sel == 0) return EMFEM_OK;
+    tri_abc2_kernel<<<grid_for(n_sel, 128), 128, 0, h->h.stream>>>(n_nodes, nodes, n_sel, tri_nodes, cf_re, cf_im,
+                                                                   (double2*)blocks, h->h.dev_status);
+    EMFEM_LAUNCH("tri_abc2_kernel");
+    return EMFEM_OK;
+}

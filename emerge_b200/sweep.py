@@ -25,7 +25,7 @@ import numpy as np
 import torch
 
 from ._lib import Handle, check, lib, ptr, ERR_NOT_CONVERGED
-from .assembly import CsrPlan, DeviceMesh, dunavant4, tri_robin_device
+from .assembly import CsrPlan, DeviceMesh, dunavant4, tri_abc2_device, tri_robin_device
 from .ports import k0_of
 
 PRECOND = {"none": 0, "jacobi": 1, "block_jacobi": 2, "aux": 3, "learned": 4}
@@ -129,9 +129,6 @@ class FrequencySweep:
         blocks_all, meta_rows, meta_cols, meta_port = [], [], [], []
         self.bhat = []
         robin = list(getattr(P, "robin", []) or [])
-        nports = len(P.ports) + len(robin)
-        if nports > 8:
-            raise ValueError("at most 8 ports + Robin boundaries per sweep")
         off = 0
         for q, port in enumerate(P.ports):
             tid = np.asarray(port.tri_ids, dtype=np.int64)
@@ -154,17 +151,26 @@ class FrequencySweep:
             bh[torch.from_numpy(ud).to(dev)] = vals
             self.bhat.append(bh)
             off += len(rows)
-        # non-excited Robin boundaries: R̂ with γ = 1 (no excitation), as extra patch "ports"
-        for r, bc in enumerate(robin):
-            q = len(P.ports) + r
+        # non-excited Robin boundaries: R̂ with γ = 1 (no excitation), as extra patch "ports"; a
+        # second-order ABC adds its correction matrix (coefficient 1) as one more
+        self._gamma_fns = [p.get_gamma for p in P.ports]
+        for bc in robin:
             tid = np.asarray(bc.tri_ids, dtype=np.int64)
-            tn = mesh.tris[:, tid]
-            blocks, _ = tri_robin_device(self.dmesh, torch.from_numpy(np.ascontiguousarray(tn)).to(dev), 1.0)
+            tn = torch.from_numpy(np.ascontiguousarray(mesh.tris[:, tid])).to(dev)
             t2f = fld.tri_to_field[:, tid]
-            blocks_all.append(blocks.reshape(-1))
-            meta_rows.append(np.repeat(t2f.T, 8, axis=1).ravel())
-            meta_cols.append(np.tile(t2f.T, (1, 8)).ravel())
-            meta_port.append(np.full(8 * 8 * len(tid), q))
+            parts = [(tri_robin_device(self.dmesh, tn, 1.0)[0], bc.get_gamma)]
+            if getattr(bc, "order", 1) == 2:
+                parts.append((tri_abc2_device(self.dmesh, tn, 1.0), bc.get_gamma2))
+            for blocks, gfn in parts:
+                q = len(self._gamma_fns)
+                self._gamma_fns.append(gfn)
+                blocks_all.append(blocks.reshape(-1))
+                meta_rows.append(np.repeat(t2f.T, 8, axis=1).ravel())
+                meta_cols.append(np.tile(t2f.T, (1, 8)).ravel())
+                meta_port.append(np.full(8 * 8 * len(tid), q))
+        nports = len(self._gamma_fns)
+        if nports > 8:
+            raise ValueError("at most 8 ports + Robin terms per sweep")
         if not meta_rows:                     # no ports and no Robin boundaries (a closed cavity)
             i32 = dict(dtype=torch.int32, device=dev)
             self.patch_vals = torch.zeros(0, dtype=torch.complex128, device=dev)
@@ -257,9 +263,9 @@ class FrequencySweep:
         return np.array([k0_of(f) ** 2 for f in freqs])
 
     def gammas(self, freqs) -> np.ndarray:
-        """(nsys, n_ports) complex γ of every port, then every non-excited Robin boundary, at every frequency."""
-        bcs = list(self.problem.ports) + list(getattr(self.problem, "robin", []) or [])
-        return np.array([[complex(p.get_gamma(k0_of(f))) for p in bcs] for f in freqs])
+        """(nsys, n_ports) complex coefficients of every patch term (ports, then non-excited Robin
+        boundaries and second-order ABC corrections) at every frequency."""
+        return np.array([[complex(g(k0_of(f))) for g in self._gamma_fns] for f in freqs]).reshape(len(freqs), -1)
 
     def rhs(self, systems) -> torch.Tensor:
         """(N, nsys) right-hand sides b + port_vector[p] (``MW/simjob.py:88-92``, b = 0)."""

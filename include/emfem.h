@@ -178,6 +178,13 @@ int emfem_sweep_spmv(emfem_handle h, int64_t n, const int32_t *indptr, const int
                      int n_ports, const double *gamma_dev, const uint8_t *free_mask,
                      const void *x, void *y);
 
+/* Second-order absorbing-boundary correction: abc_order_2_matrix's per-triangle 8x8 blocks
+ * (ASM/robin_abc_order2.py:192-373), cf * L_i L_j (int curl_t N_i curl_t N_j - int div_t N_i div_t N_j) |A|
+ * in the triangle's plane frame with that module's 6-point rule.  tri_nodes (3, n_sel) i64 sorted
+ * node ids; blocks (n_sel, 64) c128 row-major, DOF order of tri_to_field.  Device arrays. */
+int emfem_ned2_tri_abc2(emfem_handle h, int64_t n_nodes, const double *nodes, int64_t n_sel,
+                        const int64_t *tri_nodes, double cf_re, double cf_im, void *blocks);
+
 /* ---- S-parameter overlap integrals -------------------------------------------------------------
  * For the port triangles (tri_nodes (3, n_tri) i64, their owning tets tri_tet (n_tri) i64) and nsys
  * solutions x (n_field, nsys) c128, computes the port-mode overlap of every solution,

@@ -31,6 +31,9 @@ Fixtures
     roughness, user impedance function: ``:1243-1343``) over 2-40 GHz, the objects built without their
     geometry (only the attributes ``get_gamma`` reads are set).
 
+``abc2.npz``           the reference's ``abc_order_2_matrix`` (``ASM/robin_abc_order2.py:350-373``) on the
+    element_small mesh's z=0 and x=a faces with coefficient 0.3-0.7j: the touched 64-entry blocks.
+
 Fixtures can be generated one at a time: ``python tests/golden/make_golden.py mesh_conn``.
 
 ``ASM/`` = ``src/emerge/_emerge/physics/microwave/assembly/``; ``MW/`` = ``src/emerge/_emerge/physics/microwave/``.
@@ -253,6 +256,18 @@ def mesh_conn():
     np.savez_compressed(os.path.join(HERE, "mesh_conn.npz"), **out)
 
 
+def abc2():
+    import importlib
+    d = np.load(os.path.join(HERE, "element_small.npz"))
+    mesh = TetMesh(d["nodes"], d["tets"])
+    fld = R.nedelec2.Nedelec2(mesh)
+    mod = importlib.import_module("emerge._emerge.physics.microwave.assembly.robin_abc_order2")
+    tri = np.concatenate([mesh.tris_on_plane(2, 0.0), mesh.tris_on_plane(0, 1.0e-2)])
+    cf = 0.3 - 0.7j
+    Mat = mod.abc_order_2_matrix(fld, tri, cf)
+    np.savez_compressed(os.path.join(HERE, "abc2.npz"), tri_ids=tri, cf=cf, blocks=Mat.reshape(-1, 64)[tri])
+
+
 def robin_gamma():
     class _Scalar:
         def __init__(self, v):
@@ -300,7 +315,7 @@ def robin_gamma():
 
 
 if __name__ == "__main__":
-    which = sys.argv[1:] or ["element_small", "config1", "mesh_conn", "robin_gamma"]
+    which = sys.argv[1:] or ["element_small", "config1", "mesh_conn", "robin_gamma", "abc2"]
     if "element_small" in which:
         m, f = element_small()
         robin_small(m, f)
@@ -310,6 +325,8 @@ if __name__ == "__main__":
         mesh_conn()
     if "robin_gamma" in which:
         robin_gamma()
+    if "abc2" in which:
+        abc2()
     for fn in sorted(os.listdir(HERE)):
         if fn.endswith(".npz"):
             print(fn, os.path.getsize(os.path.join(HERE, fn)))

@@ -8,14 +8,30 @@ from emerge_b200.boundaries import ABC_O2_COEFFS, AbsorbingBoundary, SurfaceImpe
 
 def test_absorbing_boundary_gamma(golden):
     g = golden("robin_gamma")
-    abc = AbsorbingBoundary(np.arange(3))
+    abc = AbsorbingBoundary(np.arange(3), order=1)
     got = np.array([abc.get_gamma(k) for k in g["k0"]])
     assert np.abs(got - g["abc1"]).max() <= 1e-14 * np.abs(g["abc1"]).max()
-    for t in "ABCDE":       # the order-2 coefficient table, applied as the reference does
-        got2 = np.array([1j * k * ABC_O2_COEFFS[t][0] for k in g["k0"]])
+    assert abc.get_gamma2(100.0) == 0.0
+    for t in "ABCDE":       # order 2 (the reference's default): γ = j k0 c0, correction j c2 / k0
+        abc2 = AbsorbingBoundary(np.arange(3), order=2, abctype=t)
+        got2 = np.array([abc2.get_gamma(k) for k in g["k0"]])
         assert np.abs(got2 - g["abc2_" + t]).max() <= 1e-14 * np.abs(g["abc2_" + t]).max()
-    with pytest.raises(NotImplementedError):
-        AbsorbingBoundary(np.arange(3), order=2)
+        assert abc2.get_gamma2(250.0) == 1j * ABC_O2_COEFFS[t][1] / 250.0
+    assert AbsorbingBoundary(np.arange(3)).order == 2
+    with pytest.raises(ValueError):
+        AbsorbingBoundary(np.arange(3), order=3)
+
+
+def test_abc2_oracle_matches_reference(golden):
+    """The second-order ABC correction oracle reproduces the reference's abc_order_2_matrix."""
+    from oracle import abc2
+    from emerge_b200.mesh import TetMesh
+    from emerge_b200.nedelec2 import Nedelec2
+    g = golden("abc2")
+    d = golden("element_small")
+    f = Nedelec2(TetMesh(d["nodes"], d["tets"]))
+    M = abc2.abc_order_2_matrix(f, g["tri_ids"], complex(g["cf"])).reshape(-1, 64)[g["tri_ids"]]
+    assert np.abs(M - g["blocks"]).max() <= 1e-13 * np.abs(g["blocks"]).max()
 
 
 @pytest.mark.parametrize("i", range(4))

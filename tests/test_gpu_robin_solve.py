@@ -88,7 +88,15 @@ def test_solver_plugin_through_solve_routine(cuda, golden):
         assert np.linalg.norm(x - gx) / np.linalg.norm(gx) <= 1e-10
 
 
-@pytest.mark.parametrize("kind", ["abc", "surface"])
+def test_abc2_kernel_vs_reference_golden(cuda, golden):
+    g = golden("abc2")
+    d = golden("element_small")
+    f = Nedelec2(TetMesh(d["nodes"], d["tets"]))
+    M = assembly.abc_order_2_matrix(f, g["tri_ids"], complex(g["cf"])).reshape(-1, 64)[g["tri_ids"]]
+    assert np.abs(M - g["blocks"]).max() <= 1e-12 * np.abs(g["blocks"]).max()
+
+
+@pytest.mark.parametrize("kind", ["abc", "abc2", "surface"])
 def test_sweep_with_robin_boundaries_matches_superlu(cuda, kind):
     """Non-excited Robin boundaries in the device sweep (an absorbing boundary in place of the
     second port; a conducting surface-impedance wall in place of a PEC wall) vs the oracle's
@@ -97,8 +105,8 @@ def test_sweep_with_robin_boundaries_matches_superlu(cuda, kind):
     P = problems.waveguide()
     m = P.mesh
     a, b, l = P.dims
-    if kind == "abc":
-        P.robin = [AbsorbingBoundary(P.ports[1].tri_ids)]
+    if kind in ("abc", "abc2"):
+        P.robin = [AbsorbingBoundary(P.ports[1].tri_ids, order=1 if kind == "abc" else 2)]
         P.ports = P.ports[:1]
     else:
         wall = m.tris_on_plane(1, b)
@@ -120,6 +128,9 @@ def test_sweep_with_robin_boundaries_matches_superlu(cuda, kind):
         pvs.append(bp)
     for bc in P.robin:
         Bm = oracle.assemble_robin_bc(P.field, Bm, bc.tri_ids, bc.get_gamma(k0))
+        if getattr(bc, "order", 1) == 2:
+            from oracle import abc2 as oabc2
+            Bm = Bm + oabc2.abc_order_2_matrix(P.field, bc.tri_ids, bc.get_gamma2(k0))
     K = K + P.field.generate_csr(Bm)
     xs = oracle.solve_routine(K, pvs, P.solve_ids)
     x = res.x.cpu().numpy()

@@ -207,15 +207,39 @@ class CsrPlan:
             self._host_pattern = (self.indptr.cpu().numpy(), self.indices.cpu().numpy())
         return self._host_pattern
 
+    POOL_BUFFERS = 4
+
     def download(self, vals: torch.Tensor) -> np.ndarray:
-        """Device values -> a fresh host array.  The copy goes through a pinned staging buffer owned
-        by the plan (pageable device-to-host copies run at a few GB/s) and then a multi-threaded
-        host copy into new memory, so every call returns storage the caller owns."""
-        if getattr(self, "_stage", None) is None or self._stage.numel() < vals.numel():
-            self._stage = torch.empty(vals.numel(), dtype=vals.dtype, pin_memory=True)
-        stage = self._stage[:vals.numel()]
+        """Device values -> a host array the caller owns.
+
+        The values are copied once, device to host, straight into a pinned buffer from a small pool
+        held by the plan, and the returned array is a view of that buffer.  A buffer is handed out
+        again only after every array returned from it has been released: a weak reference on the
+        returned array tracks that, and any view the caller derives keeps the array alive.  Results
+        never alias one another.  When all ``POOL_BUFFERS`` buffers are in use, the values go
+        through a pinned staging copy into fresh pageable memory instead."""
+        import weakref
+        n = vals.numel()
+        pool = getattr(self, "_pool", None)
+        if pool is None:
+            pool = self._pool = []
+        entry = None
+        for e in pool:
+            if e[0].numel() >= n and (e[1] is None or e[1]() is None):
+                entry = e
+                break
+        if entry is None and len(pool) < self.POOL_BUFFERS:
+            entry = [torch.empty(n, dtype=vals.dtype, pin_memory=True), None]
+            pool.append(entry)
+        if entry is not None:
+            buf = entry[0][:n]
+            buf.copy_(vals)
+            arr = buf.numpy()
+            entry[1] = weakref.ref(arr)
+            return arr
+        stage = torch.empty(n, dtype=vals.dtype, pin_memory=True)
         stage.copy_(vals)
-        out = torch.empty(vals.numel(), dtype=vals.dtype)
+        out = torch.empty(n, dtype=vals.dtype)
         out.copy_(stage)
         return out.numpy()
 

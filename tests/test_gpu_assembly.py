@@ -111,3 +111,19 @@ def test_every_kernel_variant_gives_identical_values(cuda):
             ref = cur
         else:
             assert np.array_equal(cur[0], ref[0]) and np.array_equal(cur[1], ref[1]), v
+
+
+def test_drop_in_results_never_alias(cuda, small):
+    """tet_mass_stiffness_matrices hands out pinned pool buffers: a result held by the caller keeps
+    its values across later calls, and a released buffer is reused."""
+    d, m, f = small
+    E1, B1 = assembly.tet_mass_stiffness_matrices(f, d["er"], d["ur"])
+    keep = E1.data.copy()
+    view = B1.data[5:9]
+    er2 = d["er"] * 2.0
+    for _ in range(6):                       # more calls than pool buffers while E1/B1 are held
+        E2, B2 = assembly.tet_mass_stiffness_matrices(f, er2, d["ur"])
+    assert np.array_equal(E1.data, keep)
+    np.testing.assert_array_equal(view, B1.data[5:9])
+    assert not np.shares_memory(E1.data, E2.data) and not np.shares_memory(B1.data, B2.data)
+    assert np.abs(B2.data - 2.0 * B1.data).max() <= 1e-12 * np.abs(B1.data).max()   # B is linear in er

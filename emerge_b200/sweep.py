@@ -119,6 +119,8 @@ class FrequencySweep:
 
     def assemble(self):
         self.E, self.B = self.plan.assemble(self.er, self.ur, self.E, self.B)
+        if getattr(self, "_aux", None) is not None:    # the aux diagonals follow the operator
+            self._aux.set_operator(self)
         return self.E, self.B
 
     def _build_ports(self):

@@ -209,6 +209,11 @@ class CsrPlan:
 
     POOL_BUFFERS = 4
 
+    def release_host_buffers(self) -> None:
+        """Drop the plan's pinned result buffers.  Arrays already handed out stay valid; they
+        keep their own buffer alive."""
+        self._pool = []
+
     def download(self, vals: torch.Tensor) -> np.ndarray:
         """Device values -> a host array the caller owns.
 
@@ -398,3 +403,10 @@ def abc_order_2_matrix(field, surf_triangle_indices, coeff, device=None) -> np.n
         blocks = tri_abc2_device(dm, _to_dev(field.mesh.tris[:, tid], torch.int64, dev), coeff).cpu().numpy()
         np.add.at(out.reshape(-1, 64), tid, blocks)
     return out
+
+
+def release_host_buffers(field) -> None:
+    """Release the pinned result buffers of the plan cached on ``field`` (if any)."""
+    cache = getattr(field, "_emfem_cache", None)
+    if cache is not None:
+        cache[2].release_host_buffers()

@@ -88,6 +88,7 @@ _SIGS = {
     "emfem_mpnn_nparams": ([], _i32),
     "emfem_mpnn_workspace_floats": ([_vp, _i32, ctypes.POINTER(_i64), ctypes.POINTER(_i64)], _i32),
     "emfem_mpnn_forward": ([_vp, _i32, _vp, _vp, _vp, _vp], _i32),
+    "emfem_mpnn_infer": ([_vp, _i32, _vp, _vp, _vp, _vp], _i32),
     "emfem_mpnn_backward": ([_vp, _i32, _vp, _vp, _vp, _vp, _vp, _vp], _i32),
     "emfem_adam_step": ([_vp, _i64, _vp, _vp, _vp, _vp, ctypes.c_float, ctypes.c_float, ctypes.c_float,
                          ctypes.c_float, ctypes.c_float, _i32], _i32),

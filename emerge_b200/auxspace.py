@@ -192,6 +192,16 @@ class Network:
         self._x = x
         return za
 
+    def infer(self, x: torch.Tensor) -> torch.Tensor:
+        """za = N(x) through the tensor-core inference kernels the solver uses (TF32 inputs)."""
+        x = x.to(torch.complex64).contiguous()
+        work = torch.empty(2 * self.aux.n_aux * x.shape[1] * 2 * CHANNELS, dtype=torch.float32, device=x.device)
+        za = torch.empty_like(x)
+        Handle.get(self.aux.device)
+        check(lib().emfem_mpnn_infer(self.aux.handle, x.shape[1], ptr(self.params), ptr(x), ptr(work), ptr(za)),
+              "emfem_mpnn_infer")
+        return za
+
     def backward(self, dza: torch.Tensor) -> torch.Tensor:
         """Parameter gradient for dza = dL/dRe(za) + i dL/dIm(za) of the last forward."""
         dza = dza.to(torch.complex64).contiguous()

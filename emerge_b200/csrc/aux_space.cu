@@ -24,6 +24,8 @@
 // on values), so results are reproducible.
 #include "emfem_internal.cuh"
 
+#include <mma.h>
+
 #include <utility>
 #include <vector>
 
@@ -424,6 +426,146 @@ static unsigned warp_grid(long long rows) {
     return (unsigned)(blocks < cap ? (blocks > 0 ? blocks : 1) : cap);
 }
 
+// Tensor-core layer for inference inside the solve (TF32 inputs, FP32 accumulation, via wmma).
+// A warp takes 8 rows (y, s) at a time.  It gathers in_y and m_y into shared memory with lanes over
+// channels (coalesced), as 16 matrix rows (re and im of each row) x 32 channels.  It multiplies them
+// by W_l[t] and U_l[t] for both node types on the tensor cores, then writes each row's result for its
+// own type, lanes over channels again.  Real weights act on the re and im rows alike, so this is the
+// same complex-linear layer as mpnn_layer_kernel, rounded to TF32 on input.
+constexpr int TC_LD = 40;                // padded row stride (floats) of the shared tiles
+constexpr int TC_WARPS = 4;
+
+template <typename TX>
+__global__ void __launch_bounds__(TC_WARPS * 32) mpnn_layer_tc_kernel(
+    long long na, int S, int layer, const float* __restrict__ P, const int* __restrict__ nptr,
+    const int* __restrict__ nbr, const float* __restrict__ inv_deg, const uint8_t* __restrict__ atype,
+    const TX* __restrict__ x, const float2* __restrict__ Hin, float2* __restrict__ Hout, TX* __restrict__ za) {
+    using namespace nvcuda;
+    __shared__ __align__(32) float sWU[4][NN_C * TC_LD];          // W0, W1, U0, U1 as [k][c]
+    __shared__ __align__(32) float sA[TC_WARPS][16 * TC_LD], sM[TC_WARPS][16 * TC_LD];
+    __shared__ float sWin[2][NN_C], sWout[2][NN_C];
+    for (int i = threadIdx.x; i < 4 * NN_C * NN_C; i += blockDim.x) {
+        int m = i / (NN_C * NN_C), r = i % (NN_C * NN_C), k = r / NN_C, c = r % NN_C;
+        int t = m & 1, isU = m >> 1;
+        float v = P[(isU ? nn_off_U(layer) : nn_off_W(layer)) + t * NN_C * NN_C + r];
+        sWU[m][k * TC_LD + c] = wmma::__float_to_tf32(v);
+    }
+    for (int k = threadIdx.x; k < 2 * NN_C; k += blockDim.x) {
+        sWin[k / NN_C][k % NN_C] = P[nn_off_win() + k];
+        sWout[k / NN_C][k % NN_C] = P[nn_off_wout() + k];
+    }
+    __syncthreads();
+    const int lane = threadIdx.x & 31, wl = threadIdx.x >> 5;
+    float* A = sA[wl];
+    float* M = sM[wl];
+    const long long total = na * S;
+    const long long ntiles = (total + 7) / 8;
+    for (long long tile = (long long)blockIdx.x * TC_WARPS + wl; tile < ntiles; tile += (long long)gridDim.x * TC_WARPS) {
+        const long long w0 = tile * 8;
+        bool has[2] = {false, false};
+        for (int r = 0; r < 8; r++) {
+            long long w = w0 + r;
+            float2 in = make_float2(0.f, 0.f), m = make_float2(0.f, 0.f);
+            if (w < total) {
+                long long y = w / S;
+                int s = (int)(w % S), t = atype[y];
+                has[t] = true;
+                if (layer == 0) {
+                    TX xv = x[w];
+                    in = make_float2((float)xv.x * sWin[t][lane], (float)xv.y * sWin[t][lane]);
+                    for (int k = nptr[y]; k < nptr[y + 1]; k++) {
+                        long long j = nbr[k];
+                        TX xj = x[j * S + s];
+                        float wj = sWin[atype[j]][lane];
+                        m.x += (float)xj.x * wj;
+                        m.y += (float)xj.y * wj;
+                    }
+                } else {
+                    in = Hin[w * NN_C + lane];
+                    for (int k = nptr[y]; k < nptr[y + 1]; k++) {
+                        float2 hj = Hin[((long long)nbr[k] * S + s) * NN_C + lane];
+                        m.x += hj.x;
+                        m.y += hj.y;
+                    }
+                }
+                float idg = inv_deg[y];
+                m.x *= idg; m.y *= idg;
+            }
+            A[(2 * r) * TC_LD + lane] = wmma::__float_to_tf32(in.x);
+            A[(2 * r + 1) * TC_LD + lane] = wmma::__float_to_tf32(in.y);
+            M[(2 * r) * TC_LD + lane] = wmma::__float_to_tf32(m.x);
+            M[(2 * r + 1) * TC_LD + lane] = wmma::__float_to_tf32(m.y);
+        }
+        __syncwarp();
+        wmma::fragment<wmma::accumulator, 16, 16, 8, float> acc[2][2];
+        for (int t = 0; t < 2; t++)
+            for (int n = 0; n < 2; n++) wmma::fill_fragment(acc[t][n], 0.0f);
+        for (int kk = 0; kk < NN_C; kk += 8) {
+            wmma::fragment<wmma::matrix_a, 16, 16, 8, wmma::precision::tf32, wmma::row_major> fa, fm;
+            wmma::load_matrix_sync(fa, A + kk, TC_LD);
+            wmma::load_matrix_sync(fm, M + kk, TC_LD);
+            for (int t = 0; t < 2; t++) {
+                if (!__any_sync(0xffffffffu, has[t])) continue;
+                for (int n = 0; n < 2; n++) {
+                    wmma::fragment<wmma::matrix_b, 16, 16, 8, wmma::precision::tf32, wmma::row_major> fw, fu;
+                    wmma::load_matrix_sync(fw, sWU[t] + kk * TC_LD + 16 * n, TC_LD);
+                    wmma::load_matrix_sync(fu, sWU[2 + t] + kk * TC_LD + 16 * n, TC_LD);
+                    wmma::mma_sync(acc[t][n], fa, fw, acc[t][n]);
+                    wmma::mma_sync(acc[t][n], fm, fu, acc[t][n]);
+                }
+            }
+        }
+        __syncwarp();
+        // type-0 results into A, type-1 results into M (the inputs are consumed)
+        for (int n = 0; n < 2; n++) {
+            wmma::store_matrix_sync(A + 16 * n, acc[0][n], TC_LD, wmma::mem_row_major);
+            wmma::store_matrix_sync(M + 16 * n, acc[1][n], TC_LD, wmma::mem_row_major);
+        }
+        __syncwarp();
+        for (int r = 0; r < 8; r++) {
+            long long w = w0 + r;
+            if (w >= total) break;
+            int t = atype[w / S];
+            const float* src = t ? M : A;
+            float2 o = make_float2(src[(2 * r) * TC_LD + lane], src[(2 * r + 1) * TC_LD + lane]);
+            if (Hout) Hout[w * NN_C + lane] = o;
+            if (za) {
+                float zr = o.x * sWout[t][lane], zi = o.y * sWout[t][lane];
+                for (int off = 16; off > 0; off >>= 1) {
+                    zr += __shfl_down_sync(0xffffffffu, zr, off);
+                    zi += __shfl_down_sync(0xffffffffu, zi, off);
+                }
+                if (lane == 0) {
+                    TX xv = x[w], rr;
+                    rr.x = xv.x + zr;
+                    rr.y = xv.y + zi;
+                    za[w] = rr;
+                }
+            }
+        }
+        __syncwarp();
+    }
+}
+
+template <typename TX>
+int mpnn_forward_tc(const emfem_aux_s* a, int S, const float* P, const TX* x, float2* H0, float2* H1, TX* za,
+                    cudaStream_t s) {
+    long long na = a->na;
+    long long tiles = (na * S + 7) / 8;
+    long long blocks = (tiles + TC_WARPS - 1) / TC_WARPS;
+    unsigned grid = (unsigned)(blocks < 148LL * 16 ? (blocks > 0 ? blocks : 1) : 148LL * 16);
+    const float2* hin = nullptr;
+    for (int l = 0; l < NN_L; l++) {
+        float2* hout = (l % 2 == 0) ? H0 : H1;
+        bool last = l == NN_L - 1;
+        mpnn_layer_tc_kernel<TX><<<grid, TC_WARPS * 32, 0, s>>>(na, S, l, P, a->inc_ptr, a->inc, a->inv_deg,
+                                                                a->atype, x, hin, last ? nullptr : hout,
+                                                                last ? za : nullptr);
+        hin = hout;
+    }
+    return check_cuda(cudaGetLastError(), "mpnn_layer_tc_kernel");
+}
+
 // Hstore non-null: every layer's output is kept (training); else layers alternate H0/H1 and the
 // last layer writes only za.
 template <typename TX>
@@ -687,7 +829,7 @@ int aux_correct(const emfem_aux_s* a, int S, bool learned, const T* dinv, const 
                                                                      v, ra);
     const T* zsrc = ra;
     if (learned) {
-        EMFEM_TRY(mpnn_forward<T>(a, S, a->params, ra, H0, H1, nullptr, za, s));
+        EMFEM_TRY(mpnn_forward_tc<T>(a, S, a->params, ra, H0, H1, za, s));
         zsrc = za;
     }
     aux_prolong_kernel<T, T><<<grid_for(a->n * S, AB), AB, 0, s>>>(a->n, S, a->gcol, a->gval, zsrc, mask, z, 1);
@@ -933,6 +1075,13 @@ int emfem_mpnn_forward(emfem_aux a, int nsys, const float* params, const void* x
     EMFEM_REQUIRE(a && params && x && act && za && nsys >= 1, "emfem_mpnn_forward: bad argument");
     return mpnn_forward<float2>(a, nsys, params, (const float2*)x, nullptr, nullptr, (float2*)act, (float2*)za,
                                 a->h->stream);
+}
+
+int emfem_mpnn_infer(emfem_aux a, int nsys, const float* params, const void* x, float* work, void* za) {
+    EMFEM_REQUIRE(a && params && x && work && za && nsys >= 1, "emfem_mpnn_infer: bad argument");
+    float2* H0 = (float2*)work;
+    float2* H1 = H0 + (size_t)a->na * nsys * NN_C;
+    return mpnn_forward_tc<float2>(a, nsys, params, (const float2*)x, H0, H1, (float2*)za, a->h->stream);
 }
 
 int emfem_mpnn_backward(emfem_aux a, int nsys, const float* params, const void* x, const float* act, const void* dza,

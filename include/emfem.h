@@ -276,6 +276,9 @@ int emfem_aux_prolong(emfem_aux aux, int nsys, const void *za, const uint8_t *fr
 int emfem_mpnn_nparams(void);
 int emfem_mpnn_workspace_floats(emfem_aux aux, int nsys, int64_t *activation_floats, int64_t *scratch_floats);
 int emfem_mpnn_forward(emfem_aux aux, int nsys, const float *params, const void *x, float *act, void *za);
+/* Inference form used inside emfem_krylov_solve (precond 4): the same network on the tensor cores
+ * (TF32 inputs, FP32 accumulation); work holds 2 * n_aux * nsys * 64 floats. */
+int emfem_mpnn_infer(emfem_aux aux, int nsys, const float *params, const void *x, float *work, void *za);
 int emfem_mpnn_backward(emfem_aux aux, int nsys, const float *params, const void *x, const float *act,
                         const void *dza, float *grad, float *scratch);
 int emfem_adam_step(emfem_handle h, int64_t n, float *params, const float *grad, float *m, float *v, float lr,

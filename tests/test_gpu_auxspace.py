@@ -121,6 +121,9 @@ def test_network_forward_backward_vs_oracle(guide):
     assert np.abs(grad - go).max() <= 1e-4 * scale, np.abs(grad - go).max() / scale
     # every parameter block receives its gradient (w_in, W/U of each layer, w_out)
     assert np.abs(grad[:64]).max() > 0 and np.abs(grad[-64:]).max() > 0
+    # the tensor-core inference form used inside the solve (TF32 inputs): same network, looser bound
+    zt = net.infer(torch.from_numpy(x).to(aux.device)).cpu().numpy()
+    assert np.abs(zt - zo).max() <= 5e-3 * np.abs(zo).max(), np.abs(zt - zo).max() / np.abs(zo).max()
 
 
 def test_training_reduces_correction_loss_and_learned_solve_converges(guide, golden):

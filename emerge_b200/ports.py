@@ -111,5 +111,54 @@ class RectangularWaveguidePort:
         return np.array(self.frame.to_global_vec(eh, ev, 0 * eh))
 
 
+@dataclass
+class LumpedPort:
+    """Lumped port (``LumpedPort``, ``src/emerge/_emerge/physics/microwave/microwave_bc.py:1018-1162``):
+    a sheet of impedance Z_s = Z0_port·width/height on the port triangles, excited by a uniform field
+    along ``direction``.  γ = j k0 Z0 / Z_s (``:1117-1126``); U_inc = −2j k0 (V/height)(Z0/Z_s) · direction
+    (``:1128-1130``) with V = √(2 P Z0_port) (``:1100-1106``).  Its S-parameters come from voltage line
+    integrals in the reference (``microwave_3d.py:1271-1291``), which this package does not build."""
+    port_number: int
+    tri_ids: np.ndarray
+    width: float
+    height: float
+    direction: tuple = (0.0, 0.0, 1.0)
+    power: float = 1.0
+    Z0: float = 50.0
+    active: bool = False
+
+    def __post_init__(self):
+        d = np.asarray(self.direction, dtype=np.float64)
+        self.direction = d / np.linalg.norm(d)
+        self.tri_ids = np.asarray(self.tri_ids, dtype=np.int64)
+
+    @property
+    def surfZ(self) -> float:
+        return self.Z0 * self.width / self.height
+
+    @property
+    def voltage(self) -> float:
+        return np.sqrt(2 * self.power * self.Z0)
+
+    def get_beta(self, k0: float) -> float:
+        return k0
+
+    def get_gamma(self, k0: float) -> complex:
+        return 1j * k0 * Z0 / self.surfZ
+
+    def port_mode_3d_global(self, x, y, z, k0: float = 0.0) -> np.ndarray:
+        one = np.ones_like(np.asarray(x, dtype=np.float64))
+        return np.array([self.direction[0] * one, self.direction[1] * one, self.direction[2] * one])
+
+    def get_Uinc(self, x, y, z, k0: float) -> np.ndarray:
+        return self.uinc_scale(k0) * self.port_mode_3d_global(x, y, z, k0)
+
+    def uinc_scale(self, k0: float) -> complex:
+        return -1j * 2 * k0 * self.voltage / self.height * (Z0 / self.surfZ)
+
+    def shape_global(self, x, y, z) -> np.ndarray:
+        return self.port_mode_3d_global(x, y, z)
+
+
 def k0_of(f: float) -> float:
     return 2 * np.pi * f / C0

@@ -247,6 +247,9 @@ class FrequencySweep:
         the excited ports filled (NaN elsewhere).  S[q, p] is field_power / mode_power / sqrt(P_p) of
         the reference's ``_post_process`` (``MW/microwave_3d.py:1110-1247``); ``corrections`` applies its
         default column-power and |S| <= 1 caps."""
+        if not all(hasattr(p, "qmode") for p in self.problem.ports):
+            raise NotImplementedError("S-parameters are built for waveguide mode ports; lumped-port voltage "
+                                      "integration (MW/microwave_3d.py:1271-1291) is not")
         ov, nm = self.port_overlaps(res.x)
         P = self.problem
         out: dict = {}

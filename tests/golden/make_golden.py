@@ -311,6 +311,14 @@ def robin_gamma():
     si = object.__new__(R.bc.SurfaceImpedance)
     si._Zf = lambda f: (0.02 + 1e-12 * f) + 1j * (0.01 + 3e-12 * f)
     out["surf_fn"] = np.array([si.get_gamma(k) for k in k0s])
+    # LumpedPort: γ and U_inc at two points (direction (0.6, 0, 0.8), 2 mm x 3 mm, 50 and 75 ohm)
+    for i, (zp, pw) in enumerate(((50.0, 1.0), (75.0, 0.5))):
+        lp = object.__new__(R.bc.LumpedPort)
+        lp.Z0, lp.width, lp.height, lp.power = zp, 2e-3, 3e-3, pw
+        lp.Vdirection = R.cs.Axis(np.array([0.6, 0.0, 0.8]))
+        out[f"lumped{i}_gamma"] = np.array([lp.get_gamma(k) for k in k0s])
+        xs, ys, zs = np.array([1e-3, 2e-3]), np.array([0.5e-3, 0.0]), np.array([0.0, 1e-3])
+        out[f"lumped{i}_uinc"] = np.array([lp.get_Uinc(xs, ys, zs, k) for k in k0s])
     np.savez_compressed(os.path.join(HERE, "robin_gamma.npz"), **out)
 
 

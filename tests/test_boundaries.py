@@ -52,3 +52,16 @@ def test_surface_impedance_function_gamma(golden):
     assert np.abs(got - g["surf_fn"]).max() <= 1e-12 * np.abs(g["surf_fn"]).max()
     with pytest.raises(ValueError):
         SurfaceImpedance(np.arange(3))
+
+
+@pytest.mark.parametrize("i,zp,pw", [(0, 50.0, 1.0), (1, 75.0, 0.5)])
+def test_lumped_port_gamma_and_uinc(golden, i, zp, pw):
+    from emerge_b200.ports import LumpedPort
+    g = golden("robin_gamma")
+    lp = LumpedPort(1, np.arange(3), width=2e-3, height=3e-3, direction=(0.6, 0.0, 0.8), power=pw, Z0=zp)
+    got = np.array([lp.get_gamma(k) for k in g["k0"]])
+    assert np.abs(got - g[f"lumped{i}_gamma"]).max() <= 1e-13 * np.abs(got).max()
+    xs, ys, zs = np.array([1e-3, 2e-3]), np.array([0.5e-3, 0.0]), np.array([0.0, 1e-3])
+    u = np.array([lp.get_Uinc(xs, ys, zs, k) for k in g["k0"]])
+    ref = g[f"lumped{i}_uinc"]
+    assert np.abs(u - ref).max() <= 1e-13 * np.abs(ref).max()

@@ -96,7 +96,7 @@ def test_abc2_kernel_vs_reference_golden(cuda, golden):
     assert np.abs(M - g["blocks"]).max() <= 1e-12 * np.abs(g["blocks"]).max()
 
 
-@pytest.mark.parametrize("kind", ["abc", "abc2", "surface"])
+@pytest.mark.parametrize("kind", ["abc", "abc2", "surface", "lumped"])
 def test_sweep_with_robin_boundaries_matches_superlu(cuda, kind):
     """Non-excited Robin boundaries in the device sweep (an absorbing boundary in place of the
     second port; a conducting surface-impedance wall in place of a PEC wall) vs the oracle's
@@ -105,7 +105,10 @@ def test_sweep_with_robin_boundaries_matches_superlu(cuda, kind):
     P = problems.waveguide()
     m = P.mesh
     a, b, l = P.dims
-    if kind in ("abc", "abc2"):
+    if kind == "lumped":
+        from emerge_b200.ports import LumpedPort
+        P.ports = [P.ports[0], LumpedPort(2, P.ports[1].tri_ids, width=a, height=b, direction=(0.0, 1.0, 0.0))]
+    elif kind in ("abc", "abc2"):
         P.robin = [AbsorbingBoundary(P.ports[1].tri_ids, order=1 if kind == "abc" else 2)]
         P.ports = P.ports[:1]
     else:

@@ -36,6 +36,106 @@ __device__ __forceinline__ double sp_dist(const double* xs, const double* ys, co
     return sqrt(dx * dx + dy * dy + dz * dz);
 }
 
+// Interpolation data of one tet (tet_coefficients, ned2_interp.py:59-77) and the field at a point
+// in it (ned2_tet_interp, ned2_interp.py:230-295), with the local orientation taken from the global
+// node order (local_mapping of the sorted edge / triangle lists).
+struct TetInterp {
+    double xs[4], ys[4], zs[4], a[4], b[4], c[4], d[4], V1;
+    int rank[4];
+};
+
+__device__ __forceinline__ bool load_tet_interp(long long nn, const double* __restrict__ nodes, long long nt,
+                                                const int64_t* __restrict__ tets, long long T, TetInterp& ti) {
+    int64_t vid[4];
+    for (int i = 0; i < 4; i++) {
+        int64_t id = tets[i * nt + T];
+        if (id < 0 || id >= nn) return false;
+        vid[i] = id;
+        ti.xs[i] = nodes[id]; ti.ys[i] = nodes[nn + id]; ti.zs[i] = nodes[2 * nn + id];
+    }
+    const double *xs = ti.xs, *ys = ti.ys, *zs = ti.zs;
+    for (int i = 0; i < 4; i++) {
+        int j = i == 0 ? 1 : 0, k = i <= 1 ? 2 : 1, l = i <= 2 ? 3 : 2;
+        double sgn = (i % 2 == 0) ? 1.0 : -1.0;
+        ti.a[i] = sgn * tet_det3(xs[j], ys[j], zs[j], xs[k], ys[k], zs[k], xs[l], ys[l], zs[l]);
+        ti.b[i] = -sgn * sp_det1(ys[j], zs[j], ys[k], zs[k], ys[l], zs[l]);
+        ti.c[i] = sgn * sp_det1(xs[j], zs[j], xs[k], zs[k], xs[l], zs[l]);
+        ti.d[i] = -sgn * sp_det1(xs[j], ys[j], xs[k], ys[k], xs[l], ys[l]);
+    }
+    double V = fabs(tet_det3(xs[1] - xs[0], ys[1] - ys[0], zs[1] - zs[0], xs[2] - xs[0], ys[2] - ys[0], zs[2] - zs[0],
+                             xs[3] - xs[0], ys[3] - ys[0], zs[3] - zs[0])) / 6.0;
+    ti.V1 = 216.0 * V * V * V;
+    for (int i = 0; i < 4; i++) {
+        int r = 0;
+        for (int j = 0; j < 4; j++) r += vid[j] < vid[i];
+        ti.rank[i] = r;
+    }
+    return true;
+}
+
+__device__ __forceinline__ void eval_field(const TetInterp& ti, const double2 dof[20], double px, double py,
+                                           double pz, double Er[3], double Ei[3]) {
+    const int ep[6] = {0, 0, 0, 1, 3, 2}, eq[6] = {1, 2, 3, 2, 1, 3};
+    const int fv[4][3] = {{0, 1, 2}, {0, 2, 3}, {0, 3, 1}, {1, 2, 3}};
+    const double *xs = ti.xs, *ys = ti.ys, *zs = ti.zs, *b = ti.b, *c = ti.c, *d = ti.d;
+    const double V1 = ti.V1;
+    double Fv[4];
+    for (int i = 0; i < 4; i++) Fv[i] = ti.a[i] + b[i] * px + c[i] * py + d[i] * pz;
+    for (int q = 0; q < 3; q++) { Er[q] = 0; Ei[q] = 0; }
+    for (int e = 0; e < 6; e++) {
+        int v1 = ep[e], v2 = eq[e];
+        if (ti.rank[v2] < ti.rank[v1]) { int t = v1; v1 = v2; v2 = t; }
+        double L = sp_dist(xs, ys, zs, v1, v2);
+        double2 m1 = dof[e], m2 = dof[10 + e];
+        double wr = m1.x * Fv[v1] + m2.x * Fv[v2], wi = m1.y * Fv[v1] + m2.y * Fv[v2];
+        double gg[3] = {b[v1] * Fv[v2] - b[v2] * Fv[v1], c[v1] * Fv[v2] - c[v2] * Fv[v1], d[v1] * Fv[v2] - d[v2] * Fv[v1]};
+        for (int q = 0; q < 3; q++) { Er[q] += L * wr * gg[q] / V1; Ei[q] += L * wi * gg[q] / V1; }
+    }
+    for (int f = 0; f < 4; f++) {
+        int v1 = fv[f][0], v2 = fv[f][1], v3 = fv[f][2], t;
+        if (ti.rank[v2] < ti.rank[v1]) { t = v1; v1 = v2; v2 = t; }
+        if (ti.rank[v3] < ti.rank[v2]) { t = v2; v2 = v3; v3 = t; }
+        if (ti.rank[v2] < ti.rank[v1]) { t = v1; v1 = v2; v2 = t; }
+        double L1 = sp_dist(xs, ys, zs, v1, v3), L2 = sp_dist(xs, ys, zs, v1, v2);
+        double2 m1 = dof[6 + f], m2 = dof[16 + f];
+        double q1r = m1.x * L1 * Fv[v2], q1i = m1.y * L1 * Fv[v2];
+        double q2r = m2.x * L2 * Fv[v3], q2i = m2.y * L2 * Fv[v3];
+        double g13[3] = {b[v1] * Fv[v3] - b[v3] * Fv[v1], c[v1] * Fv[v3] - c[v3] * Fv[v1], d[v1] * Fv[v3] - d[v3] * Fv[v1]};
+        double g12[3] = {b[v1] * Fv[v2] - b[v2] * Fv[v1], c[v1] * Fv[v2] - c[v2] * Fv[v1], d[v1] * Fv[v2] - d[v2] * Fv[v1]};
+        for (int q = 0; q < 3; q++) {
+            Er[q] += (-q1r * g13[q] + q2r * g12[q]) / V1;
+            Ei[q] += (-q1i * g13[q] + q2i * g12[q]) / V1;
+        }
+    }
+}
+
+// E . dl at given points inside given tets, for every system: out[p * nsys + s] (lumped-port voltage
+// lines, microwave_3d.py:1271-1291; the caller applies the line rule's weights)
+__global__ void point_field_dot_kernel(long long nn, const double* __restrict__ nodes, long long nt,
+                                       const int64_t* __restrict__ tets, const int64_t* __restrict__ t2f, long long N,
+                                       long long npts, const int64_t* __restrict__ pt_tet,
+                                       const double* __restrict__ pts, const double* __restrict__ dl, int nsys,
+                                       const double2* __restrict__ x, double2* __restrict__ out, int* status) {
+    long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= npts * nsys) return;
+    long long p = g / nsys;
+    int s = (int)(g % nsys);
+    out[g] = make_double2(0, 0);
+    long long T = pt_tet[p];
+    TetInterp ti;
+    if (T < 0 || T >= nt || !load_tet_interp(nn, nodes, nt, tets, T, ti)) { flag(status, DEV_BAD_INDEX); return; }
+    double2 dof[20];
+    for (int k = 0; k < 20; k++) {
+        int64_t id = t2f[k * nt + T];
+        if (id < 0 || id >= N) { flag(status, DEV_BAD_INDEX); return; }
+        dof[k] = x[id * nsys + s];
+    }
+    double Er[3], Ei[3];
+    eval_field(ti, dof, pts[p], pts[npts + p], pts[2 * npts + p], Er, Ei);
+    const double* w = dl + 3 * p;
+    out[g] = make_double2(Er[0] * w[0] + Er[1] * w[1] + Er[2] * w[2], Ei[0] * w[0] + Ei[1] * w[1] + Ei[2] * w[2]);
+}
+
 __global__ void port_overlap_kernel(long long nn, const double* __restrict__ nodes, long long nt,
                                     const int64_t* __restrict__ tets, const int64_t* __restrict__ t2f, long long N,
                                     long long ntri, const int64_t* __restrict__ tri_tet,
@@ -184,5 +284,19 @@ extern "C" int emfem_port_overlap(emfem_handle h, int64_t n_nodes, const double*
     overlap_sum_kernel<<<grid_for(nsys + 1, 64), 64, 0, h->h.stream>>>(n_tri, nsys, F, Nn, (double2*)overlap,
                                                                         (double2*)mode_norm);
     EMFEM_LAUNCH("overlap_sum_kernel");
+    return EMFEM_OK;
+}
+
+extern "C" int emfem_point_field_dot(emfem_handle h, int64_t n_nodes, const double* nodes, int64_t n_tets,
+                                     const int64_t* tets, const int64_t* tet_to_field, int64_t n_field, int64_t npts,
+                                     const int64_t* pt_tet, const double* pts, const double* dl, int nsys,
+                                     const void* x, void* out) {
+    EMFEM_REQUIRE(h && nodes && tets && tet_to_field && pt_tet && pts && dl && x && out && npts >= 0 && nsys >= 1,
+                  "emfem_point_field_dot: bad argument");
+    if (npts == 0) return EMFEM_OK;
+    point_field_dot_kernel<<<grid_for(npts * nsys, 128), 128, 0, h->h.stream>>>(
+        n_nodes, nodes, n_tets, tets, tet_to_field, n_field, npts, pt_tet, pts, dl, nsys, (const double2*)x,
+        (double2*)out, h->h.dev_status);
+    EMFEM_LAUNCH("point_field_dot_kernel");
     return EMFEM_OK;
 }

@@ -117,7 +117,7 @@ class LumpedPort:
     a sheet of impedance Z_s = Z0_port·width/height on the port triangles, excited by a uniform field
     along ``direction``.  γ = j k0 Z0 / Z_s (``:1117-1126``); U_inc = −2j k0 (V/height)(Z0/Z_s) · direction
     (``:1128-1130``) with V = √(2 P Z0_port) (``:1100-1106``).  Its S-parameters come from voltage line
-    integrals in the reference (``microwave_3d.py:1271-1291``), which this package does not build."""
+    integrals (``microwave_3d.py:1271-1291``; ``FrequencySweep.port_voltages``)."""
     port_number: int
     tri_ids: np.ndarray
     width: float

@@ -242,21 +242,94 @@ class FrequencySweep:
         h.raise_on_device_status("emfem_port_overlap")
         return np.array(ov), np.array(nm)
 
+    def _lumped_lines(self, port) -> dict:
+        """Voltage lines of a lumped port (``define_lumped_port_integration_points``,
+        ``MW/microwave_3d.py:1432-1470``): from every port-face node of minimal projection on the
+        port direction, 21 points over ``height`` along it; each point is assigned the last of the
+        face tets (ascending, ``Mesh3D.get_face_tets``) that contains it, with the reference's
+        inclusion test (``elements/ned2_interp.py:174-211``).  The composite 3-point Gauss rule of
+        ``Line.line_integral`` (``coord.py:24-61, :149-153``) on equally spaced samples is Simpson's
+        rule, so V = Σ_p w_p E(x_p)·dl with w = (1, 4, 2, ..., 4, 1)/3, averaged over the lines."""
+        cache = getattr(self, "_lumped_cache", None)
+        if cache is None:
+            cache = self._lumped_cache = {}
+        if id(port) in cache:
+            return cache[id(port)]
+        mesh, dev = self.problem.mesh, self.device
+        tid = np.asarray(port.tri_ids, dtype=np.int64)
+        nids = np.unique(mesh.tris[:, tid])
+        dirv = np.asarray(port.direction, dtype=np.float64)
+        xs, ys, zs = mesh.nodes[0, nids], mesh.nodes[1, nids], mesh.nodes[2, nids]
+        dot = xs * dirv[0] + ys * dirv[1] + zs * dirv[2]
+        start = np.flatnonzero(dot == np.min(dot))
+        npl = 21
+        lines_pts, lines_dl = [], []
+        for k in start:
+            p0 = np.array([xs[k], ys[k], zs[k]])
+            p1 = p0 + dirv * port.height
+            pts = np.stack([np.linspace(p0[i], p1[i], npl) for i in range(3)])
+            lines_pts.append(pts)
+            lines_dl.append(np.repeat((pts[:, 1] - pts[:, 0])[None, :], npl, axis=0))
+        pts = np.concatenate(lines_pts, axis=1)
+        dl = np.concatenate(lines_dl, axis=0)
+        w1 = np.ones(npl)
+        w1[1:-1:2] = 4.0
+        w1[2:-1:2] = 2.0
+        w = np.tile(w1 / 3.0, len(start)) / len(start)
+        ftets = mesh.face_tets(tid)
+        owner = np.full(pts.shape[1], -1, dtype=np.int64)
+        for t in ftets:
+            v = mesh.nodes[:, mesh.tets[:, t]]
+            basis = np.linalg.inv(np.stack([v[:, 1] - v[:, 0], v[:, 2] - v[:, 0], v[:, 3] - v[:, 0]], axis=1))
+            loc = basis @ (pts - v[:, :1])
+            inside = (loc.sum(axis=0) <= 1.00000001) & (loc >= -1e-6).all(axis=0)
+            owner[inside] = t
+        if (owner < 0).any():
+            raise RuntimeError("lumped port: a voltage-line point lies in none of the port's face tets")
+        d = dict(npts=pts.shape[1], w=w,
+                 pts=torch.from_numpy(np.ascontiguousarray(pts)).to(dev),
+                 dl=torch.from_numpy(np.ascontiguousarray(dl)).to(dev),
+                 pt_tet=torch.from_numpy(owner).to(dev))
+        cache[id(port)] = d
+        return d
+
+    def port_voltages(self, port, x: torch.Tensor) -> np.ndarray:
+        """Lumped-port voltage V (nsys,) of the solutions x (N, nsys), E·dl on the device."""
+        d = self._lumped_lines(port)
+        x = x.contiguous()
+        nsys = x.shape[1]
+        out = torch.empty((d["npts"], nsys), dtype=torch.complex128, device=self.device)
+        h = Handle.get(self.device)
+        dm = self.dmesh
+        check(lib().emfem_point_field_dot(h.h, dm.n_nodes, ptr(dm.nodes), dm.n_tets, ptr(dm.tets),
+                                          ptr(dm.tet_to_field), self.n, d["npts"], ptr(d["pt_tet"]), ptr(d["pts"]),
+                                          ptr(d["dl"]), nsys, ptr(x), ptr(out)), "emfem_point_field_dot")
+        h.raise_on_device_status("emfem_point_field_dot")
+        return d["w"] @ out.cpu().numpy()
+
     def sparams(self, res: SolveResult, corrections: bool = False) -> dict:
         """S-parameters of solved systems: {frequency: (n_ports, n_ports) complex S} with the columns of
-        the excited ports filled (NaN elsewhere).  S[q, p] is field_power / mode_power / sqrt(P_p) of
-        the reference's ``_post_process`` (``MW/microwave_3d.py:1110-1247``); ``corrections`` applies its
-        default column-power and |S| <= 1 caps."""
-        if not all(hasattr(p, "qmode") for p in self.problem.ports):
-            raise NotImplementedError("S-parameters are built for waveguide mode ports; lumped-port voltage "
-                                      "integration (MW/microwave_3d.py:1271-1291) is not")
-        ov, nm = self.port_overlaps(res.x)
+        the excited ports filled (NaN elsewhere).  For a waveguide mode port S[q, p] is field_power /
+        mode_power / sqrt(P_p) of the reference's ``_post_process`` (``MW/microwave_3d.py:1110-1247``);
+        for a lumped port it is (b / a) / sqrt(P_p) with a = the port voltage √(2 P Z0) and b = V − a
+        (excited) or V, V from the voltage lines (``:1271-1291``).  ``corrections`` applies the
+        reference's default column-power and |S| <= 1 caps."""
         P = self.problem
+        mode_ports = [q for q, port in enumerate(P.ports) if hasattr(port, "qmode")]
+        ov = nm = None
+        if mode_ports:
+            ov, nm = self.port_overlaps(res.x)
+        volts = {q: self.port_voltages(port, res.x) for q, port in enumerate(P.ports) if not hasattr(port, "qmode")}
         out: dict = {}
         for s, (f, p) in enumerate(res.systems):
             k0 = k0_of(f)
             S = out.setdefault(f, np.full((len(P.ports), len(P.ports)), np.nan + 0j))
             for q, port in enumerate(P.ports):
+                if q in volts:
+                    a = port.voltage
+                    b = volts[q][s] - a if q == p else volts[q][s]
+                    S[q, p] = (b / a) / np.sqrt(P.ports[p].power)
+                    continue
                 scale = port.qmode(k0) * port.polarization * port.amplitude()
                 S[q, p] = (ov[q, s] / (scale * nm[q]) - (1.0 if q == p else 0.0)) / np.sqrt(P.ports[p].power)
         if corrections:

@@ -201,6 +201,14 @@ int emfem_port_overlap(emfem_handle h, int64_t n_nodes, const double *nodes, int
                        const int64_t *tri_nodes, const double *dpts, int npts, const void *shape,
                        const void *tri_const, int nsys, const void *x, void *work, void *overlap, void *mode_norm);
 
+/* E . dl at arbitrary points: for point p inside tet pt_tet[p] (the caller locates it), the Nedelec-2
+ * field of each solution (ned2_tet_interp's formulas, elements/ned2_interp.py:230-295) dotted with
+ * dl[3 p .. 3 p + 2]; out (npts, nsys) c128.  Used for lumped-port voltage lines
+ * (physics/microwave/microwave_3d.py:1271-1291).  pts (3, npts) f64; x (n_field, nsys) c128; device. */
+int emfem_point_field_dot(emfem_handle h, int64_t n_nodes, const double *nodes, int64_t n_tets, const int64_t *tets,
+                          const int64_t *tet_to_field, int64_t n_field, int64_t npts, const int64_t *pt_tet,
+                          const double *pts, const double *dl, int nsys, const void *x, void *out);
+
 /* ---- mesh connectivity ---------------------------------------------------------------------
  * Replaces the connectivity part of Mesh3D._pre_update (src/emerge/_emerge/mesh3d.py:385-497):
  * the unique sorted edge / triangle node lists in lexicographic order (:386-406), tet_to_edge with

@@ -37,14 +37,22 @@ def interp_on_owner(mesh, field, solution, tri_ids, dpts) -> np.ndarray:
     """E (3, npts, n_tri) at the quadrature points of boundary triangles, from their owning tets."""
     tri_ids = np.asarray(tri_ids)
     T = mesh.tri_to_tet[0, tri_ids]
+    P = np.einsum("cvs,vp->cps", mesh.nodes[:, mesh.tris[:, tri_ids]], dpts[1:4])
+    return interp_in_tets(mesh, field, solution, T, P)
+
+
+def interp_in_tets(mesh, field, solution, T, P) -> np.ndarray:
+    """E (3, npts, n) at points P (3, npts, n), the points of column j inside tet T[j]
+    (``ned2_tet_interp``, ``ned2_interp.py:230-295``)."""
+    T = np.asarray(T)
     tv = mesh.tets[:, T]
     xs, ys, zs = (mesh.nodes[k][tv] for k in range(3))
     a, b, c, d, V = _tet_coefficients(xs, ys, zs)
     V1 = 216 * V ** 3
-    P = np.einsum("cvs,vp->cps", mesh.nodes[:, mesh.tris[:, tri_ids]], dpts[1:4])
     F = a[:, None, :] + b[:, None, :] * P[0] + c[:, None, :] * P[1] + d[:, None, :] * P[2]   # (4, npts, nt)
     rank = np.argsort(np.argsort(tv, axis=0), axis=0)
-    nt = len(tri_ids)
+    nt = len(T)
+    dpts = np.zeros((1, P.shape[1]))
     cols = np.arange(nt)
     dofs = solution[field.tet_to_field[:, T]]
     grads = (b, c, d)
@@ -87,6 +95,12 @@ def sparams(problem, solutions: dict, k0: float, dpts) -> np.ndarray:
     S = np.full((nports, nports), np.nan + 0j)
     for p, sol in solutions.items():
         for q, port in enumerate(problem.ports):
+            if not hasattr(port, "Zmode"):          # lumped port: voltage lines (microwave_3d.py:1271-1291)
+                V = lumped_voltage(problem, port, sol)
+                a = port.voltage
+                b = V - a if q == p else V
+                S[q, p] = (b / a) / np.sqrt(problem.ports[p].power)
+                continue
             tid = np.asarray(port.tri_ids)
             E = interp_on_owner(mesh, field, sol, tid, dpts)
             tn = mesh.tris[:, tid]
@@ -102,3 +116,42 @@ def sparams(problem, solutions: dict, k0: float, dpts) -> np.ndarray:
             mp = np.sum(const * A * np.einsum("p,cpt->t", dpts[0], m * np.conj(m))) / (2 * Zm)
             S[q, p] = fp / mp / np.sqrt(problem.ports[p].power)
     return S
+
+
+def simpson_line_weights(npl: int) -> np.ndarray:
+    """Per-sample weights of ``gauss3_composite`` (``src/emerge/_emerge/coord.py:24-61``) on equally
+    spaced samples: its per-section sum (2/3) a + 2 c with a = y0/2 - y1 + y2/2, c = y1 is
+    (y0 + 4 y1 + y2) / 3."""
+    w = np.ones(npl)
+    w[1:-1:2] = 4.0
+    w[2:-1:2] = 2.0
+    return w / 3.0
+
+
+def lumped_voltage(problem, port, solution) -> complex:
+    """Lumped-port voltage of one solution: the reference's integration lines
+    (``define_lumped_port_integration_points``, ``MW/microwave_3d.py:1432-1470``), each point in the
+    last face tet containing it (``ned2_tet_interp``'s search, ``ned2_interp.py:174-211``),
+    ``Line.line_integral`` (``coord.py:149-153``), averaged over the lines (``microwave_3d.py:1277-1278``)."""
+    mesh, field = problem.mesh, problem.field
+    nids = np.unique(mesh.tris[:, np.asarray(port.tri_ids)])
+    d = np.asarray(port.direction, float)
+    xs, ys, zs = mesh.nodes[0, nids], mesh.nodes[1, nids], mesh.nodes[2, nids]
+    dot = xs * d[0] + ys * d[1] + zs * d[2]
+    starts = np.argwhere(dot == np.min(dot)).flatten()
+    ftets = mesh.face_tets(np.asarray(port.tri_ids))
+    volts = []
+    for k in starts:
+        p0 = np.array([xs[k], ys[k], zs[k]])
+        p1 = p0 + d * port.height
+        pts = np.stack([np.linspace(p0[i], p1[i], 21) for i in range(3)])
+        owner = np.full(21, -1)
+        for t in ftets:
+            v = mesh.nodes[:, mesh.tets[:, t]]
+            B = np.linalg.inv(np.stack([v[:, 1] - v[:, 0], v[:, 2] - v[:, 0], v[:, 3] - v[:, 0]], axis=1))
+            loc = B @ (pts - v[:, :1])
+            owner[(loc.sum(0) <= 1.00000001) & (loc >= -1e-6).all(0)] = t
+        E = interp_in_tets(mesh, field, solution, owner, pts[:, None, :])[:, 0, :]     # (3, 21)
+        dl = pts[:, 1] - pts[:, 0]
+        volts.append(np.sum(simpson_line_weights(21) * (E[0] * dl[0] + E[1] * dl[1] + E[2] * dl[2])))
+    return sum(volts) / len(volts)

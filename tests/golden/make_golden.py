@@ -319,6 +319,11 @@ def robin_gamma():
         out[f"lumped{i}_gamma"] = np.array([lp.get_gamma(k) for k in k0s])
         xs, ys, zs = np.array([1e-3, 2e-3]), np.array([0.5e-3, 0.0]), np.array([0.0, 1e-3])
         out[f"lumped{i}_uinc"] = np.array([lp.get_Uinc(xs, ys, zs, k) for k in k0s])
+    import importlib
+    coord = importlib.import_module("emerge._emerge.coord")
+    yl = np.random.default_rng(9).standard_normal(21) + 1j * np.random.default_rng(10).standard_normal(21)
+    out["line_samples"] = yl
+    out["line_gauss3"] = coord.gauss3_composite(np.linspace(0.0, 3e-3, 21), yl)
     np.savez_compressed(os.path.join(HERE, "robin_gamma.npz"), **out)
 
 

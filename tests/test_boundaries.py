@@ -65,3 +65,12 @@ def test_lumped_port_gamma_and_uinc(golden, i, zp, pw):
     u = np.array([lp.get_Uinc(xs, ys, zs, k) for k in g["k0"]])
     ref = g[f"lumped{i}_uinc"]
     assert np.abs(u - ref).max() <= 1e-13 * np.abs(ref).max()
+
+
+def test_voltage_line_rule_matches_reference(golden):
+    """The lumped-port line integral: the reference's composite 3-point Gauss rule on equally spaced
+    samples (coord.py:24-61) equals per-sample Simpson weights."""
+    from oracle.sparams import simpson_line_weights
+    g = golden("robin_gamma")
+    got = simpson_line_weights(21) @ g["line_samples"]
+    assert abs(got - complex(g["line_gauss3"])) <= 1e-14 * abs(complex(g["line_gauss3"]))

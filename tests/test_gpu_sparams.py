@@ -48,3 +48,22 @@ def test_sparams_other_mesh_vs_oracle(cuda):
     S_dev = sw.sparams(res)[f]
     S_or = osp.sparams(P, {0: x[:, 0], 1: x[:, 1]}, k0_of(f), oracle.dunavant4())
     assert np.abs(S_dev - S_or).max() <= 1e-12
+
+
+def test_lumped_port_sparams_match_oracle(cuda):
+    """A guide with a TE10 port at z=0 and a lumped port on the z=l face: the device S (mode overlap
+    and voltage lines) against the oracle's from the same device solutions."""
+    from oracle import sparams as osp
+    from emerge_b200.ports import LumpedPort
+    P = problems.waveguide()
+    a, b, l = P.dims
+    P.ports = [P.ports[0], LumpedPort(2, P.ports[1].tri_ids, width=a, height=b, direction=(0.0, 1.0, 0.0))]
+    sw = FrequencySweep(P)
+    f = 10e9
+    res = sw.solve([(f, 0), (f, 1)], tol=1e-11, maxit=20000, precond="aux")
+    assert (res.status == 0).all()
+    S = sw.sparams(res)[f]
+    x = res.x.cpu().numpy()
+    So = osp.sparams(P, {0: x[:, 0], 1: x[:, 1]}, k0_of(f), oracle.dunavant4())
+    assert np.abs(S - So).max() <= 1e-9 * max(1.0, np.abs(So).max()), (S, So)
+    assert np.isfinite(S).all()

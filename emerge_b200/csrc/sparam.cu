@@ -162,36 +162,9 @@ __global__ void port_overlap_kernel(long long nn, const double* __restrict__ nod
     double e2x = tx[2] - tx[0], e2y = ty[2] - ty[0], e2z = tz[2] - tz[0];
     double cxp = e1y * e2z - e1z * e2y, cyp = e1z * e2x - e1x * e2z, czp = e1x * e2y - e1y * e2x;
     double area = sqrt(cxp * cxp + cyp * cyp + czp * czp) / 2;
-    // owning tet: vertices and barycentric coefficients (tet_coefficients, ned2_interp.py:59-77)
-    int64_t vid[4];
-    double xs[4], ys[4], zs[4];
-    for (int i = 0; i < 4; i++) {
-        int64_t id = tets[i * nt + T];
-        if (id < 0 || id >= nn) { flag(status, DEV_BAD_INDEX); return; }
-        vid[i] = id;
-        xs[i] = nodes[id]; ys[i] = nodes[nn + id]; zs[i] = nodes[2 * nn + id];
-    }
-    double a[4], b[4], c[4], d[4];
-    for (int i = 0; i < 4; i++) {
-        int j = i == 0 ? 1 : 0, k = i <= 1 ? 2 : 1, l = i <= 2 ? 3 : 2;
-        double sgn = (i % 2 == 0) ? 1.0 : -1.0;
-        a[i] = sgn * tet_det3(xs[j], ys[j], zs[j], xs[k], ys[k], zs[k], xs[l], ys[l], zs[l]);
-        b[i] = -sgn * sp_det1(ys[j], zs[j], ys[k], zs[k], ys[l], zs[l]);
-        c[i] = sgn * sp_det1(xs[j], zs[j], xs[k], zs[k], xs[l], zs[l]);
-        d[i] = -sgn * sp_det1(xs[j], ys[j], xs[k], ys[k], xs[l], ys[l]);
-    }
-    double V = fabs(tet_det3(xs[1] - xs[0], ys[1] - ys[0], zs[1] - zs[0], xs[2] - xs[0], ys[2] - ys[0], zs[2] - zs[0],
-                             xs[3] - xs[0], ys[3] - ys[0], zs[3] - zs[0])) / 6.0;
-    double V1 = 216.0 * V * V * V;
-    // local orientation from global node order (local_mapping of the sorted edge / triangle lists)
-    int rank[4];
-    for (int i = 0; i < 4; i++) {
-        int r = 0;
-        for (int j = 0; j < 4; j++) r += vid[j] < vid[i];
-        rank[i] = r;
-    }
-    const int ep[6] = {0, 0, 0, 1, 3, 2}, eq[6] = {1, 2, 3, 2, 1, 3};
-    const int fv[4][3] = {{0, 1, 2}, {0, 2, 3}, {0, 3, 1}, {1, 2, 3}};
+    // owning tet: interpolation data (tet_coefficients, ned2_interp.py:59-77) and its 20 DOFs
+    TetInterp ti;
+    if (!load_tet_interp(nn, nodes, nt, tets, T, ti)) { flag(status, DEV_BAD_INDEX); return; }
     double2 dof[20];
     for (int k = 0; k < 20; k++) {
         int64_t id = t2f[k * nt + T];
@@ -204,34 +177,8 @@ __global__ void port_overlap_kernel(long long nn, const double* __restrict__ nod
         double px = tx[0] * dpts[npts + p] + tx[1] * dpts[2 * npts + p] + tx[2] * dpts[3 * npts + p];
         double py = ty[0] * dpts[npts + p] + ty[1] * dpts[2 * npts + p] + ty[2] * dpts[3 * npts + p];
         double pz = tz[0] * dpts[npts + p] + tz[1] * dpts[2 * npts + p] + tz[2] * dpts[3 * npts + p];
-        double Fv[4];
-        for (int i = 0; i < 4; i++) Fv[i] = a[i] + b[i] * px + c[i] * py + d[i] * pz;
-        double Er[3] = {0, 0, 0}, Ei[3] = {0, 0, 0};
-        for (int e = 0; e < 6; e++) {
-            int v1 = ep[e], v2 = eq[e];
-            if (rank[v2] < rank[v1]) { int t = v1; v1 = v2; v2 = t; }
-            double L = sp_dist(xs, ys, zs, v1, v2);
-            double2 m1 = dof[e], m2 = dof[10 + e];
-            double wr = m1.x * Fv[v1] + m2.x * Fv[v2], wi = m1.y * Fv[v1] + m2.y * Fv[v2];
-            double gg[3] = {b[v1] * Fv[v2] - b[v2] * Fv[v1], c[v1] * Fv[v2] - c[v2] * Fv[v1], d[v1] * Fv[v2] - d[v2] * Fv[v1]};
-            for (int q = 0; q < 3; q++) { Er[q] += L * wr * gg[q] / V1; Ei[q] += L * wi * gg[q] / V1; }
-        }
-        for (int f = 0; f < 4; f++) {
-            int v1 = fv[f][0], v2 = fv[f][1], v3 = fv[f][2], t;
-            if (rank[v2] < rank[v1]) { t = v1; v1 = v2; v2 = t; }
-            if (rank[v3] < rank[v2]) { t = v2; v2 = v3; v3 = t; }
-            if (rank[v2] < rank[v1]) { t = v1; v1 = v2; v2 = t; }
-            double L1 = sp_dist(xs, ys, zs, v1, v3), L2 = sp_dist(xs, ys, zs, v1, v2);
-            double2 m1 = dof[6 + f], m2 = dof[16 + f];
-            double q1r = m1.x * L1 * Fv[v2], q1i = m1.y * L1 * Fv[v2];
-            double q2r = m2.x * L2 * Fv[v3], q2i = m2.y * L2 * Fv[v3];
-            double g13[3] = {b[v1] * Fv[v3] - b[v3] * Fv[v1], c[v1] * Fv[v3] - c[v3] * Fv[v1], d[v1] * Fv[v3] - d[v3] * Fv[v1]};
-            double g12[3] = {b[v1] * Fv[v2] - b[v2] * Fv[v1], c[v1] * Fv[v2] - c[v2] * Fv[v1], d[v1] * Fv[v2] - d[v2] * Fv[v1]};
-            for (int q = 0; q < 3; q++) {
-                Er[q] += (-q1r * g13[q] + q2r * g12[q]) / V1;
-                Ei[q] += (-q1i * g13[q] + q2i * g12[q]) / V1;
-            }
-        }
+        double Er[3], Ei[3];
+        eval_field(ti, dof, px, py, pz, Er, Ei);
         const double2* m = shape + (long long)(p * ntri + it);  // shape (3, npts, ntri)
         double2 mx = m[0], my = m[(long long)npts * ntri], mz = m[2LL * npts * ntri];
         // E . conj(m)

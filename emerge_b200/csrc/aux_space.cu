@@ -460,9 +460,66 @@ __global__ void __launch_bounds__(TC_WARPS * 32) mpnn_layer_tc_kernel(
     float* M = sM[wl];
     const long long total = na * S;
     const long long ntiles = (total + 7) / 8;
+    // S a multiple of 8: the 8 rows of a tile are systems s0..s0+7 of one node y, so the neighbour
+    // list is read once and each neighbour's 8 rows are loaded together (8 loads in flight instead
+    // of one dependent index-then-row chain per row).  Each row still sums its neighbours in list
+    // order, so the result is the same as the row-by-row gather below.
+    const bool same_node = (S & 7) == 0;
     for (long long tile = (long long)blockIdx.x * TC_WARPS + wl; tile < ntiles; tile += (long long)gridDim.x * TC_WARPS) {
         const long long w0 = tile * 8;
         bool has[2] = {false, false};
+        if (same_node) {
+            const long long y = w0 / S;
+            const int t = atype[y], k0 = nptr[y], k1 = nptr[y + 1];
+            has[t] = true;
+            float2 in[8], m[8];
+            if (layer == 0) {
+#pragma unroll
+                for (int r = 0; r < 8; r++) {
+                    TX xv = x[w0 + r];
+                    in[r] = make_float2((float)xv.x * sWin[t][lane], (float)xv.y * sWin[t][lane]);
+                    m[r] = make_float2(0.f, 0.f);
+                }
+                for (int k = k0; k < k1; k++) {
+                    const long long j = nbr[k];
+                    const float wj = sWin[atype[j]][lane];
+                    const TX* xj = x + j * S + (w0 - y * S);
+                    TX v[8];
+#pragma unroll
+                    for (int r = 0; r < 8; r++) v[r] = xj[r];
+#pragma unroll
+                    for (int r = 0; r < 8; r++) {
+                        m[r].x += (float)v[r].x * wj;
+                        m[r].y += (float)v[r].y * wj;
+                    }
+                }
+            } else {
+#pragma unroll
+                for (int r = 0; r < 8; r++) {
+                    in[r] = Hin[(w0 + r) * NN_C + lane];
+                    m[r] = make_float2(0.f, 0.f);
+                }
+                for (int k = k0; k < k1; k++) {
+                    const float2* hj = Hin + ((long long)nbr[k] * S + (w0 - y * S)) * NN_C + lane;
+                    float2 v[8];
+#pragma unroll
+                    for (int r = 0; r < 8; r++) v[r] = hj[r * NN_C];
+#pragma unroll
+                    for (int r = 0; r < 8; r++) {
+                        m[r].x += v[r].x;
+                        m[r].y += v[r].y;
+                    }
+                }
+            }
+            const float idg = inv_deg[y];
+#pragma unroll
+            for (int r = 0; r < 8; r++) {
+                A[(2 * r) * TC_LD + lane] = wmma::__float_to_tf32(in[r].x);
+                A[(2 * r + 1) * TC_LD + lane] = wmma::__float_to_tf32(in[r].y);
+                M[(2 * r) * TC_LD + lane] = wmma::__float_to_tf32(m[r].x * idg);
+                M[(2 * r + 1) * TC_LD + lane] = wmma::__float_to_tf32(m[r].y * idg);
+            }
+        } else
         for (int r = 0; r < 8; r++) {
             long long w = w0 + r;
             float2 in = make_float2(0.f, 0.f), m = make_float2(0.f, 0.f);

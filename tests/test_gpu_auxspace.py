@@ -124,6 +124,14 @@ def test_network_forward_backward_vs_oracle(guide):
     # the tensor-core inference form used inside the solve (TF32 inputs): same network, looser bound
     zt = net.infer(torch.from_numpy(x).to(aux.device)).cpu().numpy()
     assert np.abs(zt - zo).max() <= 5e-3 * np.abs(zo).max(), np.abs(zt - zo).max() / np.abs(zo).max()
+    # S a multiple of 8 takes the one-node-per-tile gather of the inference kernel
+    x16 = (rng.standard_normal((aux.n_aux, 16)) + 1j * rng.standard_normal((aux.n_aux, 16))).astype(np.complex64)
+    z16 = net.infer(torch.from_numpy(x16).to(aux.device)).cpu().numpy()
+    zo16, _ = oa.mpnn_forward(p, x16.astype(np.complex128), ptr, nbr, atype)
+    assert np.abs(z16 - zo16).max() <= 5e-3 * np.abs(zo16).max(), np.abs(z16 - zo16).max() / np.abs(zo16).max()
+    # each column depends on its own input column only: the row-by-row gather (S = 3) agrees
+    z3 = net.infer(torch.from_numpy(x16[:, :3].copy()).to(aux.device)).cpu().numpy()
+    assert np.abs(z3 - z16[:, :3]).max() <= 1e-6 * np.abs(z16).max()
 
 
 def test_training_reduces_correction_loss_and_learned_solve_converges(guide, golden):

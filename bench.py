@@ -42,10 +42,11 @@ def peaks():
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
+    """nvidia-smi clocks and throttle reasons sampled every 100 ms during the timed region."""
     FIELDS = "index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown," \
              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown," \
              "clocks_event_reasons.sw_power_cap"
+    PERIOD_MS = 100
 
     def __init__(self, gpu_index: int):
         self.gpu = gpu_index
@@ -55,30 +56,47 @@ class ClockSampler:
     def __enter__(self):
         fd, self.path = tempfile.mkstemp(suffix=".csv")
         os.close(fd)
+        self.n0 = 0
         try:
             self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", str(self.PERIOD_MS)],
                                          stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
         except OSError:
             self.proc = None
+        # the timed region starts only once the sampler is producing rows
+        t0 = time.perf_counter()
+        while self.proc is not None and time.perf_counter() - t0 < 10.0 and self.proc.poll() is None:
+            self.n0 = len(self._rows())
+            if self.n0 > 0:
+                break
+            time.sleep(0.02)
         return self
 
     def __exit__(self, *a):
         if self.proc is not None:
+            time.sleep(1.5 * self.PERIOD_MS / 1e3)      # one more sample as the region ends
             self.proc.terminate()
             try:
                 self.proc.wait(timeout=5)
             except subprocess.TimeoutExpired:
                 self.proc.kill()
 
-    def summary(self) -> dict:
+    def _rows(self) -> list:
         rows = []
         if self.path and os.path.exists(self.path):
-            for line in open(self.path):
-                parts = [p.strip() for p in line.split(",")]
-                if len(parts) >= 9:
-                    rows.append(parts)
+            with open(self.path) as fh:
+                for line in fh:
+                    parts = [p.strip() for p in line.split(",")]
+                    if len(parts) >= 9:
+                        rows.append(parts)
+        return rows
+
+    def summary(self) -> dict:
+        rows = self._rows()
+        if self.path and os.path.exists(self.path):
             os.unlink(self.path)
+        # rows written after the region started (the row the start waited for is before it)
+        rows = rows[self.n0:] or rows[-1:]
         if not rows:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
         sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
@@ -86,7 +104,7 @@ class ClockSampler:
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         reasons = sorted({n for r in rows for n, v in zip(names, r[5:9]) if v.lower() == "active"})
         return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(smax) if smax else None,
-                "reasons": reasons, "samples": len(rows)}
+                "reasons": reasons, "samples": len(rows), "period_ms": self.PERIOD_MS}
 
 
 def dist_init(gpus: int):
@@ -157,8 +175,10 @@ def run_reference(args, ws, rank):
     P = problems.cavity()
     t_all = []
     cb = None
+    # each step a bounded sample, sized so the whole run stays near two and a half minutes
+    per_step = max(1.0, min(8.0, 150.0 / (args.warmup + args.steps)))
     for i in range(args.warmup + args.steps):
-        cb = cpu_baseline(P, seconds_target=8.0)
+        cb = cpu_baseline(P, seconds_target=per_step)
         if i >= args.warmup:
             t_all.append(cb["value"])
     v = float(np.mean(t_all))
@@ -317,7 +337,7 @@ def sweep_section(P_cavity, cavity_systems: int, cavity_maxit: int) -> dict:
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="native", choices=["native", "reference"])
     ap.add_argument("--no-sweep", action="store_true")

@@ -93,6 +93,8 @@ _SIGS = {
     "emfem_adam_step": ([_vp, _i64, _vp, _vp, _vp, _vp, ctypes.c_float, ctypes.c_float, ctypes.c_float,
                          ctypes.c_float, ctypes.c_float, _i32], _i32),
     "emfem_ned2_tri_abc2": ([_vp, _i64, _vp, _i64, _vp, _dbl, _dbl, _vp], _i32),
+    "emfem_ned2_bma_tri_matrices": ([_vp, _i64, _vp, _i64, _vp, _i64, _vp, _vp, _vp, _vp, _dbl, _vp, _vp], _i32),
+    "emfem_ned2_tri_field": ([_vp, _i64, _vp, _i64, _vp, _i64, _vp, _vp, _vp, _i64, _vp, _i32, _vp, _i32, _dbl, _dbl, _vp, _vp], _i32),
     "emfem_point_field_dot": ([_vp, _i64, _vp, _i64, _vp, _vp, _i64, _i64, _vp, _vp, _vp, _i32, _vp, _vp], _i32),
     "emfem_sweep_spmv_noalloc": ([_vp, _i64, _vp, _vp, _vp, _vp, _i32, _vp, _i64, _vp, _vp, _vp, _vp, _vp, _i32,
                                   _vp, _vp, _vp, _vp], _i32),

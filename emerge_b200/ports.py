@@ -18,12 +18,12 @@ from dataclasses import dataclass, field
 
 import numpy as np
 
-from .constants import C0, MU0, Z0
+from .constants import C0, EPS0, MU0, Z0
 
 
 @dataclass
 class PortFrame:
-    origin: np.ndarray
+    origin: np.ndarray = field(default_factory=lambda: np.zeros(3))
     xax: np.ndarray = field(default_factory=lambda: np.array([1.0, 0.0, 0.0]))
     yax: np.ndarray = field(default_factory=lambda: np.array([0.0, 1.0, 0.0]))
     zax: np.ndarray = field(default_factory=lambda: np.array([0.0, 0.0, 1.0]))
@@ -48,6 +48,14 @@ class PortFrame:
         return (X[0] * ex + Y[0] * ey + Zv[0] * ez,
                 X[1] * ex + Y[1] * ey + Zv[1] * ez,
                 X[2] * ex + Y[2] * ey + Zv[2] * ez)
+
+    def in_local_cs(self, xyz: np.ndarray) -> np.ndarray:
+        """(3, n) global points -> (3, n) local coordinates."""
+        return np.array(self.to_local(*np.asarray(xyz, dtype=np.float64)))
+
+    def in_global_basis(self, v: np.ndarray) -> np.ndarray:
+        """(3, n) local vector components -> global basis."""
+        return np.array(self.to_global_vec(*v))
 
 
 @dataclass
@@ -162,3 +170,117 @@ class LumpedPort:
 
 def k0_of(f: float) -> float:
     return 2 * np.pi * f / C0
+
+
+@dataclass
+class ModalPort:
+    """Wave port whose mode comes from the 2-D eigen-analysis of its face (``ModalPort``,
+    ``src/emerge/_emerge/physics/microwave/microwave_bc.py:469-753``, filled by ``modal_analysis``,
+    ``microwave_3d.py:474-650``).  Call :meth:`analyse` once; the sweep then uses it like any mode port:
+
+    * beta(k0) = sqrt(beta_m^2 + k0^2 (1 - (f_m / f)^2)) for TE/TM, beta_m k0 / k0_m for TEM (:716-723);
+    * Z_mode: Z0 (TEM), k0 c mu0 / beta (TE), beta / (k0 c eps0) (TM) (``PortBC.Zmode``, :218-230);
+    * the port field is norm · q(k0) · polarity · E_mode (:650-660) with q = sqrt(Z_mode / Z0) and
+      norm = 1 / sqrt(|P q_m^2|), P the mode's power flux (``compute_avg_power_flux``) and q_m the amplitude
+      factor ``modal_analysis`` evaluates right after adding the mode (:648): that of the selected entry of
+      the modes added so far, i.e. of the first accepted mode when ``mode_number`` is 0;
+    * polarity: +1 for the first mode, sign(Re sum e_i^2) for later ones at the same frequency (``add_mode``
+      compares each new mode with the last one stored, which is itself, :692-700);
+    * modes sorted by descending beta (``sort_modes``, :613-637, no alignment vectors); the sweep uses entry
+      ``mode_number``.
+
+    Voltage-line characteristic impedances of TEM ports (``_find_tem_conductors``, :607-632) are not built.
+    """
+    port_number: int
+    tri_ids: np.ndarray
+    frame: PortFrame = field(default_factory=PortFrame)
+    power: float = 1.0
+    active: bool = False
+    mode_number: int = 0
+    TEM: bool = False
+
+    def __post_init__(self):
+        self.tri_ids = np.asarray(self.tri_ids, dtype=np.int64)
+        self.modes = []
+        self.field = None
+        self._ur = None
+
+    def analyse(self, mesh, er, ur, freq: float, nmodes: int = 6, pec_edges=None, sig=None, direct: bool = True,
+                target_kz=None, target_neff=None, device=None) -> "ModalPort":
+        """Modes of the face at ``freq``; er, ur (3, 3, n_tri) complex tensors of the port triangles."""
+        from . import modal
+        modes, fld = modal.modal_analysis(mesh, self.tri_ids, self.frame, er, ur, freq, nmodes, direct, self.TEM,
+                                          target_kz, target_neff, sig, pec_edges, device, sort=False)
+        added = []
+        for i, m in enumerate(modes):
+            m.polarity = 1.0 if i == 0 else float(np.sign(np.sum(m.modefield * m.modefield).real))
+            added.append(m)
+            ref = added[min(len(added) - 1, self.mode_number)]
+            P = modal.mode_power(fld.mesh, fld, m.modefield, m.k0, ur, m.beta, device)
+            m.power = P
+            m.norm_factor = float(np.sqrt(1.0 / abs(P * self._qmode_of(ref, m.k0) ** 2)))
+        self.modes = sorted(added, key=lambda m: m.beta.real, reverse=True)
+        self.field = fld
+        self._ur = np.asarray(ur, dtype=np.complex128)
+        return self
+
+    @property
+    def mode(self):
+        if not self.modes:
+            raise ValueError("ModalPort: no modes; call analyse() first")
+        return self.modes[min(len(self.modes) - 1, self.mode_number)]
+
+    @property
+    def polarization(self) -> float:
+        return self.mode.polarity
+
+    def modetype(self, k0: float = 0.0) -> str:
+        return "TEM" if self.TEM else self.mode.modetype
+
+    @staticmethod
+    def _beta_of(m, TEM: bool, k0: float) -> complex:
+        if TEM:
+            return m.beta / m.k0 * k0
+        f = k0 * C0 / (2 * np.pi)
+        return np.sqrt(m.beta ** 2 + k0 ** 2 * (1 - (m.freq / f) ** 2))
+
+    def _qmode_of(self, m, k0: float) -> float:
+        mt = "TEM" if self.TEM else m.modetype
+        beta = self._beta_of(m, self.TEM, k0)
+        if mt == "TEM":
+            zm = Z0
+        elif mt == "TE":
+            zm = k0 * C0 / beta * MU0
+        else:
+            zm = beta / (k0 * C0 * EPS0)
+        return np.sqrt(zm / Z0)
+
+    def get_beta(self, k0: float):
+        return self._beta_of(self.mode, self.TEM, k0)
+
+    def get_gamma(self, k0: float) -> complex:
+        return 1j * self.get_beta(k0)
+
+    def Zmode(self, k0: float):
+        return self._qmode_of(self.mode, k0) ** 2 * Z0
+
+    def qmode(self, k0: float):
+        return self._qmode_of(self.mode, k0)
+
+    def amplitude(self) -> float:
+        return self.mode.norm_factor
+
+    def shape_global(self, x, y, z) -> np.ndarray:
+        """Unit-free mode E (global basis) at per-triangle points (npts, n_tri), column t in triangle t."""
+        from . import modal
+        pts = np.stack([np.asarray(x, float), np.asarray(y, float), np.asarray(z, float)])
+        return modal.mode_fields_global(self.field.mesh, self.field, self.mode.modefield, pts)
+
+    def port_mode_3d_global(self, x, y, z, k0: float) -> np.ndarray:
+        return self.amplitude() * self.qmode(k0) * self.polarization * self.shape_global(x, y, z)
+
+    def get_Uinc(self, x, y, z, k0: float) -> np.ndarray:
+        return -2j * self.get_beta(k0) * self.port_mode_3d_global(x, y, z, k0)
+
+    def uinc_scale(self, k0: float) -> complex:
+        return -2j * self.get_beta(k0) * self.qmode(k0) * self.polarization * self.amplitude()

@@ -98,3 +98,23 @@ def pec_cavity(nx=8, ny=4, nz=12, a=22.86e-3, b=10.16e-3, d=30e-3, seed=0, jitte
                                                                       (2, 0.0), (2, d))])
     return Problem("pec_cavity", mesh, fld, identity_tensors(nt), identity_tensors(nt), [], walls,
                    np.zeros(0), (a, b, d))
+
+
+def with_modal_ports(P: Problem, freq: float, nmodes: int = 1, device=None) -> Problem:
+    """The same problem with every wave port replaced by a ``ModalPort`` on the same face and frame,
+    its mode found by the face eigen-analysis at ``freq``.  Port-face materials are those of the first
+    tet owning each triangle (``modal_analysis``, ``microwave_3d.py:536-540``); the edges of the PEC wall
+    triangles are PEC for the mode (``assemble_bma_matrices``, ``assembler.py:168-177``)."""
+    import dataclasses
+    from .ports import ModalPort
+    mesh = P.mesh
+    pec_edges = mesh.edges[:, mesh.tri_to_edge[:, np.asarray(P.pec_tris, dtype=np.int64)].ravel()]
+    ports = []
+    for port in P.ports:
+        tid = np.asarray(port.tri_ids, dtype=np.int64)
+        owner = mesh.tri_to_tet[0, tid]
+        mp = ModalPort(port.port_number, tid, port.frame, power=port.power)
+        mp.analyse(mesh, P.er[:, :, owner], P.ur[:, :, owner], freq, nmodes=max(nmodes, 1), pec_edges=pec_edges,
+                   device=device)
+        ports.append(mp)
+    return dataclasses.replace(P, ports=ports)

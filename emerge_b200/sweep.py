@@ -199,8 +199,9 @@ class FrequencySweep:
 
     # ---------------------------------------------------------------- S-parameters
     def _port_sp_data(self) -> list:
-        """Per port: owning tets, node ids, unit mode shape at the quadrature points and the TE weight
-        1/mean(diag ur) of the owning tet (``_compute_s_data``, ``MW/microwave_3d.py:1250-1303``)."""
+        """Per port: owning tets, node ids, unit mode shape at the quadrature points and the weight of the
+        owning tet by mode type: 1/sqrt(mean diag ur / mean diag er) (TEM), 1/mean(diag ur) (TE),
+        1/mean(diag er) (TM) (``_compute_s_data``, ``MW/microwave_3d.py:1295-1303``)."""
         if getattr(self, "_spdata", None) is not None:
             return self._spdata
         P, mesh, dev = self.problem, self.problem.mesh, self.device
@@ -212,8 +213,15 @@ class FrequencySweep:
             owner = mesh.tri_to_tet[0, tid]
             pts = np.einsum("cvs,vp->cps", mesh.nodes[:, tn], dp[1:4])               # (3, npts, ntri)
             shape = port.shape_global(pts[0], pts[1], pts[2]).astype(np.complex128)
-            ur = P.ur[:, :, owner]
-            const = (1.0 / ((ur[0, 0] + ur[1, 1] + ur[2, 2]) / 3)).astype(np.complex128)
+            ur, er = P.ur[:, :, owner], P.er[:, :, owner]
+            mt = port.modetype(0.0) if hasattr(port, "modetype") else "TE"
+            if mt == "TEM":
+                const = 1.0 / np.sqrt((ur[0, 0] + ur[1, 1] + ur[2, 2]) / (er[0, 0] + er[1, 1] + er[2, 2]))
+            elif mt == "TE":
+                const = 1.0 / ((ur[0, 0] + ur[1, 1] + ur[2, 2]) / 3)
+            else:
+                const = 1.0 / ((er[0, 0] + er[1, 1] + er[2, 2]) / 3)
+            const = np.asarray(const, dtype=np.complex128)
             out.append(dict(n=len(tid),
                             tri_tet=torch.from_numpy(np.ascontiguousarray(owner)).to(dev),
                             tri_nodes=torch.from_numpy(np.ascontiguousarray(tn)).to(dev),

@@ -185,6 +185,32 @@ int emfem_sweep_spmv(emfem_handle h, int64_t n, const int32_t *indptr, const int
 int emfem_ned2_tri_abc2(emfem_handle h, int64_t n_nodes, const double *nodes, int64_t n_sel,
                         const int64_t *tri_nodes, double cf_re, double cf_im, void *blocks);
 
+/* ---- boundary-mode analysis (port modes) ----------------------------------------------------
+ * Replaces generalized_matrix_GQ / _matrix_builder (ASM/generalized_eigen_hb.py:257-458), called by
+ * Assembler.assemble_bma_matrices (ASM/assembler.py:110-187): the 14x14 blocks A ("E") and B ("B") of
+ * the mixed Nedelec-2 / Lagrange-2 triangle element of every port-face triangle, DOF order
+ * tri_to_field of NedelecLegrange2 (elements/nedleg2.py:140-150), for the eigenproblem
+ * A e = -beta^2 B e.  local_nodes (2, n_nodes) f64: x then y in the port's local frame; tris (3, n_tris)
+ * and tri_to_edge (3, n_tris) i64; edges (2, n_edges) i64 (any node order; it fixes the edge
+ * orientation); er, ur (9, n_tris) c128 row-major 3x3 per triangle (the reference's (3,3,N) layout);
+ * A, B (n_tris, 196) c128 row-major, i.e. the reference's dataE / dataB.  Device arrays. */
+int emfem_ned2_bma_tri_matrices(emfem_handle h, int64_t n_nodes, const double *local_nodes, int64_t n_tris,
+                                const int64_t *tris, int64_t n_edges, const int64_t *edges,
+                                const int64_t *tri_to_edge, const void *er, const void *ur, double k0, void *A,
+                                void *B);
+
+/* A port-mode vector x (n_field) c128 of the NedelecLegrange2 field evaluated at points inside known
+ * triangles: what = 0 gives E (ned2_tri_interp_full, elements/nedleg2.py -> elements/ned2_interp.py:616-685),
+ * what = 1 the curl form of ned2_tri_interp_curl (:687-760) without its constant j/(k0 c0 mu0):
+ * (d_y E_z - j beta E_y, -d_x E_z + j beta E_x, curl_t E_t), each component times the diagonal of
+ * diadic (3, n_tris) c128 (ur^-1), or of the identity when diadic is NULL.  pts (2, npts, n_tris) f64
+ * local coordinates, column t inside triangle t; tri_to_field (14, n_tris) i64; out (3, npts, n_tris)
+ * c128 in the port's local frame.  Device arrays. */
+int emfem_ned2_tri_field(emfem_handle h, int64_t n_nodes, const double *local_nodes, int64_t n_tris,
+                         const int64_t *tris, int64_t n_edges, const int64_t *edges, const int64_t *tri_to_edge,
+                         const int64_t *tri_to_field, int64_t n_field, const void *x, int npts, const double *pts,
+                         int what, double beta_re, double beta_im, const void *diadic, void *out);
+
 /* ---- S-parameter overlap integrals -------------------------------------------------------------
  * For the port triangles (tri_nodes (3, n_tri) i64, their owning tets tri_tet (n_tri) i64) and nsys
  * solutions x (n_field, nsys) c128, computes the port-mode overlap of every solution,

@@ -34,6 +34,17 @@ Fixtures
 ``abc2.npz``           the reference's ``abc_order_2_matrix`` (``ASM/robin_abc_order2.py:350-373``) on the
     element_small mesh's z=0 and x=a faces with coefficient 0.3-0.7j: the touched 64-entry blocks.
 
+``bma.npz``            the boundary-mode-analysis (port-mode) matrices of the reference
+    (``ASM/generalized_eigen_hb.py:257-458``): (1) ``_matrix_builder`` on 40 jittered 2-D triangles with
+    random vertex and edge orientations and general complex εr/μr tensors (the 14×14 A and B blocks);
+    (2) the whole chain of ``Assembler.assemble_bma_matrices`` (``ASM/assembler.py:110-187``) on the z=0
+    face of a 10×5×2 WR-90 guide: ``SurfaceMesh`` (``mesh3d.py:717-880``), ``NedelecLegrange2``
+    (``elements/nedleg2.py:102-166``), E/B CSR, the PEC DOFs of the four walls, and the eigenvalues of the
+    dense ``SolverLAPACK`` path (``solver.py:780-810``) at 10 GHz, for an air-filled guide and one half
+    filled with εr = 2.2 - 0.01j; for the top mode, its post-processed vector, E and H from
+    ``ned2_tri_interp_full`` / ``ned2_tri_interp_curl`` (``elements/ned2_interp.py:616-760``) at the face's
+    order-4 points and its power flux ``compute_avg_power_flux`` (``MW/port_functions.py:21-36``).
+
 Fixtures can be generated one at a time: ``python tests/golden/make_golden.py mesh_conn``.
 
 ``ASM/`` = ``src/emerge/_emerge/physics/microwave/assembly/``; ``MW/`` = ``src/emerge/_emerge/physics/microwave/``.
@@ -327,8 +338,129 @@ def robin_gamma():
     np.savez_compressed(os.path.join(HERE, "robin_gamma.npz"), **out)
 
 
+def bma():
+    import importlib
+    mesh3d = importlib.import_module("emerge._emerge.mesh3d")
+    nl2 = importlib.import_module("emerge._emerge.elements.nedleg2")
+    ge = importlib.import_module("emerge._emerge.physics.microwave.assembly.generalized_eigen_hb")
+    out = {}
+    # (1) element blocks on a jittered 2-D patch with shuffled orientations
+    rng = np.random.default_rng(21)
+    gx, gy = np.meshgrid(np.linspace(0, 3e-3, 6), np.linspace(0, 2e-3, 5), indexing="ij")
+    pts = np.stack([gx.ravel(), gy.ravel()])
+    pts = pts + rng.uniform(-0.15, 0.15, pts.shape) * 5e-4
+    nid = lambda i, j: i * 5 + j
+    tris = []
+    for i in range(5):
+        for j in range(4):
+            tris += [[nid(i, j), nid(i + 1, j), nid(i + 1, j + 1)], [nid(i, j), nid(i + 1, j + 1), nid(i, j + 1)]]
+    tris = np.array(tris).T
+    tris = np.array([rng.permutation(t) for t in tris.T]).T.astype(np.int64)
+    ekey = {}
+    t2e = np.zeros((3, tris.shape[1]), dtype=np.int64)
+    for t in range(tris.shape[1]):
+        for k, (p, q) in enumerate(((0, 1), (1, 2), (0, 2))):
+            key = tuple(sorted((int(tris[p, t]), int(tris[q, t]))))
+            if key not in ekey:
+                ekey[key] = len(ekey)
+            t2e[k, t] = ekey[key]
+    edges = np.zeros((2, len(ekey)), dtype=np.int64)
+    for key, e in ekey.items():
+        edges[:, e] = key if rng.random() < 0.5 else key[::-1]
+    nt, ne, nn = tris.shape[1], edges.shape[1], pts.shape[1]
+    t2f = np.zeros((14, nt), dtype=np.int64)
+    t2f[:3] = t2e; t2f[3] = np.arange(nt) + ne; t2f[4:7] = t2e + ne + nt; t2f[7] = np.arange(nt) + 2 * ne + nt
+    t2f[8:11] = tris + 2 * ne + 2 * nt; t2f[11:14] = t2e + 2 * ne + 2 * nt + nn
+    er = (rng.uniform(1, 4, (3, 3, nt)) + 1j * rng.uniform(-0.2, 0.2, (3, 3, nt)))
+    ur = (rng.uniform(0.3, 0.6, (3, 3, nt)) + 1j * rng.uniform(-0.1, 0.1, (3, 3, nt)))
+    for i in range(3):
+        ur[i, i] += 1.5
+    half = np.arange(nt) % 2 == 0
+    for i in range(3):
+        for j in range(3):
+            if i != j:
+                ur[i, j, half] = 0
+    k0 = 2 * np.pi * 30e9 / K.C0
+    local = np.concatenate([pts, np.zeros((1, nn))])
+    dE, dB, rows, cols = ge._matrix_builder(local, tris, edges, t2f, ur, er, k0)
+    out.update(el_nodes=local, el_tris=tris, el_edges=edges, el_t2f=t2f, el_er=er, el_ur=ur, el_k0=k0,
+               el_A=dE.reshape(nt, 196), el_B=dB.reshape(nt, 196), el_rows=rows.reshape(nt, 196),
+               el_cols=cols.reshape(nt, 196))
+    # (2) the port face of a WR-90 guide through the reference's own surface mesh and field classes
+    a, b = 22.86e-3, 10.16e-3
+    nodes, tets = box_tet_mesh(10, 5, 2, a, b, 5e-3, seed=0)
+    m = TetMesh(nodes, tets)
+    tri_ids = m.tris_on_plane(2, 0.0)
+    orig = types.SimpleNamespace(tris=m.tris, nodes=m.nodes, edges=m.edges)
+    sm = mesh3d.SurfaceMesh(orig, tri_ids, (0.0, 0.0, -1.0))
+    cs = R.cs.CoordinateSystem(R.cs.Axis(np.array([1.0, 0, 0])), R.cs.Axis(np.array([0, 1.0, 0])),
+                               R.cs.Axis(np.array([0, 0, 1.0])), np.array([0.0, 0, 0]))
+    f = nl2.NedelecLegrange2(sm, cs)
+    # PEC: every wall triangle's edges mapped into the surface mesh (ASM/assembler.py:168-177)
+    walls = np.concatenate([m.tris_on_plane(0, 0.0), m.tris_on_plane(0, a), m.tris_on_plane(1, 0.0),
+                            m.tris_on_plane(1, b)])
+    pec = []
+    for ie in m.tri_to_edge[:, walls].ravel():
+        i2 = sm.from_source_edge(ie)
+        if i2 is not None:
+            pec.extend(list(f.edge_to_field[:, i2]))
+    pec = set(int(p) for p in pec)
+    solve_ids = np.array([i for i in range(f.n_field) if i not in pec], dtype=np.int64)
+    freq = 10e9
+    k0 = 2 * np.pi * freq / K.C0
+    out.update(wg_a=a, wg_b=b, wg_k0=k0, wg_tri_ids=tri_ids, wg_sm_nodes=sm.nodes, wg_sm_tris=sm.tris,
+               wg_sm_edges=sm.edges, wg_sm_tri_to_edge=sm.tri_to_edge, wg_n_field=f.n_field,
+               wg_tri_to_field=f.tri_to_field, wg_edge_to_field=f.edge_to_field, wg_solve_ids=solve_ids)
+    lap = R.solver.SolverLAPACK("golden")
+    for tag, fill in (("air", None), ("half", 2.2 - 0.01j)):
+        er = np.zeros((3, 3, sm.n_tris), dtype=np.complex128)
+        ur = np.zeros_like(er)
+        for i in range(3):
+            er[i, i] = 1.0; ur[i, i] = 1.0
+        if fill is not None:
+            cy = sm.nodes[1][sm.tris].mean(axis=0)
+            for i in range(3):
+                er[i, i, cy < b / 2] = fill
+        E, B = ge.generelized_eigenvalue_matrix(f, er, ur, cs._basis, k0)
+        Asel = E[np.ix_(solve_ids, solve_ids)]
+        Bsel = B[np.ix_(solve_ids, solve_ids)]
+        ermean = 1.0 if fill is None else np.mean(np.diagonal(er[:, :, :]).ravel())
+        lam, vecs = lap.eig(Asel, Bsel, 6, 0.7 * k0 * ermean, "LM", sign=-1.0)
+        out[f"wg_{tag}_er"] = er
+        out[f"wg_{tag}_E_data"], out[f"wg_{tag}_B_data"] = E.data, B.data
+        out[f"wg_{tag}_indptr"], out[f"wg_{tag}_indices"] = E.indptr, E.indices
+        out[f"wg_{tag}_lambda"] = lam
+        top = int(np.argmax(np.sqrt(-lam).real))
+        out[f"wg_{tag}_mode"] = vecs[:, top]
+        # the mode as modal_analysis post-processes it (MW/microwave_3d.py:576-620): full vector,
+        # phase-normalised, beta capped; its E and H at the face's order-4 points and its power flux
+        em = np.zeros(f.n_field, dtype=np.complex128)
+        em[solve_ids] = vecs[:, top]
+        em = em * np.exp(-1j * np.angle(em[np.argmax(np.abs(em))]))
+        beta = min(k0 * np.sqrt(np.max(er) * np.max(ur)), np.emath.sqrt(-lam[top]))
+        dp = R.optimized.gaus_quad_tri(4)
+        v = sm.nodes[:, sm.tris]
+        pts = np.einsum("cvs,vp->cps", v, dp[1:4]).reshape(3, -1)
+        loc = np.array(cs.in_local_cs(pts[0], pts[1], pts[2]))
+        interp = importlib.import_module("emerge._emerge.elements.ned2_interp")
+        Ei = np.array(interp.ned2_tri_interp_full(loc[:2].copy(), em, sm.tris, f.local_nodes, f.tri_to_field))
+        urinv = np.zeros_like(ur)
+        for i in range(sm.n_tris):
+            urinv[:, :, i] = R.optimized.matinv(ur[:, :, i])
+        Hi = np.array(interp.ned2_tri_interp_curl(loc[:2].copy(), em, sm.tris, f.local_nodes, f.tri_to_field,
+                                                  urinv, complex(beta)))
+        pf = importlib.import_module("emerge._emerge.physics.microwave.port_functions")
+        out[f"wg_{tag}_emode"] = em
+        out[f"wg_{tag}_beta"] = complex(beta)
+        out[f"wg_{tag}_interpE"] = Ei
+        out[f"wg_{tag}_interpH"] = Hi
+        out[f"wg_{tag}_power"] = complex(pf.compute_avg_power_flux(f, em, k0, ur, beta))
+    out["wg_normal"] = sm.normals[:, 0]
+    np.savez_compressed(os.path.join(HERE, "bma.npz"), **out)
+
+
 if __name__ == "__main__":
-    which = sys.argv[1:] or ["element_small", "config1", "mesh_conn", "robin_gamma", "abc2"]
+    which = sys.argv[1:] or ["element_small", "config1", "mesh_conn", "robin_gamma", "abc2", "bma"]
     if "element_small" in which:
         m, f = element_small()
         robin_small(m, f)
@@ -340,6 +472,8 @@ if __name__ == "__main__":
         robin_gamma()
     if "abc2" in which:
         abc2()
+    if "bma" in which:
+        bma()
     for fn in sorted(os.listdir(HERE)):
         if fn.endswith(".npz"):
             print(fn, os.path.getsize(os.path.join(HERE, fn)))

@@ -306,26 +306,33 @@ def batch_section(n_meshes: int = 64, seed: int = 7, reps: int = 3) -> dict:
     return out
 
 
-def sweep_section(P_cavity, cavity_systems: int, cavity_maxit: int) -> dict:
+SWEEP_ARMS = ("plain_block_jacobi_fp64", "aux_jacobi_fp64", "aux_jacobi_mixed", "learned_fp64", "learned_mixed")
+
+
+def sweep_section(P_cavity, cavity_systems: int, cavity_maxit: int, arm_names=SWEEP_ARMS) -> dict:
     from emerge_b200 import problems
     wg = problems.waveguide()
     wg_sys = [(float(f), q) for f in np.linspace(8e9, 12e9, 16) for q in range(2)]
-    net, trep = train_network(wg, np.linspace(8.125e9, 11.875e9, 9))
-    arms = {
-        "plain_block_jacobi_fp64": sweep_measure(wg, wg_sys, 40000, "fp64", "block_jacobi"),
-        "aux_jacobi_fp64": sweep_measure(wg, wg_sys, 40000, "fp64", "aux"),
-        "aux_jacobi_mixed": sweep_measure(wg, wg_sys, 40000, "mixed", "aux", fallback=True),
-        "learned_fp64": sweep_measure(wg, wg_sys, 40000, "fp64", "learned", network=net, fallback=True),
-        "learned_mixed": sweep_measure(wg, wg_sys, 40000, "mixed", "learned", network=net, fallback=True),
+    net, trep = None, None
+    if any(a.startswith("learned") for a in arm_names):
+        net, trep = train_network(wg, np.linspace(8.125e9, 11.875e9, 9))
+    spec = {
+        "plain_block_jacobi_fp64": lambda: sweep_measure(wg, wg_sys, 40000, "fp64", "block_jacobi"),
+        "aux_jacobi_fp64": lambda: sweep_measure(wg, wg_sys, 40000, "fp64", "aux"),
+        "aux_jacobi_mixed": lambda: sweep_measure(wg, wg_sys, 40000, "mixed", "aux", fallback=True),
+        "learned_fp64": lambda: sweep_measure(wg, wg_sys, 40000, "fp64", "learned", network=net, fallback=True),
+        "learned_mixed": lambda: sweep_measure(wg, wg_sys, 40000, "mixed", "learned", network=net, fallback=True),
     }
-    plain = arms["plain_block_jacobi_fp64"]["solves_per_s"]
-    best_learned = max(arms["learned_fp64"]["solves_per_s"], arms["learned_mixed"]["solves_per_s"])
+    arms = {name: spec[name]() for name in SWEEP_ARMS if name in arm_names}
+    plain = arms.get("plain_block_jacobi_fp64", {}).get("solves_per_s")
+    learned = [arms[a]["solves_per_s"] for a in ("learned_fp64", "learned_mixed") if a in arms]
     out = {"waveguide_6000_tets": {
         "workload": "22.86x10.16x50 mm air guide, 10x5x20 hex grid x6 tets, TE10 ports, 16 frequencies 8-12 GHz "
                     "x 2 ports = 32 systems in one batched launch, FP64 true relative residual 1e-8",
         "arms": arms, "training": trep,
-        "learned_vs_plain_solves_per_s": best_learned / plain if plain > 0 else None,
-        "aux_jacobi_vs_plain_solves_per_s": arms["aux_jacobi_fp64"]["solves_per_s"] / plain if plain > 0 else None}}
+        "learned_vs_plain_solves_per_s": max(learned) / plain if plain and learned else None,
+        "aux_jacobi_vs_plain_solves_per_s": arms["aux_jacobi_fp64"]["solves_per_s"] / plain
+        if plain and "aux_jacobi_fp64" in arms else None}}
     cav_sys = [(float(f), 0) for f in P_cavity.freqs[:: max(1, len(P_cavity.freqs) // cavity_systems)][:cavity_systems]]
     out["cavity_384000_tets"] = {
         "workload": "the assembly workload, BiCGStab with bounded iterations (no preconditioner here reaches 1e-8)",
@@ -344,6 +351,8 @@ def main():
     ap.add_argument("--no-batch", action="store_true")
     ap.add_argument("--sweep-systems", type=int, default=4)
     ap.add_argument("--sweep-maxit", type=int, default=2000)
+    ap.add_argument("--sweep-arms", default=",".join(SWEEP_ARMS),
+                    help="comma-separated waveguide sweep arms to measure (default: all)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--grid", type=int, default=40, help="cavity hex grid size (40 = the 384 000-tet workload)")
     ap.add_argument("--variant", type=int, default=-1, help="assembly kernel variant (default: autotune)")
@@ -450,7 +459,8 @@ def main():
     if rank == 0:
         sweep = None
         if not args.no_sweep:
-            sweep = sweep_section(P, args.sweep_systems, args.sweep_maxit)
+            sweep = sweep_section(P, args.sweep_systems, args.sweep_maxit,
+                                  tuple(a for a in args.sweep_arms.split(",") if a))
         batch = None if args.no_batch else batch_section()
         cb = None if args.no_cpu_baseline else cpu_baseline(P)
         out = {

@@ -14,6 +14,7 @@ restatement of the reference's numba integrator plus SciPy's COO→CSR) on the h
 from __future__ import annotations
 
 import argparse
+import gc
 import json
 import os
 import subprocess
@@ -252,6 +253,54 @@ def train_network(P, train_freqs, steps: int = 300) -> tuple:
                  "objective": "mean ||G za - e||^2 / ||e||^2 over (residual, correction) pairs"}
 
 
+def precision_section(reps: int = 3) -> dict:
+    """The precision workload: assembly of the full 1 497 600-tet substrate box (80x60x52 grid x 6), and
+    on a downsized member (20x15x13 grid, 23 400 tets) the FP32-inner / FP64-refinement sweep against
+    the FP64 sweep at two frequencies x two lumped ports (relative difference of the solutions per
+    system; the FP64 solve itself is checked against the direct solve in the tests)."""
+    import torch
+    from emerge_b200 import problems
+    from emerge_b200.assembly import CsrPlan, DeviceMesh
+    from emerge_b200.sweep import FrequencySweep
+    t0 = time.perf_counter()
+    P = problems.substrate_box()
+    t_mesh = time.perf_counter() - t0
+    dev = torch.device("cuda", torch.cuda.current_device())
+    dm = DeviceMesh(P.mesh, P.field, dev)
+    plan = CsrPlan(dm)
+    er = torch.from_numpy(np.ascontiguousarray(P.er)).to(dev)
+    ur = torch.from_numpy(np.ascontiguousarray(P.ur)).to(dev)
+    E, B = plan.assemble(er, ur)
+    stream = torch.cuda.current_stream(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(reps):
+        E, B = plan.assemble(er, ur, E, B)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / reps
+    out = {"workload": "substrate box 16x12x10.4 mm, 80x60x52 hex grid x6 tets, eps_r 3.5-0.007j below grid plane 10, "
+                       "PEC strip W/10 on the interface, lumped ports at both ends, order-2 ABC on the end faces",
+           "n_tets": int(P.mesh.n_tets), "n_dof": int(P.field.n_field), "nnz": int(plan.nnz),
+           "assembly_ms": ms, "assembly_tets_per_s": P.mesh.n_tets / (ms / 1e3), "host_mesh_seconds": t_mesh}
+    del E, B, plan, dm, er, ur
+    gc.collect()
+    torch.cuda.empty_cache()
+    Q = problems.substrate_box(20, 15, 13)
+    sw = FrequencySweep(Q)
+    systems = [(f, q) for f in (4.5e9, 8e9) for q in range(2)]
+    r64 = sweep_measure(Q, systems, 40000, "fp64", "aux", tol=1e-8)
+    rmx = sweep_measure(Q, systems, 40000, "mixed", "aux", tol=1e-8, fallback=True)
+    a = sw.solve(systems, tol=1e-8, maxit=40000, precond="aux").x
+    b = sw.solve(systems, tol=1e-8, maxit=40000, precond="aux", precision="mixed", fallback=True).x
+    diff = (torch.linalg.vector_norm(a - b, dim=0) / torch.linalg.vector_norm(a, dim=0)).cpu().numpy()
+    out["downsized"] = {"workload": "same family, 20x15x13 grid x6 (23 400 tets), 4.5 and 8 GHz x 2 ports to 1e-8",
+                        "fp64_aux": r64, "mixed_aux_with_fallback": rmx,
+                        "mixed_vs_fp64_rel_diff": [float(v) for v in diff]}
+    return out
+
+
 def batch_section(n_meshes: int = 64, seed: int = 7, reps: int = 3) -> dict:
     """Uneven meshes assembled in one launch: box meshes with seeded grid sizes giving 5 000-200 000
     tets each, per-tet eps' ~ U[1,12], tan d ~ U[0,5e-3], diagonal mu_r ~ U[1,2] on a seeded 10 % of tets
@@ -349,6 +398,7 @@ def main():
     ap.add_argument("--impl", default="native", choices=["native", "reference"])
     ap.add_argument("--no-sweep", action="store_true")
     ap.add_argument("--no-batch", action="store_true")
+    ap.add_argument("--no-precision", action="store_true")
     ap.add_argument("--sweep-systems", type=int, default=4)
     ap.add_argument("--sweep-maxit", type=int, default=2000)
     ap.add_argument("--sweep-arms", default=",".join(SWEEP_ARMS),
@@ -462,6 +512,7 @@ def main():
             sweep = sweep_section(P, args.sweep_systems, args.sweep_maxit,
                                   tuple(a for a in args.sweep_arms.split(",") if a))
         batch = None if args.no_batch else batch_section()
+        precision = None if args.no_precision else precision_section()
         cb = None if args.no_cpu_baseline else cpu_baseline(P)
         out = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
@@ -482,6 +533,7 @@ def main():
             "plan_seconds": t_plan, "nnz": int(nnz), "autotune": tuning,
             "sweep": sweep,
             "batched_meshes": batch,
+            "precision_workload": precision,
             "cpu_baseline": cb,
         }
         print(json.dumps(out), flush=True)

@@ -7,6 +7,13 @@ configurations (no public dataset is involved; meshes come from :func:`mesh.box_
   takes the diagonal εr = εr'(1−j·tanδ) of the last of 8 seeded axis-aligned blocks containing its
   centroid (air elsewhere), εr' ~ U[1,10], tanδ ~ U[1e-4,1e-2], μr = 1; one TE10 port on z=0 and PEC
   on every other face.  The configuration names no excitation, so this port is a choice.
+* :func:`substrate_box` — the precision workload: an 80×60×52 hex grid (1 497 600 tets) box with a
+  substrate of εr = 3.5 − 0.007j under air and a PEC strip of width W/10 on the interface.  52/5 is not
+  an integer, so the interface sits on grid plane round(nz/5) = 10 (z = 10/52 H); its nodes are jittered
+  in x and y only, so the interface and the strip stay planar.  Excitation and walls are choices (the
+  configuration names none): the strip runs along y between lumped ports (strip to ground, 50 Ω) on the
+  two end faces, the rest of the end faces is a second-order absorbing boundary, and the floor (ground),
+  lid and side walls are PEC.
 """
 from __future__ import annotations
 
@@ -16,7 +23,7 @@ import numpy as np
 
 from .mesh import TetMesh, box_tet_mesh
 from .nedelec2 import Nedelec2
-from .ports import PortFrame, RectangularWaveguidePort
+from .ports import LumpedPort, PortFrame, RectangularWaveguidePort
 
 
 @dataclass
@@ -98,6 +105,46 @@ def pec_cavity(nx=8, ny=4, nz=12, a=22.86e-3, b=10.16e-3, d=30e-3, seed=0, jitte
                                                                       (2, 0.0), (2, d))])
     return Problem("pec_cavity", mesh, fld, identity_tensors(nt), identity_tensors(nt), [], walls,
                    np.zeros(0), (a, b, d))
+
+
+def substrate_box(nx=80, ny=60, nz=52, W=16e-3, L=12e-3, H=10.4e-3, er_sub=3.5 - 0.007j, seed=0, jitter=0.1,
+                  nfreq=51, fmin=1e9, fmax=8e9, abc_order=2) -> Problem:
+    """Shielded microstrip section (see the module docstring); the strip runs along y."""
+    from .boundaries import AbsorbingBoundary
+    nodes, tets = box_tet_mesh(nx, ny, nz, W, L, H, jitter=0.0, seed=seed)
+    ki = int(round(nz / 5))
+    zi = H * ki / nz
+    I = np.arange(nodes.shape[1]) % (nx + 1)
+    J = (np.arange(nodes.shape[1]) // (nx + 1)) % (ny + 1)
+    K = np.arange(nodes.shape[1]) // ((nx + 1) * (ny + 1))
+    interior = (I > 0) & (I < nx) & (J > 0) & (J < ny) & (K > 0) & (K < nz)
+    rng = np.random.default_rng(seed)
+    h = np.array([W / nx, L / ny, H / nz])
+    d = rng.uniform(-1.0, 1.0, (3, int(interior.sum()))) * jitter * h[:, None]
+    d[2, K[interior] == ki] = 0.0                      # the interface plane stays flat
+    nodes = nodes.copy()
+    nodes[:, interior] += d
+    mesh = TetMesh(nodes, tets)
+    fld = Nedelec2(mesh)
+    nt = mesh.n_tets
+    cz = nodes[2][tets].mean(axis=0)
+    er = identity_tensors(nt)
+    for i in range(3):
+        er[i, i, cz < zi] = er_sub
+    cx = mesh.tri_centers()
+    half = W / 20
+    iface = mesh.tris_on_plane(2, zi)
+    strip = iface[np.abs(cx[0, iface] - W / 2) <= half]
+    ports, robin = [], []
+    for q, y0 in enumerate((0.0, L)):
+        face = mesh.tris_on_plane(1, y0)
+        sheet = face[(np.abs(cx[0, face] - W / 2) <= half) & (cx[2, face] <= zi)]
+        ports.append(LumpedPort(q + 1, sheet, width=2 * half, height=zi, direction=(0.0, 0.0, 1.0), Z0=50.0))
+        robin.append(AbsorbingBoundary(np.setdiff1d(face, sheet), order=abc_order))
+    walls = np.concatenate([mesh.tris_on_plane(0, 0.0), mesh.tris_on_plane(0, W), mesh.tris_on_plane(2, 0.0),
+                            mesh.tris_on_plane(2, H), strip])
+    return Problem("substrate_box", mesh, fld, er, identity_tensors(nt), ports, walls,
+                   np.linspace(fmin, fmax, nfreq), (W, L, H), robin)
 
 
 def with_modal_ports(P: Problem, freq: float, nmodes: int = 1, device=None) -> Problem:

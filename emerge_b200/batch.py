@@ -14,9 +14,17 @@ union CSR lists exactly mesh k's columns, in mesh k's own order.  Each value is 
 tets in the same order as a separate assembly.  :meth:`MeshBatch.csr` therefore returns every mesh's
 matrices bit for bit equal to assembling that mesh alone.
 
+:class:`BatchSweep` goes one step further: the frequency sweeps of all meshes run as ONE batched Krylov
+call (``emfem_krylov_solve_grouped``).  The union CSR is permuted so that every mesh's DOF pairs form one
+contiguous range of whole 256-pair blocks (padded with eliminated rows); each mesh is a group of the
+same number of systems, and each system keeps its own BiCGStab scalars and convergence test while one
+graph-captured iteration serves all of them.
+
 ``ASM/`` = ``src/emerge/_emerge/physics/microwave/assembly/``.
 """
 from __future__ import annotations
+
+import time
 
 import numpy as np
 import torch
@@ -25,7 +33,7 @@ from scipy.sparse import csr_matrix
 from .assembly import CsrPlan, DeviceMesh
 from .connectivity import DeviceTetMesh
 
-__all__ = ["MeshBatch"]
+__all__ = ["MeshBatch", "BatchSweep"]
 
 
 class MeshBatch:
@@ -84,3 +92,172 @@ class MeshBatch:
             raise RuntimeError("MeshBatch: a row couples two meshes (inputs are not disjoint)")
         new_ptr = np.concatenate([[0], np.cumsum(ends - starts)])
         return csr_matrix((vals[sel], cols.astype(np.int32), new_ptr.astype(np.int32)), shape=(n, n))
+
+
+class BatchSweep:
+    """Sweeps of several problems (``problems.Problem``: mesh, materials, ports, PEC, Robin boundaries)
+    solved together.  Assembly: one fused launch for all meshes (:class:`MeshBatch`).  Solve: one
+    batched call per :meth:`solve`, ``nsys`` systems per mesh."""
+
+    PAIR_ALIGN = 256
+
+    def __init__(self, problems, device=None):
+        import ctypes  # noqa: F401
+        from .assembly import DeviceMesh
+        from .sweep import FrequencySweep
+        self.problems = list(problems)
+        dev = torch.device("cuda", torch.cuda.current_device()) if device is None else torch.device(device)
+        self.device = dev
+        self.batch = MeshBatch([(P.mesh.nodes, P.mesh.tets) for P in self.problems], dev)
+        er = torch.cat([torch.from_numpy(np.ascontiguousarray(P.er)) for P in self.problems], dim=2).to(dev)
+        ur = torch.cat([torch.from_numpy(np.ascontiguousarray(P.ur)) for P in self.problems], dim=2).to(dev)
+        E, B = self.batch.assemble(er, ur)                      # one launch for every mesh
+        del er, ur
+        # grouped layout: mesh g's DOF pairs at [hoff[g], hoff[g] + H_g) of each half, padded to 256
+        G = len(self.problems)
+        Hg = np.array([P.field.n_field // 2 for P in self.problems], dtype=np.int64)
+        Hp = (Hg + self.PAIR_ALIGN - 1) // self.PAIR_ALIGN * self.PAIR_ALIGN
+        self.hoff = np.concatenate([[0], np.cumsum(Hp)]).astype(np.int64)
+        self.Hg = Hg
+        self.h = int(self.hoff[-1])
+        self.n = 2 * self.h
+        self.pair_group = torch.from_numpy(np.repeat(np.arange(G, dtype=np.int32), Hp)).to(dev)
+        # union DOF -> grouped DOF
+        b = self.batch
+        ne, nf = b.dmesh.n_edges, b.dmesh.n_tris
+        Hu = ne + nf
+        eo, to = b.edge_off.astype(np.int64), b.tri_off.astype(np.int64)
+        ne_g = np.diff(eo)
+        x = np.arange(Hu, dtype=np.int64)
+        is_e = x < ne
+        g_e = np.searchsorted(eo, x[is_e], side="right") - 1
+        g_f = np.searchsorted(to, x[~is_e] - ne, side="right") - 1
+        first = np.empty(Hu, dtype=np.int64)
+        first[is_e] = self.hoff[g_e] + (x[is_e] - eo[g_e])
+        first[~is_e] = self.hoff[g_f] + ne_g[g_f] + (x[~is_e] - ne - to[g_f])
+        perm = np.concatenate([first, first + self.h])              # union DOF u -> grouped row
+        inv = np.full(self.n, -1, dtype=np.int64)
+        inv[perm] = np.arange(2 * Hu)
+        # grouped CSR: rows moved, columns relabelled (their order inside a row is kept)
+        indptr_u = b.plan.indptr.to(torch.int64)
+        lens_u = indptr_u[1:] - indptr_u[:-1]
+        inv_d = torch.from_numpy(inv).to(dev)
+        has = inv_d >= 0
+        lens = torch.zeros(self.n, dtype=torch.int64, device=dev)
+        lens[has] = lens_u[inv_d[has]]
+        indptr = torch.zeros(self.n + 1, dtype=torch.int64, device=dev)
+        indptr[1:] = torch.cumsum(lens, 0)
+        nnz = int(indptr[-1])
+        row_of_slot = torch.repeat_interleave(torch.arange(self.n, device=dev), lens)
+        start_u = torch.zeros(self.n, dtype=torch.int64, device=dev)
+        start_u[has] = indptr_u[:-1][inv_d[has]]
+        slot = start_u[row_of_slot] + (torch.arange(nnz, device=dev) - indptr[:-1][row_of_slot])
+        perm_d = torch.from_numpy(perm).to(dev)
+        self.indices = perm_d[b.plan.indices.to(torch.int64)[slot]].to(torch.int32).contiguous()
+        self.indptr = indptr.to(torch.int32).contiguous()
+        self.E = E[slot].contiguous()
+        self.B = B[slot].contiguous()
+        self.nnz = nnz
+        del slot, row_of_slot, start_u, lens
+        # per mesh: Robin / port terms and port vectors (built on each mesh's own numbering), mask
+        self.sweeps = []
+        mask = torch.zeros(self.n, dtype=torch.uint8, device=dev)
+        rows_l, ptr_l, cols_l, port_l, vals_l = [], [], [], [], []
+        nrow_off = 0
+        nslot_off = 0
+        self.n_ports = 0
+        for g, P in enumerate(self.problems):
+            fs = object.__new__(FrequencySweep)
+            fs.problem, fs.device = P, dev
+            fs.dmesh = DeviceMesh(P.mesh, P.field, dev)
+            fs.n = P.field.n_field
+            fs._build_ports()
+            self.sweeps.append(fs)
+            loc = self.local_to_grouped(g)
+            m = np.ones(fs.n, dtype=np.uint8)
+            m[P.pec_ids] = 0
+            mask[loc] = torch.from_numpy(m).to(dev)
+            self.n_ports = max(self.n_ports, fs.n_ports)
+            if fs.patch_rows.numel():
+                rows_l.append(loc[fs.patch_rows.long()].to(torch.int32))
+                ptr_l.append((fs.patch_rowptr[:-1] + nslot_off).to(torch.int32))
+                cols_l.append(loc[fs.patch_cols.long()].to(torch.int32))
+                port_l.append(fs.patch_port)
+                vals_l.append(fs.patch_vals)
+                nrow_off += fs.patch_rows.numel()
+                nslot_off += fs.patch_vals.numel()
+        if self.n_ports > 8:
+            raise ValueError("at most 8 ports + Robin terms per mesh")
+        i32 = dict(dtype=torch.int32, device=dev)
+        self.mask = mask
+        self.patch_rows = torch.cat(rows_l) if rows_l else torch.zeros(0, **i32)
+        self.patch_rowptr = torch.cat(ptr_l + [torch.tensor([nslot_off], **i32)]) if ptr_l else torch.zeros(1, **i32)
+        self.patch_cols = torch.cat(cols_l) if cols_l else torch.zeros(0, **i32)
+        self.patch_port = torch.cat(port_l) if port_l else torch.zeros(0, **i32)
+        self.patch_vals = torch.cat(vals_l) if vals_l else torch.zeros(0, dtype=torch.complex128, device=dev)
+        self._ws = None
+
+    def local_to_grouped(self, g: int) -> torch.Tensor:
+        """Rows of the grouped system holding mesh g's DOFs, in that mesh's own DOF order."""
+        H = int(self.Hg[g])
+        d = torch.arange(2 * H, device=self.device)
+        return torch.where(d < H, self.hoff[g] + d, self.h + self.hoff[g] + d - H)
+
+    def solve(self, systems, tol: float = 1e-8, maxit: int = 20000, precond: str = "block_jacobi",
+              method: str = "bicgstab"):
+        """systems: one list of (frequency, port) per mesh, all of the same length (<= 64).  Returns one
+        ``SolveResult`` per mesh, solutions in that mesh's own DOF numbering."""
+        import ctypes
+        from ._lib import ERR_NOT_CONVERGED, Handle, check, lib, ptr
+        from .ports import k0_of
+        from .sweep import METHOD, PRECOND, SolveResult
+        G = len(self.problems)
+        if len(systems) != G or len({len(s) for s in systems}) != 1:
+            raise ValueError("give the same number of systems for every mesh")
+        nsys = len(systems[0])
+        if PRECOND[precond] > 2:
+            raise ValueError("grouped solves take precond none, jacobi or block_jacobi")
+        npt = max(self.n_ports, 1)
+        k0 = np.zeros(G * nsys)
+        gam = np.zeros((G * nsys, npt), dtype=np.complex128)
+        b = torch.zeros((self.n, nsys), dtype=torch.complex128, device=self.device)
+        for g, (fs, sl) in enumerate(zip(self.sweeps, systems)):
+            loc = self.local_to_grouped(g)
+            freqs = [f for f, _ in sl]
+            k0[g * nsys:(g + 1) * nsys] = fs.k0sq(freqs)
+            if fs.n_ports:
+                gam[g * nsys:(g + 1) * nsys, :fs.n_ports] = fs.gammas(freqs)
+            if fs.problem.ports:
+                b[loc] = fs.rhs(sl)
+        ga = np.ascontiguousarray(np.stack([gam.real, gam.imag], axis=-1).reshape(-1))
+        sz = ctypes.c_size_t()
+        check(lib().emfem_krylov_workspace_size_grouped(self.n, self.nnz, nsys, G, ctypes.byref(sz)),
+              "emfem_krylov_workspace_size_grouped")
+        if self._ws is None or self._ws.numel() < sz.value:
+            self._ws = torch.empty(sz.value, dtype=torch.uint8, device=self.device)
+        x = torch.zeros_like(b)
+        st = (ctypes.c_int * (G * nsys))()
+        it = (ctypes.c_int * (G * nsys))()
+        rr = (ctypes.c_double * (G * nsys))()
+        h = Handle.get(self.device)
+        t0 = time.perf_counter()
+        rc = lib().emfem_krylov_solve_grouped(
+            h.h, METHOD[method], self.n, self.nnz, ptr(self.indptr), ptr(self.indices), ptr(self.E), ptr(self.B), G,
+            ptr(self.pair_group), nsys, (ctypes.c_double * (G * nsys))(*k0), self.patch_rows.numel(),
+            ptr(self.patch_rows), ptr(self.patch_rowptr), ptr(self.patch_cols), ptr(self.patch_vals),
+            ptr(self.patch_port), self.n_ports, (ctypes.c_double * len(ga))(*ga), ptr(self.mask), ptr(b), ptr(x),
+            tol, maxit, PRECOND[precond], ptr(self._ws), self._ws.numel(), st, it, rr)
+        torch.cuda.synchronize(self.device)
+        dt = time.perf_counter() - t0
+        if rc not in (0, ERR_NOT_CONVERGED):
+            check(rc, "emfem_krylov_solve_grouped")
+        out = []
+        for g, sl in enumerate(systems):
+            sel = slice(g * nsys, (g + 1) * nsys)
+            out.append(SolveResult(x[self.local_to_grouped(g)].contiguous(), np.array(st[sel]), np.array(it[sel]),
+                                   np.array(rr[sel]), list(sl), dt))
+        return out
+
+    def sparams(self, g: int, res) -> dict:
+        """S-parameters of mesh g's solved systems (``FrequencySweep.sparams``)."""
+        return self.sweeps[g].sparams(res)

@@ -55,7 +55,15 @@ struct OpArgs {
     int n_ports;
     const double* gamma;            // [S][n_ports] complex (interleaved)
     const uint8_t* mask;            // [n]
+    // grouped systems (emfem_krylov_solve_grouped): group of every DOF pair i < hh, or null.  Row i
+    // (or i - hh) of system column s then belongs to system pg[i] * S + s of the per-system arrays.
+    const int* pg;
+    long long hh;
 };
+
+__device__ __forceinline__ int sys_of_row(const int* pg, long long hh, long long i, int S, int s) {
+    return pg ? pg[i < hh ? i : i - hh] * S + s : s;
+}
 
 template <typename T>
 __device__ __forceinline__ double2 dotu(T a, T b) {  // a^T b contribution (unconjugated)
@@ -207,7 +215,8 @@ __global__ void __launch_bounds__(VB) spmv_kernel(OpArgs a, const typename V2<R>
                     bi += b.x * xi + b.y * xr;
                 }
             }
-            double k2 = a.k0sq[s];
+            const int sy = sys_of_row(a.pg, a.hh, i, S, s);
+            double k2 = a.k0sq[sy];
             yr = er - k2 * br;
             yi = ei - k2 * bi;
             int pr = a.patch_of_row ? a.patch_of_row[i] : -1;
@@ -222,7 +231,7 @@ __global__ void __launch_bounds__(VB) spmv_kernel(OpArgs a, const typename V2<R>
                         pr_ += v.x * xv.x - v.y * xv.y;
                         pi_ += v.x * xv.y + v.y * xv.x;
                     }
-                    double gr = a.gamma[2 * (s * a.n_ports + q)], gi = a.gamma[2 * (s * a.n_ports + q) + 1];
+                    double gr = a.gamma[2 * (sy * a.n_ports + q)], gi = a.gamma[2 * (sy * a.n_ports + q) + 1];
                     yr += gr * pr_ - gi * pi_;
                     yi += gr * pi_ + gi * pr_;
                 }
@@ -282,14 +291,26 @@ __device__ void stop(SysState& q, int status) {
 }
 
 // One block per system: fixed-order sum of the block partials, then the scalar recurrences.
+// Grouped systems (G > 1): block sys = g S + s sums only group g's blocks, gblk[g] .. gblk[g + 1] of
+// a DOF-pair launch (nbh blocks), and for a launch over all rows also the same range in the second
+// half (two_halves).
 __global__ void reduce_update_kernel(const double2* __restrict__ partial, int nblocks, int S, int ncomp,
-                                     SysState* st, int mode, int maxit, double tol, int nsys) {
+                                     SysState* st, int mode, int maxit, double tol, int nsys, int G = 1,
+                                     const int* __restrict__ gblk = nullptr, int two_halves = 0, int nbh = 0) {
     __shared__ double2 red[VB];
     __shared__ double2 sums[3];
-    int s = blockIdx.x;
+    const int sys = blockIdx.x;
+    const int s = G > 1 ? sys % S : sys;
+    int b0 = 0, cnt = nblocks, total = nblocks;
+    if (G > 1) {
+        b0 = gblk[sys / S];
+        cnt = gblk[sys / S + 1] - b0;
+        total = two_halves ? 2 * cnt : cnt;
+    }
     for (int comp = 0; comp < ncomp; comp++) {
         double2 acc = make_double2(0, 0);
-        for (int b = threadIdx.x; b < nblocks; b += VB) {
+        for (int k = threadIdx.x; k < total; k += VB) {
+            int b = k < cnt ? b0 + k : nbh + b0 + (k - cnt);
             double2 v = partial[((long long)comp * nblocks + b) * S + s];
             acc.x += v.x; acc.y += v.y;
         }
@@ -303,7 +324,7 @@ __global__ void reduce_update_kernel(const double2* __restrict__ partial, int nb
         __syncthreads();
     }
     if (threadIdx.x != 0) return;
-    SysState& q = st[s];
+    SysState& q = st[sys];
     double2 c0 = sums[0], c1 = ncomp > 1 ? sums[1] : make_double2(0, 0);
     double c2 = ncomp > 2 ? sums[2].x : 0.0;
     switch (mode) {
@@ -314,7 +335,7 @@ __global__ void reduce_update_kernel(const double2* __restrict__ partial, int nb
         z.bn2 = c0.x; z.rn2 = c1.x; z.tol2 = tol * tol * c0.x;
         z.iters = 0; z.status = 0; z.restart = 0; z.rh2 = 0;
         z.active = (s < nsys) && (z.bn2 > 0) && (z.rn2 > z.tol2);
-        st[s] = z;
+        st[sys] = z;
         break;
     }
     case UPD_SET_RHO:
@@ -413,7 +434,8 @@ __global__ void __launch_bounds__(VB) cocg_init_kernel(long long h, int S, int p
 }
 
 template <typename R>
-__global__ void __launch_bounds__(VB) cocg_update_kernel(long long h, int S, int precond, const SysState* __restrict__ st,
+__global__ void __launch_bounds__(VB) cocg_update_kernel(long long h, int S, int precond, const int* __restrict__ pg,
+                                                         const SysState* __restrict__ st,
                                                          typename V2<R>::T* __restrict__ x, typename V2<R>::T* __restrict__ r,
                                                          typename V2<R>::T* __restrict__ z, const typename V2<R>::T* __restrict__ p,
                                                          const typename V2<R>::T* __restrict__ q, const typename V2<R>::T* __restrict__ minv,
@@ -424,7 +446,7 @@ __global__ void __launch_bounds__(VB) cocg_update_kernel(long long h, int S, int
     int s = (int)(g % S);
     double2 rz = make_double2(0, 0), rr = make_double2(0, 0);
     if (i < h) {
-        double2 al = st[s].alpha;
+        double2 al = st[sys_of_row(pg, h, i, S, s)].alpha;
         R ar = (R)al.x, ai = (R)al.y;
         T rv2[2];
 #pragma unroll
@@ -446,13 +468,13 @@ __global__ void __launch_bounds__(VB) cocg_update_kernel(long long h, int S, int
 }
 
 template <typename R>
-__global__ void cocg_pupdate_kernel(long long n, int S, const SysState* __restrict__ st, const typename V2<R>::T* __restrict__ z,
-                                    typename V2<R>::T* __restrict__ p) {
+__global__ void cocg_pupdate_kernel(long long n, int S, const int* __restrict__ pg, const SysState* __restrict__ st,
+                                    const typename V2<R>::T* __restrict__ z, typename V2<R>::T* __restrict__ p) {
     long long g = (long long)blockIdx.x * VB + threadIdx.x;
     if (g >= n * S) return;
-    int s = (int)(g % S);
-    if (!st[s].active) return;
-    double2 b = st[s].beta;
+    const int sy = sys_of_row(pg, n / 2, g / S, S, (int)(g % S));
+    if (!st[sy].active) return;
+    double2 b = st[sy].beta;
     R br = (R)b.x, bi = (R)b.y;
     typename V2<R>::T zv = z[g], pv = p[g];
     p[g] = mk2<R>(zv.x + br * pv.x - bi * pv.y, zv.y + br * pv.y + bi * pv.x);
@@ -478,7 +500,8 @@ __global__ void __launch_bounds__(VB) bicg_init_kernel(long long n, int S, const
 
 // p = r + beta (p - omega v); p_hat = M^-1 p   (thread per DOF pair)
 template <typename R>
-__global__ void __launch_bounds__(VB) bicg_p_kernel(long long h, int S, int precond, const SysState* __restrict__ st,
+__global__ void __launch_bounds__(VB) bicg_p_kernel(long long h, int S, int precond, const int* __restrict__ pg,
+                                                    const SysState* __restrict__ st,
                                                     const typename V2<R>::T* __restrict__ r, typename V2<R>::T* __restrict__ p,
                                                     const typename V2<R>::T* __restrict__ v, typename V2<R>::T* __restrict__ ph,
                                                     const typename V2<R>::T* __restrict__ minv, typename V2<R>::T* __restrict__ rh) {
@@ -487,9 +510,10 @@ __global__ void __launch_bounds__(VB) bicg_p_kernel(long long h, int S, int prec
     long long i = g / S;
     int s = (int)(g % S);
     if (i >= h) return;
-    double2 b = st[s].beta, w = st[s].omega;
+    const int sy = sys_of_row(pg, h, i, S, s);
+    double2 b = st[sy].beta, w = st[sy].omega;
     R br = (R)b.x, bi = (R)b.y, wr = (R)w.x, wi = (R)w.y;
-    if (st[s].restart) {
+    if (st[sy].restart) {
         rh[i * S + s] = r[i * S + s];
         rh[(i + h) * S + s] = r[(i + h) * S + s];
     }
@@ -510,7 +534,8 @@ __global__ void __launch_bounds__(VB) bicg_p_kernel(long long h, int S, int prec
 
 // s = r - alpha v (stored in r); s_hat = M^-1 s
 template <typename R>
-__global__ void __launch_bounds__(VB) bicg_s_kernel(long long h, int S, int precond, const SysState* __restrict__ st,
+__global__ void __launch_bounds__(VB) bicg_s_kernel(long long h, int S, int precond, const int* __restrict__ pg,
+                                                    const SysState* __restrict__ st,
                                                     typename V2<R>::T* __restrict__ r, const typename V2<R>::T* __restrict__ v,
                                                     typename V2<R>::T* __restrict__ sh, const typename V2<R>::T* __restrict__ minv) {
     typedef typename V2<R>::T T;
@@ -518,7 +543,7 @@ __global__ void __launch_bounds__(VB) bicg_s_kernel(long long h, int S, int prec
     long long i = g / S;
     int s = (int)(g % S);
     if (i >= h) return;
-    double2 a = st[s].alpha;
+    double2 a = st[sys_of_row(pg, h, i, S, s)].alpha;
     R ar = (R)a.x, ai = (R)a.y;
     T sn[2];
 #pragma unroll
@@ -536,7 +561,8 @@ __global__ void __launch_bounds__(VB) bicg_s_kernel(long long h, int S, int prec
 
 // x += alpha p_hat + omega s_hat; r = s - omega t; partial (r_hat, r) and ||r||^2
 template <typename R>
-__global__ void __launch_bounds__(VB) bicg_x_kernel(long long n, int S, const SysState* __restrict__ st,
+__global__ void __launch_bounds__(VB) bicg_x_kernel(long long n, int S, const int* __restrict__ pg,
+                                                    const SysState* __restrict__ st,
                                                     typename V2<R>::T* __restrict__ x, typename V2<R>::T* __restrict__ r,
                                                     const typename V2<R>::T* __restrict__ ph, const typename V2<R>::T* __restrict__ sh,
                                                     const typename V2<R>::T* __restrict__ t, const typename V2<R>::T* __restrict__ rh,
@@ -545,8 +571,8 @@ __global__ void __launch_bounds__(VB) bicg_x_kernel(long long n, int S, const Sy
     long long g = (long long)blockIdx.x * VB + threadIdx.x;
     double2 c0 = make_double2(0, 0), c1 = c0;
     if (g < n * S) {
-        int s = (int)(g % S);
-        double2 a = st[s].alpha, w = st[s].omega;
+        const int sy = sys_of_row(pg, n / 2, g / S, S, (int)(g % S));
+        double2 a = st[sy].alpha, w = st[sy].omega;
         R ar = (R)a.x, ai = (R)a.y, wr = (R)w.x, wi = (R)w.y;
         T xv = x[g], pv = ph[g], sv = sh[g], rv = r[g], tv = t[g];
         xv.x += ar * pv.x - ai * pv.y + wr * sv.x - wi * sv.y;
@@ -589,7 +615,7 @@ __global__ void __launch_bounds__(VB) residual_kernel(long long n, int S, const 
 }
 
 // Operator entry (row, col) of system s (E - k0^2 B + patch), used by the preconditioner setup.
-__device__ __forceinline__ double2 row_value(const OpArgs& a, long long row, long long col, int s) {
+__device__ __forceinline__ double2 row_value(const OpArgs& a, long long row, long long col, int sy) {
     const double2* Ev = (const double2*)a.E;
     const double2* Bv = (const double2*)a.B;
     int lo = a.indptr[row], hi = a.indptr[row + 1] - 1;
@@ -598,7 +624,7 @@ __device__ __forceinline__ double2 row_value(const OpArgs& a, long long row, lon
         while (lo < hi) { int mid = (lo + hi) >> 1; if (a.indices[mid] < col) lo = mid + 1; else hi = mid; }
         if (a.indices[lo] == col) {
             double2 e = Ev[lo];
-            double k2 = a.k0sq[s];
+            double k2 = a.k0sq[sy];
             v = e;
             if (Bv) { double2 b = Bv[lo]; v.x -= k2 * b.x; v.y -= k2 * b.y; }
         }
@@ -609,7 +635,7 @@ __device__ __forceinline__ double2 row_value(const OpArgs& a, long long row, lon
         for (int j = a.patch_rowptr[pr]; j < a.patch_rowptr[pr + 1]; j++) {
             if (a.patch_cols[j] != col) continue;
             int q = a.patch_port[j];
-            double gr = a.gamma[2 * (s * a.n_ports + q)], gi = a.gamma[2 * (s * a.n_ports + q) + 1];
+            double gr = a.gamma[2 * (sy * a.n_ports + q)], gi = a.gamma[2 * (sy * a.n_ports + q) + 1];
             double2 pv = Pv[j];
             v.x += gr * pv.x - gi * pv.y;
             v.y += gr * pv.y + gi * pv.x;
@@ -628,12 +654,13 @@ __global__ void precond_setup_kernel(OpArgs a, int precond, typename V2<R>::T* _
     long long i = g / S;
     int s = (int)(g % S);
     long long j = i + h;
+    const int sy = sys_of_row(a.pg, h, i, S, s);
     double2 m00 = make_double2(0, 0), m01 = m00, m10 = m00, m11 = m00;
     bool fi = a.mask[i] != 0, fj = a.mask[j] != 0;
-    double2 a00 = fi ? row_value(a, i, i, s) : make_double2(1, 0);
-    double2 a11 = fj ? row_value(a, j, j, s) : make_double2(1, 0);
-    double2 a01 = (fi && fj) ? row_value(a, i, j, s) : make_double2(0, 0);
-    double2 a10 = (fi && fj) ? row_value(a, j, i, s) : make_double2(0, 0);
+    double2 a00 = fi ? row_value(a, i, i, sy) : make_double2(1, 0);
+    double2 a11 = fj ? row_value(a, j, j, sy) : make_double2(1, 0);
+    double2 a01 = (fi && fj) ? row_value(a, i, j, sy) : make_double2(0, 0);
+    double2 a10 = (fi && fj) ? row_value(a, j, i, sy) : make_double2(0, 0);
     auto inv1 = [](double2 v) { return cabs1(v) > 0 ? cdiv2(make_double2(1, 0), v) : make_double2(1, 0); };
     bool done = false;
     if (precond == 2) {
@@ -753,7 +780,7 @@ static int pow2_at_least(int v) {
 
 // ---- workspace layout ----------------------------------------------------------------------
 struct Layout {
-    size_t off_state, off_gamma, off_k0, off_partial, off_patchmap, off_scale;
+    size_t off_state, off_gamma, off_k0, off_partial, off_patchmap, off_scale, off_gblk;
     size_t off_x, off_b, off_r64, off_Ax;                  // FP64 vectors (n, S)
     size_t off_v[8];                                       // Krylov vectors of the inner precision
     size_t off_minv;
@@ -762,18 +789,19 @@ struct Layout {
 
 static size_t align256(size_t v) { return (v + 255) & ~(size_t)255; }
 
-static Layout make_layout(long long n, long long nnz, long long npatch, int S, int nports, int precision) {
+static Layout make_layout(long long n, long long nnz, long long npatch, int S, int nports, int precision, int G = 1) {
     Layout L;
     size_t o = 0;
     long long nb = (n * S + VB - 1) / VB + 1;
     size_t vec64 = (size_t)n * S * sizeof(double2);
     size_t vecw = (size_t)n * S * (precision ? sizeof(float2) : sizeof(double2));
-    L.off_state = o; o = align256(o + sizeof(SysState) * 2 * S);
-    L.off_gamma = o; o = align256(o + sizeof(double) * 2 * S * (nports > 0 ? nports : 1));
-    L.off_k0 = o; o = align256(o + sizeof(double) * S);
+    L.off_state = o; o = align256(o + sizeof(SysState) * 2 * S * G);
+    L.off_gamma = o; o = align256(o + sizeof(double) * 2 * S * G * (nports > 0 ? nports : 1));
+    L.off_k0 = o; o = align256(o + sizeof(double) * S * G);
     L.off_partial = o; o = align256(o + sizeof(double2) * 3 * nb * S);
     L.off_patchmap = o; o = align256(o + sizeof(int) * n);
-    L.off_scale = o; o = align256(o + sizeof(double) * S);
+    L.off_scale = o; o = align256(o + sizeof(double) * S * G);
+    L.off_gblk = o; o = align256(o + sizeof(int) * (G + 1));
     L.off_x = o; o = align256(o + vec64);
     L.off_b = o; o = align256(o + vec64);
     L.off_r64 = o; o = align256(o + vec64);
@@ -799,6 +827,10 @@ struct Krylov {
     double2* partial = nullptr;
     SysState* st = nullptr;
     cudaStream_t s = nullptr;
+    // grouped systems: G groups of S systems, group of every DOF pair, group block ranges
+    int G = 1;
+    const int* pg = nullptr;
+    const int* gblk = nullptr;
     // auxiliary-space correction (precond 3: aux Jacobi, 4: learned network); BiCGStab only
     const emfem_aux_s* aux = nullptr;
     T* adinv = nullptr;
@@ -812,7 +844,8 @@ struct Krylov {
     // that the Krylov memory is lost
     double restart_eps = sizeof(R) == 8 ? 1e-9 : 1e-6;
     void reduce(int ncomp, unsigned nblocks, int mode) {
-        reduce_update_kernel<<<S, VB, 0, s>>>(partial, (int)nblocks, S, ncomp, st, mode, maxit, restart_eps, nsys);
+        reduce_update_kernel<<<G * S, VB, 0, s>>>(partial, (int)nblocks, S, ncomp, st, mode, maxit, restart_eps, nsys, G,
+                                                  gblk, nblocks != nb_pair() ? 1 : 0, (int)nb_pair());
     }
 
     int start() {
@@ -833,20 +866,20 @@ struct Krylov {
             T *z = v[0], *p = v[1], *q = v[2];
             spmv_kernel<R><<<nb_all(), VB, 0, s>>>(op, p, q, partial, DOT_XY, nullptr);
             reduce(1, nb_all(), UPD_COCG_ALPHA);
-            cocg_update_kernel<R><<<nb_pair(), VB, 0, s>>>(h, S, precond, st, x, r, z, p, q, minv, partial);
+            cocg_update_kernel<R><<<nb_pair(), VB, 0, s>>>(h, S, precond, pg, st, x, r, z, p, q, minv, partial);
             reduce(2, nb_pair(), UPD_COCG_BETA);
-            cocg_pupdate_kernel<R><<<nb_all(), VB, 0, s>>>(n, S, st, z, p);
+            cocg_pupdate_kernel<R><<<nb_all(), VB, 0, s>>>(n, S, pg, st, z, p);
         } else {
             T *rh = v[0], *p = v[1], *vv = v[2], *ph = v[3], *sh = v[4], *t = v[5];
-            bicg_p_kernel<R><<<nb_pair(), VB, 0, s>>>(h, S, bj(), st, r, p, vv, ph, minv, rh);
+            bicg_p_kernel<R><<<nb_pair(), VB, 0, s>>>(h, S, bj(), pg, st, r, p, vv, ph, minv, rh);
             if (aux) EMFEM_TRY(aux_correct<T>(aux, S, precond == 4, adinv, p, op.mask, ph, s));
             spmv_kernel<R><<<nb_all(), VB, 0, s>>>(op, ph, vv, partial, DOT_CONJW_Y, rh);
             reduce(1, nb_all(), UPD_BICG_ALPHA);
-            bicg_s_kernel<R><<<nb_pair(), VB, 0, s>>>(h, S, bj(), st, r, vv, sh, minv);
+            bicg_s_kernel<R><<<nb_pair(), VB, 0, s>>>(h, S, bj(), pg, st, r, vv, sh, minv);
             if (aux) EMFEM_TRY(aux_correct<T>(aux, S, precond == 4, adinv, r, op.mask, sh, s));
             spmv_kernel<R><<<nb_all(), VB, 0, s>>>(op, sh, t, partial, DOT_CONJY_W_YY, r);
             reduce(3, nb_all(), UPD_BICG_OMEGA);
-            bicg_x_kernel<R><<<nb_all(), VB, 0, s>>>(n, S, st, x, r, ph, sh, t, rh, partial);
+            bicg_x_kernel<R><<<nb_all(), VB, 0, s>>>(n, S, pg, st, x, r, ph, sh, t, rh, partial);
             reduce(2, nb_all(), UPD_BICG_RHO);
         }
         return check_cuda(cudaGetLastError(), "krylov iteration");
@@ -865,15 +898,15 @@ struct Krylov {
         if (st_cap != EMFEM_OK) { if (graph) cudaGraphDestroy(graph); return st_cap; }
         EMFEM_CUDA(e);
         EMFEM_CUDA(cudaGraphInstantiate(&exec, graph, 0));
-        std::vector<SysState> host(S);
+        std::vector<SysState> host((size_t)G * S);
         int rounds = (maxit + chunk - 1) / chunk + 1;
         int rc = EMFEM_OK;
         for (int it = 0; it < rounds; it++) {
             if ((rc = check_cuda(cudaGraphLaunch(exec, s), "cudaGraphLaunch")) != EMFEM_OK) break;
-            if ((rc = check_cuda(cudaMemcpyAsync(host.data(), st, sizeof(SysState) * S, cudaMemcpyDeviceToHost, s), "copy state")) != EMFEM_OK) break;
+            if ((rc = check_cuda(cudaMemcpyAsync(host.data(), st, sizeof(SysState) * host.size(), cudaMemcpyDeviceToHost, s), "copy state")) != EMFEM_OK) break;
             if ((rc = check_cuda(cudaStreamSynchronize(s), "sync")) != EMFEM_OK) break;
             bool any = false;
-            for (int k = 0; k < S; k++) any |= host[k].active != 0;
+            for (size_t k = 0; k < host.size(); k++) any |= host[k].active != 0;
             if (!any) break;
         }
         cudaGraphExecDestroy(exec);
@@ -892,6 +925,7 @@ static void build_op(OpArgs& a, int64_t n, int S, const int32_t* indptr, const i
     a.n = n; a.S = S; a.indptr = indptr; a.indices = indices; a.E = E; a.B = B; a.k0sq = k0dev;
     a.patch_of_row = pmap; a.patch_rowptr = prowptr; a.patch_cols = pcols; a.patch_vals = pvals; a.patch_port = pport;
     a.n_ports = nports; a.gamma = gdev; a.mask = mask;
+    a.pg = nullptr; a.hh = n / 2;
 }
 
 extern "C" {
@@ -951,13 +985,17 @@ int emfem_sweep_spmv(emfem_handle h, int64_t n, const int32_t* indptr, const int
     return EMFEM_OK;
 }
 
-int emfem_krylov_solve(emfem_handle hd, int method, int64_t n, int64_t nnz, const int32_t* indptr, const int32_t* indices,
+}  // extern "C"
+
+// The batched solve behind emfem_krylov_solve (G = 1) and emfem_krylov_solve_grouped (G groups of
+// nsys systems; row i of the (n, S) vectors belongs to group pair_group[i mod n/2]).
+static int krylov_impl(emfem_handle hd, int method, int64_t n, int64_t nnz, const int32_t* indptr, const int32_t* indices,
                        const void* E_vals, const void* B_vals, int nsys, const double* k0sq,
                        int64_t n_patch_rows, const int32_t* patch_rows, const int32_t* patch_rowptr,
                        const int32_t* patch_cols, const void* patch_vals, const int32_t* patch_port,
                        int n_ports, const double* gamma, const uint8_t* free_mask, const void* rhs, void* x,
                        double tol, int maxit, int precond, int precision, void* workspace, size_t workspace_bytes,
-                       int* status, int* iters, double* relres, emfem_aux aux) {
+                       int* status, int* iters, double* relres, emfem_aux aux, int G, const int32_t* pair_group) {
     EMFEM_REQUIRE(hd && indptr && indices && E_vals && k0sq && free_mask && rhs && x && workspace,
                   "emfem_krylov_solve: null argument");
     EMFEM_REQUIRE(method == 0 || method == 1, "emfem_krylov_solve: method must be 0 (COCG) or 1 (BiCGStab)");
@@ -983,8 +1021,29 @@ int emfem_krylov_solve(emfem_handle hd, int method, int64_t n, int64_t nnz, cons
     EMFEM_REQUIRE(npatch <= nnz, "emfem_krylov_solve: more patch entries than nnz");
     EMFEM_REQUIRE(precond < 3 || aux->kbuf_bytes >= aux_solve_bytes(aux, S),
                   "emfem_krylov_solve: call emfem_aux_reserve with at least nsys systems first");
-    Layout L = make_layout(n, nnz, npatch, S, n_ports, precision);
-    size_t need = make_layout(n, nnz, nnz, S, 8, precision).total;
+    std::vector<int> hgblk(G + 1, 0);
+    if (G > 1) {
+        EMFEM_REQUIRE(pair_group && precision == 0 && precond <= 2,
+                      "emfem_krylov_solve_grouped: pair_group required; FP64 only, precond 0-2");
+        EMFEM_REQUIRE((n / 2) % VB == 0, "emfem_krylov_solve_grouped: n/2 must be a multiple of 256");
+        std::vector<int> hp(n / 2);
+        EMFEM_CUDA(cudaMemcpy(hp.data(), pair_group, sizeof(int) * (n / 2), cudaMemcpyDeviceToHost));
+        // groups 0..G-1 in ascending order, none empty, each starting at a multiple of 256 pairs
+        int prev = -1;
+        for (long long i = 0; i < n / 2; i++) {
+            int v = hp[i];
+            if (v == prev) continue;
+            EMFEM_REQUIRE(v == prev + 1 && v < G && i % VB == 0,
+                          "emfem_krylov_solve_grouped: pair_group must run through 0..G-1 in order, each group "
+                          "starting at a multiple of 256 pairs");
+            hgblk[v] = (int)(i * S / VB);
+            prev = v;
+        }
+        EMFEM_REQUIRE(prev == G - 1, "emfem_krylov_solve_grouped: every group needs at least one DOF pair");
+        hgblk[G] = (int)((n / 2) * S / VB);
+    }
+    Layout L = make_layout(n, nnz, npatch, S, n_ports, precision, G);
+    size_t need = make_layout(n, nnz, nnz, S, 8, precision, G).total;
     if (workspace_bytes < need) {
         set_error("emfem_krylov_solve: workspace of %zu bytes, %zu needed (emfem_krylov_workspace_size)", workspace_bytes, need);
         return EMFEM_ERR_WORKSPACE;
@@ -999,7 +1058,9 @@ int emfem_krylov_solve(emfem_handle hd, int method, int64_t n, int64_t nnz, cons
         return EMFEM_ERR_CUDA;
     }
     SysState* st = (SysState*)(ws + L.off_state);
-    SysState* st_outer = st + S;
+    SysState* st_outer = st + (size_t)G * S;
+    int* gblk = (int*)(ws + L.off_gblk);
+    const int nbh = (int)grid_for((n / 2) * (long long)S, VB);
     double* gdev = (double*)(ws + L.off_gamma);
     double* k0dev = (double*)(ws + L.off_k0);
     double2* partial = (double2*)(ws + L.off_partial);
@@ -1011,19 +1072,22 @@ int emfem_krylov_solve(emfem_handle hd, int method, int64_t n, int64_t nnz, cons
     double2* Ax = (double2*)(ws + L.off_Ax);
     long long nS = n * (long long)S;
     unsigned gv = grid_for(nS, VB);
-    std::vector<double> hk0(S, 0.0), hg(2 * S * (n_ports > 0 ? n_ports : 1), 0.0);
-    for (int k = 0; k < nsys; k++) hk0[k] = k0sq[k];
-    for (int k = 0; k < nsys; k++)
-        for (int q = 0; q < n_ports; q++) {
-            hg[2 * (k * n_ports + q)] = gamma[2 * (k * n_ports + q)];
-            hg[2 * (k * n_ports + q) + 1] = gamma[2 * (k * n_ports + q) + 1];
+    std::vector<double> hk0((size_t)G * S, 0.0), hg(2 * (size_t)G * S * (n_ports > 0 ? n_ports : 1), 0.0);
+    for (int g = 0; g < G; g++)
+        for (int k = 0; k < nsys; k++) {
+            hk0[g * S + k] = k0sq[g * nsys + k];
+            for (int q = 0; q < n_ports; q++) {
+                hg[2 * ((g * S + k) * n_ports + q)] = gamma[2 * ((g * nsys + k) * n_ports + q)];
+                hg[2 * ((g * S + k) * n_ports + q) + 1] = gamma[2 * ((g * nsys + k) * n_ports + q) + 1];
+            }
         }
     OpArgs op64;
     int rc = EMFEM_OK;
 #define STRY(x) do { rc = (x); if (rc != EMFEM_OK) goto done; } while (0)
     STRY(check_cuda(cudaEventRecord(ev, h->stream), "event"));
     STRY(check_cuda(cudaStreamWaitEvent(s, ev, 0), "wait"));
-    STRY(check_cuda(cudaMemcpyAsync(k0dev, hk0.data(), sizeof(double) * S, cudaMemcpyHostToDevice, s), "copy k0"));
+    STRY(check_cuda(cudaMemcpyAsync(k0dev, hk0.data(), sizeof(double) * hk0.size(), cudaMemcpyHostToDevice, s), "copy k0"));
+    STRY(check_cuda(cudaMemcpyAsync(gblk, hgblk.data(), sizeof(int) * (G + 1), cudaMemcpyHostToDevice, s), "copy gblk"));
     STRY(check_cuda(cudaMemcpyAsync(gdev, hg.data(), sizeof(double) * hg.size(), cudaMemcpyHostToDevice, s), "copy gamma"));
     STRY(check_cuda(cudaMemsetAsync(pmap, 0xff, sizeof(int) * n, s), "memset"));
     if (n_patch_rows > 0) {
@@ -1037,10 +1101,11 @@ int emfem_krylov_solve(emfem_handle hd, int method, int64_t n, int64_t nnz, cons
     STRY(check_cuda(cudaGetLastError(), "setup copies"));
     build_op(op64, n, S, indptr, indices, E_vals, B_vals, k0dev, n_patch_rows ? pmap : nullptr, patch_rowptr,
              patch_cols, patch_vals, patch_port, n_ports, gdev, free_mask);
+    if (G > 1) op64.pg = pair_group;
     // initial residual r64 = b - A x0 and the outer state (||b||, tolerance, active)
     spmv_kernel<double><<<gv, VB, 0, s>>>(op64, x64, Ax, nullptr, DOT_NONE, nullptr);
     residual_kernel<<<gv, VB, 0, s>>>(n, S, free_mask, b64, Ax, r64, partial);
-    reduce_update_kernel<<<S, VB, 0, s>>>(partial, (int)gv, S, 2, st_outer, UPD_INIT, maxit, tol, nsys);
+    reduce_update_kernel<<<G * S, VB, 0, s>>>(partial, (int)gv, S, 2, st_outer, UPD_INIT, maxit, tol, nsys, G, gblk, 1, nbh);
     STRY(check_cuda(cudaGetLastError(), "initial residual"));
 
     if (precision == 0) {
@@ -1049,6 +1114,7 @@ int emfem_krylov_solve(emfem_handle hd, int method, int64_t n, int64_t nnz, cons
         k.x = x64; k.r = (double2*)(ws + L.off_r64); k.minv = (double2*)(ws + L.off_minv);
         for (int q = 0; q < 7; q++) k.v[q] = (double2*)(ws + L.off_v[q]);
         k.partial = partial; k.st = st; k.s = s;
+        k.G = G; k.pg = G > 1 ? pair_group : nullptr; k.gblk = gblk;
         if (precond) {
             precond_setup_kernel<double><<<grid_for((n / 2) * (long long)S, VB), VB, 0, s>>>(op64, k.bj(), k.minv);
             STRY(check_cuda(cudaGetLastError(), "precond_setup"));
@@ -1059,7 +1125,8 @@ int emfem_krylov_solve(emfem_handle hd, int method, int64_t n, int64_t nnz, cons
             STRY(aux_setup_dinv<double2>(aux, S, nsys, k0dev, gdev, k.adinv, s));
         }
         // the recurrence tolerance is half the requested one so the FP64 true residual meets it
-        reduce_update_kernel<<<S, VB, 0, s>>>(partial, (int)gv, S, 2, st, UPD_INIT, maxit, 0.5 * tol, nsys);
+        reduce_update_kernel<<<G * S, VB, 0, s>>>(partial, (int)gv, S, 2, st, UPD_INIT, maxit, 0.5 * tol, nsys, G, gblk, 1,
+                                                  nbh);
         STRY(check_cuda(cudaGetLastError(), "init state"));
         STRY(k.start());
         STRY(k.run(16));
@@ -1141,26 +1208,29 @@ int emfem_krylov_solve(emfem_handle hd, int method, int64_t n, int64_t nnz, cons
     }
     {
         // final FP64 true residual and solution copy-out
-        std::vector<SysState> hs(S);
-        STRY(check_cuda(cudaMemcpyAsync(hs.data(), st, sizeof(SysState) * S, cudaMemcpyDeviceToHost, s), "copy"));
+        const size_t GS = (size_t)G * S;
+        std::vector<SysState> hs(GS);
+        STRY(check_cuda(cudaMemcpyAsync(hs.data(), st, sizeof(SysState) * GS, cudaMemcpyDeviceToHost, s), "copy"));
         spmv_kernel<double><<<gv, VB, 0, s>>>(op64, x64, Ax, nullptr, DOT_NONE, nullptr);
         residual_kernel<<<gv, VB, 0, s>>>(n, S, free_mask, b64, Ax, r64, partial);
-        reduce_update_kernel<<<S, VB, 0, s>>>(partial, (int)gv, S, 2, st_outer, UPD_INIT, maxit, tol, S);
+        reduce_update_kernel<<<G * S, VB, 0, s>>>(partial, (int)gv, S, 2, st_outer, UPD_INIT, maxit, tol, S, G, gblk, 1, nbh);
         unpad_copy_kernel<<<grid_for(n * (long long)nsys, VB), VB, 0, s>>>(n, nsys, S, x64, (double2*)x);
         STRY(check_cuda(cudaGetLastError(), "final residual"));
-        std::vector<SysState> hf(S);
-        STRY(check_cuda(cudaMemcpyAsync(hf.data(), st_outer, sizeof(SysState) * S, cudaMemcpyDeviceToHost, s), "copy"));
+        std::vector<SysState> hf(GS);
+        STRY(check_cuda(cudaMemcpyAsync(hf.data(), st_outer, sizeof(SysState) * GS, cudaMemcpyDeviceToHost, s), "copy"));
         STRY(check_cuda(cudaStreamSynchronize(s), "sync"));
         bool all_ok = true;
-        for (int q = 0; q < nsys; q++) {
-            double rel = hf[q].bn2 > 0 ? std::sqrt(hf[q].rn2 / hf[q].bn2) : 0.0;
-            int stat = hs[q].active ? 1 : hs[q].status;
-            if (stat == 0 && rel > tol) stat = 1;  // the recurrence drifted from the true residual
-            if (status) status[q] = stat;
-            if (iters) iters[q] = hs[q].iters;
-            if (relres) relres[q] = rel;
-            all_ok &= stat == 0;
-        }
+        for (int g = 0; g < G; g++)
+            for (int q = 0; q < nsys; q++) {
+                const SysState &e = hs[g * S + q], &f = hf[g * S + q];
+                double rel = f.bn2 > 0 ? std::sqrt(f.rn2 / f.bn2) : 0.0;
+                int stat = e.active ? 1 : e.status;
+                if (stat == 0 && rel > tol) stat = 1;  // the recurrence drifted from the true residual
+                if (status) status[g * nsys + q] = stat;
+                if (iters) iters[g * nsys + q] = e.iters;
+                if (relres) relres[g * nsys + q] = rel;
+                all_ok &= stat == 0;
+            }
         if (!all_ok) {
             set_error("emfem_krylov_solve: not every system reached the tolerance");
             rc = EMFEM_ERR_NOT_CONVERGED;
@@ -1174,6 +1244,40 @@ done:
     cudaStreamDestroy(s);
     return rc;
 #undef STRY
+}
+
+extern "C" {
+
+int emfem_krylov_solve(emfem_handle hd, int method, int64_t n, int64_t nnz, const int32_t* indptr, const int32_t* indices,
+                       const void* E_vals, const void* B_vals, int nsys, const double* k0sq,
+                       int64_t n_patch_rows, const int32_t* patch_rows, const int32_t* patch_rowptr,
+                       const int32_t* patch_cols, const void* patch_vals, const int32_t* patch_port,
+                       int n_ports, const double* gamma, const uint8_t* free_mask, const void* rhs, void* x,
+                       double tol, int maxit, int precond, int precision, void* workspace, size_t workspace_bytes,
+                       int* status, int* iters, double* relres, emfem_aux aux) {
+    return krylov_impl(hd, method, n, nnz, indptr, indices, E_vals, B_vals, nsys, k0sq, n_patch_rows, patch_rows,
+                       patch_rowptr, patch_cols, patch_vals, patch_port, n_ports, gamma, free_mask, rhs, x, tol, maxit,
+                       precond, precision, workspace, workspace_bytes, status, iters, relres, aux, 1, nullptr);
+}
+
+int emfem_krylov_workspace_size_grouped(int64_t n, int64_t nnz, int nsys, int ngroups, size_t* bytes) {
+    EMFEM_REQUIRE(bytes && n > 0 && nsys > 0 && nsys <= 64 && nnz >= 0 && ngroups >= 1,
+                  "emfem_krylov_workspace_size_grouped: bad argument");
+    *bytes = make_layout(n, nnz, nnz, pow2_at_least(nsys), 8, 0, ngroups).total;
+    return EMFEM_OK;
+}
+
+int emfem_krylov_solve_grouped(emfem_handle hd, int method, int64_t n, int64_t nnz, const int32_t* indptr,
+                               const int32_t* indices, const void* E_vals, const void* B_vals, int ngroups,
+                               const int32_t* pair_group, int nsys, const double* k0sq, int64_t n_patch_rows,
+                               const int32_t* patch_rows, const int32_t* patch_rowptr, const int32_t* patch_cols,
+                               const void* patch_vals, const int32_t* patch_port, int n_ports, const double* gamma,
+                               const uint8_t* free_mask, const void* rhs, void* x, double tol, int maxit, int precond,
+                               void* workspace, size_t workspace_bytes, int* status, int* iters, double* relres) {
+    EMFEM_REQUIRE(ngroups >= 1 && ngroups <= 4096, "emfem_krylov_solve_grouped: 1 <= ngroups <= 4096");
+    return krylov_impl(hd, method, n, nnz, indptr, indices, E_vals, B_vals, nsys, k0sq, n_patch_rows, patch_rows,
+                       patch_rowptr, patch_cols, patch_vals, patch_port, n_ports, gamma, free_mask, rhs, x, tol, maxit,
+                       precond, 0, workspace, workspace_bytes, status, iters, relres, nullptr, ngroups, pair_group);
 }
 
 }  // extern "C"

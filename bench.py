@@ -253,6 +253,51 @@ def train_network(P, train_freqs, steps: int = 300) -> tuple:
                  "objective": "mean ||G za - e||^2 / ||e||^2 over (residual, correction) pairs"}
 
 
+def batched_sweep_section(tol: float = 1e-8, maxit: int = 40000) -> dict:
+    """Several meshes' sweeps in one batched Krylov call (``BatchSweep``) against the same meshes solved
+    one ``FrequencySweep`` after another: 8 air-filled guides of uneven size (3 000-12 600 tets), two
+    frequencies x two ports each, plain block-Jacobi BiCGStab FP64 to ``tol``; set-up (assembly, ports)
+    and solve inside the timed regions."""
+    import torch
+    from emerge_b200 import problems
+    from emerge_b200.batch import BatchSweep
+    from emerge_b200.sweep import FrequencySweep
+    rng = np.random.default_rng(5)
+    Ps, systems = [], []
+    for i in range(8):
+        nx, ny, nz = int(rng.integers(8, 13)), int(rng.integers(4, 7)), int(rng.integers(12, 26))
+        a = 22.86e-3 * rng.uniform(0.9, 1.1)
+        Ps.append(problems.waveguide(nx=nx, ny=ny, nz=nz, a=a, seed=100 + i))
+        fc = 299792458.0 / (2 * a)
+        systems.append([(f, q) for f in (1.35 * fc, 1.75 * fc) for q in range(2)])
+    tets = sum(P.mesh.n_tets for P in Ps)
+    BatchSweep(Ps[:2]).solve(systems[:2], tol=tol, maxit=50)        # driver / allocator warm-up
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    bs = BatchSweep(Ps)
+    rb = bs.solve(systems, tol=tol, maxit=maxit)
+    torch.cuda.synchronize()
+    t_b = time.perf_counter() - t0
+    conv_b = sum(int(((r.status == 0) & (r.relres <= tol)).sum()) for r in rb)
+    del bs
+    gc.collect()
+    t0 = time.perf_counter()
+    conv_s, its_s = 0, []
+    for P, sl in zip(Ps, systems):
+        r = FrequencySweep(P).solve(sl, tol=tol, maxit=maxit)
+        conv_s += int(((r.status == 0) & (r.relres <= tol)).sum())
+        its_s.append(int(r.iters.max()))
+    torch.cuda.synchronize()
+    t_s = time.perf_counter() - t0
+    return {"workload": "8 air-filled guides, 3 000-12 600 tets, 2 frequencies x 2 ports each, plain block-Jacobi "
+                        f"BiCGStab FP64 to {tol:g}",
+            "meshes": len(Ps), "total_tets": int(tets), "systems": 4 * len(Ps),
+            "batched": {"seconds": t_b, "converged": conv_b, "solves_per_s": conv_b / t_b,
+                        "iters_max": int(max(int(r.iters.max()) for r in rb))},
+            "one_mesh_at_a_time": {"seconds": t_s, "converged": conv_s, "solves_per_s": conv_s / t_s,
+                                   "iters_max_per_mesh": its_s}}
+
+
 def precision_section(reps: int = 3) -> dict:
     """The precision workload: assembly of the full 1 497 600-tet substrate box (80x60x52 grid x 6), and
     on a downsized member (20x15x13 grid, 23 400 tets) the FP32-inner / FP64-refinement sweep against
@@ -513,6 +558,7 @@ def main():
                                   tuple(a for a in args.sweep_arms.split(",") if a))
         batch = None if args.no_batch else batch_section()
         precision = None if args.no_precision else precision_section()
+        batched_sweeps = None if args.no_batch else batched_sweep_section()
         cb = None if args.no_cpu_baseline else cpu_baseline(P)
         out = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
@@ -534,6 +580,7 @@ def main():
             "sweep": sweep,
             "batched_meshes": batch,
             "precision_workload": precision,
+            "batched_sweeps": batched_sweeps,
             "cpu_baseline": cb,
         }
         print(json.dumps(out), flush=True)

@@ -39,6 +39,8 @@ constexpr int VB = 256;  // threads per block for vector/SpMV kernels
 #define EMFEM_INNER_TOL 1e-4
 #endif
 
+struct SysState;
+
 struct OpArgs {
     long long n;
     int S;                          // padded systems (power of two, divides VB)
@@ -59,7 +61,12 @@ struct OpArgs {
     // (or i - hh) of system column s then belongs to system pg[i] * S + s of the per-system arrays.
     const int* pg;
     long long hh;
+    // inside a Krylov iteration: the per-system state; rows of systems that are no longer active are
+    // skipped (their scalars are zero, so these vectors are not used again).  Null elsewhere.
+    const SysState* skip;
 };
+
+__device__ __forceinline__ bool sys_active(const SysState* st, int sy);
 
 __device__ __forceinline__ int sys_of_row(const int* pg, long long hh, long long i, int S, int s) {
     return pg ? pg[i < hh ? i : i - hh] * S + s : s;
@@ -121,7 +128,13 @@ __global__ void __launch_bounds__(VB) spmv_kernel(OpArgs a, const typename V2<R>
     int s = (int)(g % S);
     double2 c0 = make_double2(0.0, 0.0), c1 = c0;
     double c2 = 0.0;
-    if (i < a.n) {
+    const int sy = i < a.n ? sys_of_row(a.pg, a.hh, i, S, s) : 0;
+    bool act = i < a.n && (!a.skip || sys_active(a.skip, sy));
+    // S >= 32: the 32 lanes of a warp are 32 systems of one row and stage that row's entries together
+    // (warp-synchronous below), so the warp skips the row only when none of its systems is active.
+    // Every lane reaches this vote, and the row index is the same for the whole warp.
+    if (S >= 32) act = __any_sync(0xffffffffu, act);
+    if (act) {
         double yr = 0, yi = 0;
         if (a.mask[i]) {
             const double2* Ev = (const double2*)a.E;
@@ -215,7 +228,6 @@ __global__ void __launch_bounds__(VB) spmv_kernel(OpArgs a, const typename V2<R>
                     bi += b.x * xi + b.y * xr;
                 }
             }
-            const int sy = sys_of_row(a.pg, a.hh, i, S, s);
             double k2 = a.k0sq[sy];
             yr = er - k2 * br;
             yi = ei - k2 * bi;
@@ -269,6 +281,8 @@ struct SysState {
     int status;       // 0 converged, 1 cap, 2 breakdown
     int restart;      // BiCGStab: take r_hat = r at the next p update
 };
+
+__device__ __forceinline__ bool sys_active(const SysState* st, int sy) { return st[sy].active != 0; }
 
 __device__ __forceinline__ double2 cdiv2(double2 a, double2 b) {
     if (fabs(b.x) >= fabs(b.y)) {
@@ -445,7 +459,7 @@ __global__ void __launch_bounds__(VB) cocg_update_kernel(long long h, int S, int
     long long i = g / S;
     int s = (int)(g % S);
     double2 rz = make_double2(0, 0), rr = make_double2(0, 0);
-    if (i < h) {
+    if (i < h && st[sys_of_row(pg, h, i, S, s)].active) {
         double2 al = st[sys_of_row(pg, h, i, S, s)].alpha;
         R ar = (R)al.x, ai = (R)al.y;
         T rv2[2];
@@ -511,6 +525,7 @@ __global__ void __launch_bounds__(VB) bicg_p_kernel(long long h, int S, int prec
     int s = (int)(g % S);
     if (i >= h) return;
     const int sy = sys_of_row(pg, h, i, S, s);
+    if (!st[sy].active) return;
     double2 b = st[sy].beta, w = st[sy].omega;
     R br = (R)b.x, bi = (R)b.y, wr = (R)w.x, wi = (R)w.y;
     if (st[sy].restart) {
@@ -543,6 +558,7 @@ __global__ void __launch_bounds__(VB) bicg_s_kernel(long long h, int S, int prec
     long long i = g / S;
     int s = (int)(g % S);
     if (i >= h) return;
+    if (!st[sys_of_row(pg, h, i, S, s)].active) return;
     double2 a = st[sys_of_row(pg, h, i, S, s)].alpha;
     R ar = (R)a.x, ai = (R)a.y;
     T sn[2];
@@ -570,8 +586,8 @@ __global__ void __launch_bounds__(VB) bicg_x_kernel(long long n, int S, const in
     typedef typename V2<R>::T T;
     long long g = (long long)blockIdx.x * VB + threadIdx.x;
     double2 c0 = make_double2(0, 0), c1 = c0;
-    if (g < n * S) {
-        const int sy = sys_of_row(pg, n / 2, g / S, S, (int)(g % S));
+    const int sy = g < n * S ? sys_of_row(pg, n / 2, g / S, S, (int)(g % S)) : 0;
+    if (g < n * S && st[sy].active) {
         double2 a = st[sy].alpha, w = st[sy].omega;
         R ar = (R)a.x, ai = (R)a.y, wr = (R)w.x, wi = (R)w.y;
         T xv = x[g], pv = ph[g], sv = sh[g], rv = r[g], tv = t[g];
@@ -925,7 +941,7 @@ static void build_op(OpArgs& a, int64_t n, int S, const int32_t* indptr, const i
     a.n = n; a.S = S; a.indptr = indptr; a.indices = indices; a.E = E; a.B = B; a.k0sq = k0dev;
     a.patch_of_row = pmap; a.patch_rowptr = prowptr; a.patch_cols = pcols; a.patch_vals = pvals; a.patch_port = pport;
     a.n_ports = nports; a.gamma = gdev; a.mask = mask;
-    a.pg = nullptr; a.hh = n / 2;
+    a.pg = nullptr; a.hh = n / 2; a.skip = nullptr;
 }
 
 extern "C" {
@@ -1114,6 +1130,7 @@ static int krylov_impl(emfem_handle hd, int method, int64_t n, int64_t nnz, cons
         k.x = x64; k.r = (double2*)(ws + L.off_r64); k.minv = (double2*)(ws + L.off_minv);
         for (int q = 0; q < 7; q++) k.v[q] = (double2*)(ws + L.off_v[q]);
         k.partial = partial; k.st = st; k.s = s;
+        k.op.skip = st;
         k.G = G; k.pg = G > 1 ? pair_group : nullptr; k.gblk = gblk;
         if (precond) {
             precond_setup_kernel<double><<<grid_for((n / 2) * (long long)S, VB), VB, 0, s>>>(op64, k.bj(), k.minv);
@@ -1139,6 +1156,7 @@ static int krylov_impl(emfem_handle hd, int method, int64_t n, int64_t nnz, cons
         k.x = d32; k.r = r32; k.minv = (float2*)(ws + L.off_minv);
         for (int q = 0; q < 6; q++) k.v[q] = (float2*)(ws + L.off_v[q]);
         k.partial = partial; k.st = st; k.s = s;
+        k.op.skip = st;
         if (precond) {
             precond_setup_kernel<float><<<grid_for((n / 2) * (long long)S, VB), VB, 0, s>>>(op64, k.bj(), k.minv);
             STRY(check_cuda(cudaGetLastError(), "precond_setup"));

@@ -102,8 +102,6 @@ class BatchSweep:
     PAIR_ALIGN = 256
 
     def __init__(self, problems, device=None):
-        import ctypes  # noqa: F401
-        from .assembly import DeviceMesh
         from .sweep import FrequencySweep
         self.problems = list(problems)
         dev = torch.device("cuda", torch.cuda.current_device()) if device is None else torch.device(device)
@@ -167,16 +165,10 @@ class BatchSweep:
         nslot_off = 0
         self.n_ports = 0
         for g, P in enumerate(self.problems):
-            fs = object.__new__(FrequencySweep)
-            fs.problem, fs.device = P, dev
-            fs.dmesh = DeviceMesh(P.mesh, P.field, dev)
-            fs.n = P.field.n_field
-            fs._build_ports()
+            fs = FrequencySweep.port_terms(P, dev)
             self.sweeps.append(fs)
             loc = self.local_to_grouped(g)
-            m = np.ones(fs.n, dtype=np.uint8)
-            m[P.pec_ids] = 0
-            mask[loc] = torch.from_numpy(m).to(dev)
+            mask[loc] = fs.mask
             self.n_ports = max(self.n_ports, fs.n_ports)
             if fs.patch_rows.numel():
                 rows_l.append(loc[fs.patch_rows.long()].to(torch.int32))

@@ -104,6 +104,27 @@ class FrequencySweep:
         self._aux = None
         self.network = None
 
+    @classmethod
+    def port_terms(cls, problem, device=None) -> "FrequencySweep":
+        """A sweep object holding only the problem's port and Robin terms, port vectors and free-DOF
+        mask, with no operator: what a batch of meshes whose operator is assembled elsewhere needs
+        from each mesh (right-hand sides, Robin coefficients, S-parameters)."""
+        fs = cls.__new__(cls)
+        fs.device = torch.device("cuda", torch.cuda.current_device()) if device is None else torch.device(device)
+        fs.problem = problem
+        fs.dmesh = DeviceMesh(problem.mesh, problem.field, fs.device)
+        fs.n = problem.field.n_field
+        fs.plan = None
+        fs.E = fs.B = None
+        fs._build_ports()
+        mask = np.ones(fs.n, dtype=np.uint8)
+        mask[problem.pec_ids] = 0
+        fs.mask = torch.from_numpy(mask).to(fs.device)
+        fs._ws = None
+        fs._aux = None
+        fs.network = None
+        return fs
+
     def aux_space(self):
         """The auxiliary nodal space of this mesh with this operator's diagonals (built once)."""
         if self._aux is None:

@@ -93,6 +93,19 @@ class AuxSpace:
                                                                        "graph_ptr", "graph_nbr")]), "emfem_aux_export")
         return out
 
+    def set_rows(self, new_of_old: torch.Tensor, n_new: int, aux_group: torch.Tensor | None = None) -> None:
+        """Move G onto the rows of a grouped multi-mesh system (``emfem_aux_set_rows``); the operator
+        diagonals must be set again afterwards."""
+        nd = new_of_old.to(self.device, torch.int64).contiguous()
+        grp = None if aux_group is None else aux_group.to(self.device, torch.int32).contiguous()
+        ng = 1 if grp is None else int(grp.max().item()) + 1
+        Handle.get(self.device)
+        check(lib().emfem_aux_set_rows(self._a, int(n_new), ptr(nd), ng, None if grp is None else ptr(grp)),
+              "emfem_aux_set_rows")
+        Handle.get(self.device).raise_on_device_status("emfem_aux_set_rows")
+        self.n_field = int(n_new)
+        self.mask = None
+
     def set_operator(self, sweep) -> torch.Tensor:
         """Aux diagonals of a FrequencySweep's operator; returns [dE | dB | dR_p ...] (complex)."""
         h = Handle.get(self.device)

@@ -25,6 +25,7 @@ graph-captured iteration serves all of them.
 from __future__ import annotations
 
 import time
+from types import SimpleNamespace
 
 import numpy as np
 import torch
@@ -156,6 +157,9 @@ class BatchSweep:
         self.E = E[slot].contiguous()
         self.B = B[slot].contiguous()
         self.nnz = nnz
+        self.plan = SimpleNamespace(indptr=self.indptr, indices=self.indices, nnz=nnz)
+        self._perm = perm_d
+        self._aux = None
         del slot, row_of_slot, start_u, lens
         # per mesh: Robin / port terms and port vectors (built on each mesh's own numbering), mask
         self.sweeps = []
@@ -207,8 +211,8 @@ class BatchSweep:
         if len(systems) != G or len({len(s) for s in systems}) != 1:
             raise ValueError("give the same number of systems for every mesh")
         nsys = len(systems[0])
-        if PRECOND[precond] > 2:
-            raise ValueError("grouped solves take precond none, jacobi or block_jacobi")
+        if PRECOND[precond] > 3:
+            raise ValueError("grouped solves take precond none, jacobi, block_jacobi or aux")
         npt = max(self.n_ports, 1)
         k0 = np.zeros(G * nsys)
         gam = np.zeros((G * nsys, npt), dtype=np.complex128)
@@ -231,6 +235,11 @@ class BatchSweep:
         st = (ctypes.c_int * (G * nsys))()
         it = (ctypes.c_int * (G * nsys))()
         rr = (ctypes.c_double * (G * nsys))()
+        aux = None
+        if PRECOND[precond] == 3:
+            a = self.aux_space()
+            a.reserve(nsys)
+            aux = a.handle
         h = Handle.get(self.device)
         t0 = time.perf_counter()
         rc = lib().emfem_krylov_solve_grouped(
@@ -238,7 +247,7 @@ class BatchSweep:
             ptr(self.pair_group), nsys, (ctypes.c_double * (G * nsys))(*k0), self.patch_rows.numel(),
             ptr(self.patch_rows), ptr(self.patch_rowptr), ptr(self.patch_cols), ptr(self.patch_vals),
             ptr(self.patch_port), self.n_ports, (ctypes.c_double * len(ga))(*ga), ptr(self.mask), ptr(b), ptr(x),
-            tol, maxit, PRECOND[precond], ptr(self._ws), self._ws.numel(), st, it, rr)
+            tol, maxit, PRECOND[precond], ptr(self._ws), self._ws.numel(), st, it, rr, aux)
         torch.cuda.synchronize(self.device)
         dt = time.perf_counter() - t0
         if rc not in (0, ERR_NOT_CONVERGED):
@@ -249,6 +258,30 @@ class BatchSweep:
             out.append(SolveResult(x[self.local_to_grouped(g)].contiguous(), np.array(st[sel]), np.array(it[sel]),
                                    np.array(rr[sel]), list(sl), dt))
         return out
+
+    def aux_space(self):
+        """The auxiliary nodal space of all meshes (their disjoint union, built once), moved onto the
+        grouped rows, with the grouped operator's diagonals: ``precond="aux"`` for every mesh at once."""
+        if self._aux is None:
+            from .auxspace import AuxSpace
+            Ps = self.problems
+            G = len(Ps)
+            nn = np.array([P.mesh.n_nodes for P in Ps])
+            ne = np.array([P.mesh.n_edges for P in Ps])
+            nn_off = np.concatenate([[0], np.cumsum(nn)])
+            ne_off = np.concatenate([[0], np.cumsum(ne)])
+            union = SimpleNamespace(
+                nodes=np.zeros((3, int(nn_off[-1]))),
+                edges=np.concatenate([P.mesh.edges + nn_off[g] for g, P in enumerate(Ps)], axis=1),
+                tris=np.concatenate([P.mesh.tris + nn_off[g] for g, P in enumerate(Ps)], axis=1),
+                tri_to_edge=np.concatenate([P.mesh.tri_to_edge + ne_off[g] for g, P in enumerate(Ps)], axis=1),
+                edge_lengths=np.concatenate([P.mesh.edge_lengths for P in Ps]))
+            aux = AuxSpace(union, self.device)
+            grp = np.concatenate([np.repeat(np.arange(G), nn), np.repeat(np.arange(G), ne)]).astype(np.int32)
+            aux.set_rows(self._perm, self.n, torch.from_numpy(grp) if G > 1 else None)
+            aux.set_operator(self)
+            self._aux = aux
+        return self._aux
 
     def sparams(self, g: int, res) -> dict:
         """S-parameters of mesh g's solved systems (``FrequencySweep.sparams``)."""

@@ -249,23 +249,26 @@ __global__ void aux_diag_kernel(long long na, const int* __restrict__ gt_ptr, co
 }
 
 // ---- kernels used inside the Krylov iterations and by training ------------------------------
-// dinv[y][s] = amask ? 1 / (dE - k0_s^2 dB + sum_p gamma_{s,p} dR_p) : 0
+// dinv[y][s] = amask ? 1 / (dE - k0_s^2 dB + sum_p gamma_{s,p} dR_p) : 0; in a grouped solve column s
+// of aux node y is system agroup[y] * S + s of k0sq and gamma
 template <typename T>
 __global__ void aux_dinv_kernel(long long na, int S, int nsys, const uint8_t* __restrict__ amask,
                                 const double2* __restrict__ dE, const double2* __restrict__ dB,
                                 const double2* __restrict__ dR, int nports, const double* __restrict__ k0sq,
-                                const double* __restrict__ gamma, T* __restrict__ dinv) {
+                                const double* __restrict__ gamma, T* __restrict__ dinv,
+                                const int* __restrict__ agroup = nullptr) {
     long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (g >= na * S) return;
     long long y = g / S;
     int s = (int)(g % S);
     double dr = 0, di = 0;
     if (s < nsys && amask[y]) {
-        double k2 = k0sq[s];
+        const int sy = agroup ? agroup[y] * S + s : s;
+        double k2 = k0sq[sy];
         dr = dE[y].x - k2 * dB[y].x;
         di = dE[y].y - k2 * dB[y].y;
         for (int p = 0; p < nports; p++) {
-            double gr = gamma[2 * (s * nports + p)], gi = gamma[2 * (s * nports + p) + 1];
+            double gr = gamma[2 * (sy * nports + p)], gi = gamma[2 * (sy * nports + p) + 1];
             double2 r = dR[(long long)p * na + y];
             dr += gr * r.x - gi * r.y;
             di += gr * r.y + gi * r.x;
@@ -897,7 +900,7 @@ template <typename T>
 int aux_setup_dinv(const emfem_aux_s* a, int S, int nsys, const double* k0sq, const double* gamma, T* dinv,
                    cudaStream_t s) {
     aux_dinv_kernel<T><<<grid_for(a->na * S, AB), AB, 0, s>>>(a->na, S, nsys, a->amask, a->dE, a->dB, a->dR, a->nports,
-                                                            k0sq, gamma, dinv);
+                                                            k0sq, gamma, dinv, a->agroup);
     return check_cuda(cudaGetLastError(), "aux_dinv_kernel");
 }
 
@@ -917,8 +920,32 @@ static void aux_free(emfem_aux a) {
     if (!a) return;
     cudaFree(a->gcol); cudaFree(a->gval); cudaFree(a->gt_ptr); cudaFree(a->gt_row); cudaFree(a->gt_val);
     cudaFree(a->inc_ptr); cudaFree(a->inc); cudaFree(a->inv_deg); cudaFree(a->atype); cudaFree(a->amask);
-    cudaFree(a->dE); cudaFree(a->dB); cudaFree(a->dR); cudaFree(a->kbuf);
+    cudaFree(a->dE); cudaFree(a->dB); cudaFree(a->dR); cudaFree(a->kbuf); cudaFree(a->agroup);
     delete a;
+}
+
+// Row relabelling for a grouped (multi-mesh) solve: G row r of the aux space's own numbering becomes
+// row new_of_old[r] of an n_new-row system (rows not reached stay empty), and G^T's row indices follow.
+__global__ void aux_move_rows_kernel(long long n_old, long long n_new, const int64_t* __restrict__ new_of_old,
+                                     const int* __restrict__ gcol, const double* __restrict__ gval,
+                                     int* __restrict__ gcol_new, double* __restrict__ gval_new, int* status) {
+    long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= n_old) return;
+    long long q = new_of_old[r];
+    if (q < 0 || q >= n_new) { flag(status, DEV_BAD_INDEX); return; }
+    for (int k = 0; k < 6; k++) {
+        gcol_new[q * 6 + k] = gcol[r * 6 + k];
+        gval_new[q * 6 + k] = gval[r * 6 + k];
+    }
+}
+
+__global__ void aux_relabel_kernel(long long nnz, long long n_old, const int64_t* __restrict__ new_of_old,
+                                   int* __restrict__ gt_row, int* status) {
+    long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= nnz) return;
+    int r = gt_row[k];
+    if (r < 0 || r >= n_old) { flag(status, DEV_BAD_INDEX); return; }
+    gt_row[k] = (int)new_of_old[r];
 }
 
 extern "C" {
@@ -1085,6 +1112,41 @@ int emfem_aux_reserve(emfem_aux a, int nsys) {
 int emfem_aux_set_network(emfem_aux a, const float* params) {
     EMFEM_REQUIRE(a, "emfem_aux_set_network: null");
     a->params = (float*)params;
+    return EMFEM_OK;
+}
+
+int emfem_aux_set_rows(emfem_aux a, int64_t n_new, const int64_t* new_of_old, int ngroups, const int32_t* aux_group) {
+    EMFEM_REQUIRE(a && new_of_old && n_new >= a->n && n_new < (1LL << 31) && (n_new % 2) == 0,
+                  "emfem_aux_set_rows: bad argument (n_new must be even, >= the current rows, < 2^31)");
+    EMFEM_REQUIRE(ngroups >= 1 && (ngroups == 1 || aux_group), "emfem_aux_set_rows: aux_group required for ngroups > 1");
+    cudaStream_t st = a->h->stream;
+    int* gcol_new = nullptr;
+    double* gval_new = nullptr;
+    int* grp = nullptr;
+    int rc = EMFEM_OK;
+    if ((rc = check_cuda(cudaMalloc(&gcol_new, n_new * 6 * sizeof(int)), "cudaMalloc")) != EMFEM_OK) return rc;
+    if ((rc = check_cuda(cudaMalloc(&gval_new, n_new * 6 * sizeof(double)), "cudaMalloc")) != EMFEM_OK) {
+        cudaFree(gcol_new);
+        return rc;
+    }
+    if (ngroups > 1 && (rc = check_cuda(cudaMalloc(&grp, a->na * sizeof(int)), "cudaMalloc")) != EMFEM_OK) {
+        cudaFree(gcol_new); cudaFree(gval_new);
+        return rc;
+    }
+    cudaMemsetAsync(gcol_new, 0xff, n_new * 6 * sizeof(int), st);
+    cudaMemsetAsync(gval_new, 0, n_new * 6 * sizeof(double), st);
+    aux_move_rows_kernel<<<grid_for(a->n, AB), AB, 0, st>>>(a->n, n_new, new_of_old, a->gcol, a->gval, gcol_new, gval_new,
+                                                            a->h->dev_status);
+    if (a->nnz_gt > 0)
+        aux_relabel_kernel<<<grid_for(a->nnz_gt, AB), AB, 0, st>>>(a->nnz_gt, a->n, new_of_old, a->gt_row, a->h->dev_status);
+    if (grp) cudaMemcpyAsync(grp, aux_group, a->na * sizeof(int), cudaMemcpyDeviceToDevice, st);
+    rc = check_cuda(cudaStreamSynchronize(st), "emfem_aux_set_rows");
+    if (rc != EMFEM_OK) { cudaFree(gcol_new); cudaFree(gval_new); cudaFree(grp); return rc; }
+    cudaFree(a->gcol); cudaFree(a->gval); cudaFree(a->agroup);
+    a->gcol = gcol_new; a->gval = gval_new; a->agroup = grp;
+    a->n = n_new;
+    a->ngroups = ngroups;
+    a->have_operator = false;
     return EMFEM_OK;
 }
 

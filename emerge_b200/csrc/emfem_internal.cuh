@@ -96,6 +96,8 @@ struct emfem_aux_s {
     float* params = nullptr;    // [EMFEM_MPNN_NPARAMS], caller-owned device memory
     void* kbuf = nullptr;       // solve-time buffers (emfem_aux_reserve)
     size_t kbuf_bytes = 0;
+    int* agroup = nullptr;      // [na] group of every aux node in a grouped (multi-mesh) solve, or null
+    int ngroups = 1;
 };
 
 namespace emfem {

@@ -1022,6 +1022,8 @@ static int krylov_impl(emfem_handle hd, int method, int64_t n, int64_t nnz, cons
                   "emfem_krylov_solve: precond 3/4 need BiCGStab and an aux space of this field with its operator "
                   "set (emfem_aux_set_operator, same ports)");
     EMFEM_REQUIRE(precond != 4 || aux->params, "emfem_krylov_solve: precond 4 needs network parameters (emfem_aux_set_network)");
+    EMFEM_REQUIRE(precond < 3 || aux->ngroups == G,
+                  "emfem_krylov_solve: the aux space's groups (emfem_aux_set_rows) must match the solve's groups");
     EMFEM_REQUIRE(n_ports >= 0 && n_ports <= 8, "emfem_krylov_solve: at most 8 ports");
     EMFEM_REQUIRE(n_patch_rows == 0 || (patch_rows && patch_rowptr && patch_cols && patch_vals && patch_port && gamma),
                   "emfem_krylov_solve: patch arrays missing");
@@ -1039,8 +1041,8 @@ static int krylov_impl(emfem_handle hd, int method, int64_t n, int64_t nnz, cons
                   "emfem_krylov_solve: call emfem_aux_reserve with at least nsys systems first");
     std::vector<int> hgblk(G + 1, 0);
     if (G > 1) {
-        EMFEM_REQUIRE(pair_group && precision == 0 && precond <= 2,
-                      "emfem_krylov_solve_grouped: pair_group required; FP64 only, precond 0-2");
+        EMFEM_REQUIRE(pair_group && precision == 0 && precond <= 3,
+                      "emfem_krylov_solve_grouped: pair_group required; FP64 only, precond 0-3");
         EMFEM_REQUIRE((n / 2) % VB == 0, "emfem_krylov_solve_grouped: n/2 must be a multiple of 256");
         std::vector<int> hp(n / 2);
         EMFEM_CUDA(cudaMemcpy(hp.data(), pair_group, sizeof(int) * (n / 2), cudaMemcpyDeviceToHost));
@@ -1291,11 +1293,12 @@ int emfem_krylov_solve_grouped(emfem_handle hd, int method, int64_t n, int64_t n
                                const int32_t* patch_rows, const int32_t* patch_rowptr, const int32_t* patch_cols,
                                const void* patch_vals, const int32_t* patch_port, int n_ports, const double* gamma,
                                const uint8_t* free_mask, const void* rhs, void* x, double tol, int maxit, int precond,
-                               void* workspace, size_t workspace_bytes, int* status, int* iters, double* relres) {
+                               void* workspace, size_t workspace_bytes, int* status, int* iters, double* relres,
+                               emfem_aux aux) {
     EMFEM_REQUIRE(ngroups >= 1 && ngroups <= 4096, "emfem_krylov_solve_grouped: 1 <= ngroups <= 4096");
     return krylov_impl(hd, method, n, nnz, indptr, indices, E_vals, B_vals, nsys, k0sq, n_patch_rows, patch_rows,
                        patch_rowptr, patch_cols, patch_vals, patch_port, n_ports, gamma, free_mask, rhs, x, tol, maxit,
-                       precond, 0, workspace, workspace_bytes, status, iters, relres, nullptr, ngroups, pair_group);
+                       precond, 0, workspace, workspace_bytes, status, iters, relres, aux, ngroups, pair_group);
 }
 
 }  // extern "C"

@@ -174,7 +174,8 @@ int emfem_krylov_solve(emfem_handle h, int method, int64_t n, int64_t nnz, const
  * through 0..G-1 in order with every group starting at a multiple of 256 DOF pairs (pad a group's
  * rows with eliminated DOFs).  The CSR is block diagonal over the groups.  k0sq (G nsys), gamma
  * (G nsys n_ports complex) are host arrays; status / iters / relres have G nsys entries; rhs and x
- * are (n, nsys) c128.  FP64 vectors, precond 0-2, method 0 or 1; otherwise as emfem_krylov_solve.
+ * are (n, nsys) c128.  FP64 vectors, precond 0-3 (3 with an aux space moved onto the grouped rows by
+ * emfem_aux_set_rows, same ngroups), method 0 or 1 (1 for precond 3); otherwise as emfem_krylov_solve.
  * One graph-captured iteration serves every system of every group; each system keeps its own
  * scalars and convergence test. */
 int emfem_krylov_workspace_size_grouped(int64_t n, int64_t nnz, int nsys, int ngroups, size_t *bytes);
@@ -184,7 +185,8 @@ int emfem_krylov_solve_grouped(emfem_handle h, int method, int64_t n, int64_t nn
                                const int32_t *patch_rows, const int32_t *patch_rowptr, const int32_t *patch_cols,
                                const void *patch_vals, const int32_t *patch_port, int n_ports, const double *gamma,
                                const uint8_t *free_mask, const void *rhs, void *x, double tol, int maxit, int precond,
-                               void *workspace, size_t workspace_bytes, int *status, int *iters, double *relres);
+                               void *workspace, size_t workspace_bytes, int *status, int *iters, double *relres,
+                               emfem_aux aux);
 
 /* y_s = A_s x_s for the operator of emfem_krylov_solve (FP64), eliminated rows/cols as there;
  * nsys a power of two <= 256; k0sq_dev and gamma_dev are device arrays. */
@@ -306,6 +308,11 @@ int emfem_aux_set_operator(emfem_aux aux, int64_t n, const int32_t *indptr, cons
                            const int32_t *patch_rowptr, const int32_t *patch_cols, const void *patch_vals,
                            const int32_t *patch_port, int n_ports, const uint8_t *free_mask, void *diag_out,
                            uint8_t *mask_out);
+/* Moves the aux space onto the rows of a grouped (multi-mesh) system: row r of its own numbering
+ * becomes row new_of_old[r] (device i64, n_old entries) of an n_new-row system; aux_group (device i32,
+ * n_aux entries) is the group of every aux node, null when ngroups is 1.  Call before
+ * emfem_aux_set_operator with the grouped operator.  No counterpart in the reference. */
+int emfem_aux_set_rows(emfem_aux aux, int64_t n_new, const int64_t *new_of_old, int ngroups, const int32_t *aux_group);
 int emfem_aux_reserve(emfem_aux aux, int nsys);
 int emfem_aux_set_network(emfem_aux aux, const float *params);
 int emfem_aux_destroy(emfem_aux aux);

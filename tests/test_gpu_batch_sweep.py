@@ -57,3 +57,25 @@ def test_grouped_layout_is_validated(cuda):
     bs.pair_group = bad
     with pytest.raises(EmfemError):
         bs.solve([[(9e9, 0)], [(10e9, 0)]], tol=1e-8, maxit=10)
+
+
+def test_grouped_aux_sweep_matches_separate_aux_sweeps(cuda):
+    """precond="aux" over a batch: the union's auxiliary nodal space moved onto the grouped rows, its
+    diagonals per system from each aux node's own mesh and frequency."""
+    Ps = _mixed_problems()
+    bs = BatchSweep(Ps)
+    systems = [[(9e9, 0), (9e9, 1), (11e9, 0)],
+               [(10e9, 0), (10e9, 1), (8.5e9, 1)],
+               [(12e9, 0), (8e9, 0), (10e9, 0)]]
+    res = bs.solve(systems, tol=1e-11, maxit=20000, precond="aux")
+    for g, P in enumerate(Ps):
+        r = res[g]
+        assert (r.status == 0).all(), (g, r.status, r.iters, r.relres)
+        ref = FrequencySweep(P).solve(systems[g], tol=1e-11, maxit=20000, precond="aux")
+        assert (ref.status == 0).all()
+        err = (torch.linalg.vector_norm(r.x - ref.x, dim=0) / torch.linalg.vector_norm(ref.x, dim=0)).cpu().numpy()
+        assert err.max() <= 1e-8, (g, err)
+        # the aux correction still cuts the iterations by an order of magnitude, as for one mesh
+        assert r.iters.max() <= 3 * ref.iters.max() + 50, (r.iters, ref.iters)
+        alone = BatchSweep([P]).solve([systems[g]], tol=1e-11, maxit=20000, precond="aux")[0]
+        assert torch.equal(alone.x, r.x) and np.array_equal(alone.iters, r.iters), (alone.iters, r.iters)

@@ -158,6 +158,9 @@ class BatchSweep:
         self.B = B[slot].contiguous()
         self.nnz = nnz
         self.plan = SimpleNamespace(indptr=self.indptr, indices=self.indices, nnz=nnz)
+        # the union-ordered values are not needed again: keep one copy of E and B on the device
+        self.batch.E = self.batch.B = None
+        del E, B
         self._perm = perm_d
         self._aux = None
         del slot, row_of_slot, start_u, lens

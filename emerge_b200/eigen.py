@@ -94,24 +94,42 @@ def eigenmodes(sweep, nmodes: int = 4, target_k0: float = 1.0, tol: float = 1e-1
     A = LinearOperator((nf, nf), matvec=stiff, dtype=np.complex128)
     M = LinearOperator((nf, nf), matvec=mass, dtype=np.complex128)
     OPinv = LinearOperator((nf, nf), matvec=opinv, dtype=np.complex128)
-    v0 = np.random.default_rng(seed).standard_normal(nf) + 0j      # reproducible ARPACK start
-    vals, vecs = eigs(A, k=nmodes, M=M, sigma=sigma, which="LM", OPinv=OPinv, tol=arpack_tol, v0=v0)
-    order = np.argsort(np.abs(vals - sigma))
-    vals, vecs = vals[order], vecs[:, order]
-    # ARPACK with an iterative inverse can return a Ritz pair that is not an eigenpair (a strongly
-    # damped mode of an open resonator): judge every pair by its residual with the device operators
-    res = np.zeros(nmodes)
-    for j in range(nmodes):
-        x = full(vecs[:, j])
-        ex = torch.empty_like(x)
-        check(lib().emfem_sweep_spmv(h.h, N, ptr(sweep.plan.indptr), ptr(sweep.plan.indices), ptr(sweep.E), None, 1,
-                                     ptr(one), 0, None, None, None, None, None, 0, ptr(gam_mass), ptr(sweep.mask),
-                                     ptr(x), ptr(ex)), "emfem_sweep_spmv")
-        exf = ex[free, 0].cpu().numpy()
-        mx = mass(vecs[:, j])
-        r = exf - vals[j] * mx
-        # scaled by ||E x|| + σ ||M x||: meaningful for the λ ≈ 0 gradient modes too (E x ≈ 0)
-        res[j] = np.linalg.norm(r) / max(np.linalg.norm(exf) + sigma * np.linalg.norm(mx), 1e-300)
+
+    def residuals(vals, vecs):
+        # ARPACK with an iterative inverse can return a Ritz pair that is not an eigenpair (a strongly
+        # damped mode of an open resonator, or an unresolved near-degenerate pair): judge every pair by
+        # its residual with the device operators
+        res = np.zeros(len(vals))
+        for j in range(len(vals)):
+            x = full(vecs[:, j])
+            ex = torch.empty_like(x)
+            check(lib().emfem_sweep_spmv(h.h, N, ptr(sweep.plan.indptr), ptr(sweep.plan.indices), ptr(sweep.E), None,
+                                         1, ptr(one), 0, None, None, None, None, None, 0, ptr(gam_mass),
+                                         ptr(sweep.mask), ptr(x), ptr(ex)), "emfem_sweep_spmv")
+            exf = ex[free, 0].cpu().numpy()
+            mx = mass(vecs[:, j])
+            r = exf - vals[j] * mx
+            # scaled by ||E x|| + σ ||M x||: meaningful for the λ ≈ 0 gradient modes too (E x ≈ 0)
+            res[j] = np.linalg.norm(r) / max(np.linalg.norm(exf) + sigma * np.linalg.norm(mx), 1e-300)
+        return res
+
+    # ARPACK draws the restart vectors it needs after an invariant subspace from a generator whose
+    # state persists in the process, so an unresolved cluster can depend on earlier calls: when a pair
+    # fails the residual test, the search is repeated from other seeded start vectors and the attempt
+    # with the most converged pairs (then the smallest residual of the nearest pair) is kept
+    best = None
+    for attempt in range(3):
+        v0 = np.random.default_rng(seed + attempt).standard_normal(nf) + 0j      # reproducible start
+        vals, vecs = eigs(A, k=nmodes, M=M, sigma=sigma, which="LM", OPinv=OPinv, tol=arpack_tol, v0=v0)
+        order = np.argsort(np.abs(vals - sigma))
+        vals, vecs = vals[order], vecs[:, order]
+        res = residuals(vals, vecs)
+        key = (int((res <= residual_tol).sum()), -res[0])
+        if best is None or key > best[0]:
+            best = (key, vals, vecs, res)
+        if (res <= residual_tol).all():
+            break
+    _, vals, vecs, res = best
     modes = np.zeros((N, nmodes), dtype=np.complex128)
     modes[free.cpu().numpy()] = vecs
     return EigenResult(vals, np.sqrt(np.abs(vals.real)) * C0 / (2 * np.pi), modes, stats["solves"], stats["iters"],

@@ -163,6 +163,7 @@ class BatchSweep:
         del E, B
         self._perm = perm_d
         self._aux = None
+        self.network = None
         del slot, row_of_slot, start_u, lens
         # per mesh: Robin / port terms and port vectors (built on each mesh's own numbering), mask
         self.sweeps = []
@@ -214,8 +215,8 @@ class BatchSweep:
         if len(systems) != G or len({len(s) for s in systems}) != 1:
             raise ValueError("give the same number of systems for every mesh")
         nsys = len(systems[0])
-        if PRECOND[precond] > 3:
-            raise ValueError("grouped solves take precond none, jacobi, block_jacobi or aux")
+        if PRECOND[precond] == 4 and self.network is None:
+            raise ValueError("precond='learned' needs a network (BatchSweep.set_network)")
         npt = max(self.n_ports, 1)
         k0 = np.zeros(G * nsys)
         gam = np.zeros((G * nsys, npt), dtype=np.complex128)
@@ -239,7 +240,7 @@ class BatchSweep:
         it = (ctypes.c_int * (G * nsys))()
         rr = (ctypes.c_double * (G * nsys))()
         aux = None
-        if PRECOND[precond] == 3:
+        if PRECOND[precond] >= 3:
             a = self.aux_space()
             a.reserve(nsys)
             aux = a.handle
@@ -285,6 +286,12 @@ class BatchSweep:
             aux.set_operator(self)
             self._aux = aux
         return self._aux
+
+    def set_network(self, net) -> None:
+        """Use this :class:`auxspace.Network` for ``precond="learned"`` on every mesh (its weights are per
+        aux-node type, so a network trained on one mesh applies to the union)."""
+        self.network = net
+        self.aux_space().set_network(net.params if net is not None else None)
 
     def sparams(self, g: int, res) -> dict:
         """S-parameters of mesh g's solved systems (``FrequencySweep.sparams``)."""

@@ -1041,8 +1041,8 @@ static int krylov_impl(emfem_handle hd, int method, int64_t n, int64_t nnz, cons
                   "emfem_krylov_solve: call emfem_aux_reserve with at least nsys systems first");
     std::vector<int> hgblk(G + 1, 0);
     if (G > 1) {
-        EMFEM_REQUIRE(pair_group && precision == 0 && precond <= 3,
-                      "emfem_krylov_solve_grouped: pair_group required; FP64 only, precond 0-3");
+        EMFEM_REQUIRE(pair_group && precision == 0,
+                      "emfem_krylov_solve_grouped: pair_group required; FP64 only");
         EMFEM_REQUIRE((n / 2) % VB == 0, "emfem_krylov_solve_grouped: n/2 must be a multiple of 256");
         std::vector<int> hp(n / 2);
         EMFEM_CUDA(cudaMemcpy(hp.data(), pair_group, sizeof(int) * (n / 2), cudaMemcpyDeviceToHost));

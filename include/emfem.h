@@ -174,8 +174,9 @@ int emfem_krylov_solve(emfem_handle h, int method, int64_t n, int64_t nnz, const
  * through 0..G-1 in order with every group starting at a multiple of 256 DOF pairs (pad a group's
  * rows with eliminated DOFs).  The CSR is block diagonal over the groups.  k0sq (G nsys), gamma
  * (G nsys n_ports complex) are host arrays; status / iters / relres have G nsys entries; rhs and x
- * are (n, nsys) c128.  FP64 vectors, precond 0-3 (3 with an aux space moved onto the grouped rows by
- * emfem_aux_set_rows, same ngroups), method 0 or 1 (1 for precond 3); otherwise as emfem_krylov_solve.
+ * are (n, nsys) c128.  FP64 vectors, precond 0-4 (3 and 4 with an aux space moved onto the grouped rows
+ * by emfem_aux_set_rows, same ngroups; the network's weights are per node type, so one network serves
+ * every mesh), method 0 or 1 (1 for precond 3-4); otherwise as emfem_krylov_solve.
  * One graph-captured iteration serves every system of every group; each system keeps its own
  * scalars and convergence test. */
 int emfem_krylov_workspace_size_grouped(int64_t n, int64_t nnz, int nsys, int ngroups, size_t *bytes);

@@ -79,3 +79,24 @@ def test_grouped_aux_sweep_matches_separate_aux_sweeps(cuda):
         assert r.iters.max() <= 3 * ref.iters.max() + 50, (r.iters, ref.iters)
         alone = BatchSweep([P]).solve([systems[g]], tol=1e-11, maxit=20000, precond="aux")[0]
         assert torch.equal(alone.x, r.x) and np.array_equal(alone.iters, r.iters), (alone.iters, r.iters)
+
+
+def test_grouped_learned_sweep_matches_separate_learned_sweeps(cuda):
+    """precond="learned" over a batch: one network (weights per aux-node type) on the union's aux space."""
+    from emerge_b200.auxspace import Network
+    Ps = _mixed_problems()
+    bs = BatchSweep(Ps)
+    net = Network(bs.aux_space(), seed=4, init="random")
+    net.params.mul_(0.5)                         # a mild random correction that still converges
+    bs.set_network(net)
+    systems = [[(9e9, 0), (11e9, 0)], [(10e9, 0), (10e9, 1)], [(12e9, 0), (8e9, 0)]]
+    res = bs.solve(systems, tol=1e-11, maxit=20000, precond="learned")
+    for g, P in enumerate(Ps):
+        r = res[g]
+        assert (r.status == 0).all(), (g, r.status, r.iters, r.relres)
+        sw = FrequencySweep(P)
+        sw.set_network(Network(sw.aux_space(), params=net.params))
+        ref = sw.solve(systems[g], tol=1e-11, maxit=20000, precond="learned")
+        assert (ref.status == 0).all()
+        err = (torch.linalg.vector_norm(r.x - ref.x, dim=0) / torch.linalg.vector_norm(ref.x, dim=0)).cpu().numpy()
+        assert err.max() <= 1e-8, (g, err)

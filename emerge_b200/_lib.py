@@ -95,10 +95,10 @@ _SIGS = {
     "emfem_ned2_tri_abc2": ([_vp, _i64, _vp, _i64, _vp, _dbl, _dbl, _vp], _i32),
     "emfem_ned2_bma_tri_matrices": ([_vp, _i64, _vp, _i64, _vp, _i64, _vp, _vp, _vp, _vp, _dbl, _vp, _vp], _i32),
     "emfem_ned2_tri_field": ([_vp, _i64, _vp, _i64, _vp, _i64, _vp, _vp, _vp, _i64, _vp, _i32, _vp, _i32, _dbl, _dbl, _vp, _vp], _i32),
-    "emfem_krylov_workspace_size_grouped": ([_i64, _i64, _i32, _i32, ctypes.POINTER(ctypes.c_size_t)], _i32),
+    "emfem_krylov_workspace_size_grouped": ([_i64, _i64, _i32, _i32, _i32, ctypes.POINTER(ctypes.c_size_t)], _i32),
     "emfem_krylov_solve_grouped": ([_vp, _i32, _i64, _i64, _vp, _vp, _vp, _vp, _i32, _vp, _i32, _dblp,
                                     _i64, _vp, _vp, _vp, _vp, _vp, _i32, _dblp, _vp, _vp, _vp,
-                                    _dbl, _i32, _i32, _vp, ctypes.c_size_t, _i32p, _i32p, _dblp, _vp], _i32),
+                                    _dbl, _i32, _i32, _i32, _vp, ctypes.c_size_t, _i32p, _i32p, _dblp, _vp], _i32),
     "emfem_aux_set_rows": ([_vp, _i64, _vp, _i32, _vp], _i32),
     "emfem_point_field_dot": ([_vp, _i64, _vp, _i64, _vp, _vp, _i64, _i64, _vp, _vp, _vp, _i32, _vp, _vp], _i32),
     "emfem_sweep_spmv_noalloc": ([_vp, _i64, _vp, _vp, _vp, _vp, _i32, _vp, _i64, _vp, _vp, _vp, _vp, _vp, _i32,

@@ -204,13 +204,13 @@ class BatchSweep:
         return torch.where(d < H, self.hoff[g] + d, self.h + self.hoff[g] + d - H)
 
     def solve(self, systems, tol: float = 1e-8, maxit: int = 20000, precond: str = "block_jacobi",
-              method: str = "bicgstab"):
+              method: str = "bicgstab", precision: str = "fp64"):
         """systems: one list of (frequency, port) per mesh, all of the same length (<= 64).  Returns one
         ``SolveResult`` per mesh, solutions in that mesh's own DOF numbering."""
         import ctypes
         from ._lib import ERR_NOT_CONVERGED, Handle, check, lib, ptr
         from .ports import k0_of
-        from .sweep import METHOD, PRECOND, SolveResult
+        from .sweep import METHOD, PRECISION, PRECOND, SolveResult
         G = len(self.problems)
         if len(systems) != G or len({len(s) for s in systems}) != 1:
             raise ValueError("give the same number of systems for every mesh")
@@ -231,7 +231,8 @@ class BatchSweep:
                 b[loc] = fs.rhs(sl)
         ga = np.ascontiguousarray(np.stack([gam.real, gam.imag], axis=-1).reshape(-1))
         sz = ctypes.c_size_t()
-        check(lib().emfem_krylov_workspace_size_grouped(self.n, self.nnz, nsys, G, ctypes.byref(sz)),
+        prec = PRECISION[precision]
+        check(lib().emfem_krylov_workspace_size_grouped(self.n, self.nnz, nsys, G, prec, ctypes.byref(sz)),
               "emfem_krylov_workspace_size_grouped")
         if self._ws is None or self._ws.numel() < sz.value:
             self._ws = torch.empty(sz.value, dtype=torch.uint8, device=self.device)
@@ -251,7 +252,7 @@ class BatchSweep:
             ptr(self.pair_group), nsys, (ctypes.c_double * (G * nsys))(*k0), self.patch_rows.numel(),
             ptr(self.patch_rows), ptr(self.patch_rowptr), ptr(self.patch_cols), ptr(self.patch_vals),
             ptr(self.patch_port), self.n_ports, (ctypes.c_double * len(ga))(*ga), ptr(self.mask), ptr(b), ptr(x),
-            tol, maxit, PRECOND[precond], ptr(self._ws), self._ws.numel(), st, it, rr, aux)
+            tol, maxit, PRECOND[precond], prec, ptr(self._ws), self._ws.numel(), st, it, rr, aux)
         torch.cuda.synchronize(self.device)
         dt = time.perf_counter() - t0
         if rc not in (0, ERR_NOT_CONVERGED):

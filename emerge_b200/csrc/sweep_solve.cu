@@ -699,25 +699,30 @@ __global__ void precond_setup_kernel(OpArgs a, int precond, typename V2<R>::T* _
 }
 
 // conversions / scaled copies for the mixed-precision refinement
-__global__ void to_f32_scaled_kernel(long long n, int S, const double2* __restrict__ src, const SysState* st64,
-                                     float2* __restrict__ dst, double* __restrict__ scale) {
+// scale[q] = ||r_q|| of every system (grouped: G S of them)
+__global__ void state_scale_kernel(int GS, const SysState* __restrict__ st64, double* __restrict__ scale) {
+    int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q < GS) scale[q] = sqrt(st64[q].rn2);
+}
+
+__global__ void to_f32_scaled_kernel(long long n, int S, const int* __restrict__ pg, const double2* __restrict__ src,
+                                     const double* __restrict__ scale, float2* __restrict__ dst) {
     long long g = (long long)blockIdx.x * VB + threadIdx.x;
     if (g >= n * S) return;
-    int s = (int)(g % S);
-    double rn = sqrt(st64[s].rn2);
+    double rn = scale[sys_of_row(pg, n / 2, g / S, S, (int)(g % S))];
     double sc = rn > 0 ? 1.0 / rn : 0.0;
     double2 v = src[g];
     dst[g] = make_float2((float)(v.x * sc), (float)(v.y * sc));
-    if (g < S) scale[g] = rn;
 }
 
-__global__ void add_scaled_f32_kernel(long long n, int S, const float2* __restrict__ d, const double* __restrict__ scale,
-                                      const SysState* __restrict__ outer, double2* __restrict__ x) {
+__global__ void add_scaled_f32_kernel(long long n, int S, const int* __restrict__ pg, const float2* __restrict__ d,
+                                      const double* __restrict__ scale, const SysState* __restrict__ outer,
+                                      double2* __restrict__ x) {
     long long g = (long long)blockIdx.x * VB + threadIdx.x;
     if (g >= n * S) return;
-    int s = (int)(g % S);
-    if (!outer[s].active) return;
-    double sc = scale[s];
+    const int sy = sys_of_row(pg, n / 2, g / S, S, (int)(g % S));
+    if (!outer[sy].active) return;
+    double sc = scale[sy];
     float2 v = d[g];
     x[g].x += sc * (double)v.x;
     x[g].y += sc * (double)v.y;
@@ -729,9 +734,9 @@ __global__ void cast_values_kernel(long long nnz, const double2* __restrict__ sr
 }
 
 // inner state for one refinement step: unit-norm rhs, relative tolerance `itol`, active = outer active
-__global__ void inner_init_kernel(SysState* inner, const SysState* outer, int S, double itol) {
-    int s = threadIdx.x;
-    if (s >= S) return;
+__global__ void inner_init_kernel(SysState* inner, const SysState* outer, int GS, double itol) {
+    int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= GS) return;
     SysState z;
     z.rho = z.alpha = z.beta = z.omega = make_double2(0, 0);
     z.alpha.x = 1.0; z.omega.x = 1.0;
@@ -1041,8 +1046,7 @@ static int krylov_impl(emfem_handle hd, int method, int64_t n, int64_t nnz, cons
                   "emfem_krylov_solve: call emfem_aux_reserve with at least nsys systems first");
     std::vector<int> hgblk(G + 1, 0);
     if (G > 1) {
-        EMFEM_REQUIRE(pair_group && precision == 0,
-                      "emfem_krylov_solve_grouped: pair_group required; FP64 only");
+        EMFEM_REQUIRE(pair_group, "emfem_krylov_solve_grouped: pair_group required");
         EMFEM_REQUIRE((n / 2) % VB == 0, "emfem_krylov_solve_grouped: n/2 must be a multiple of 256");
         std::vector<int> hp(n / 2);
         EMFEM_CUDA(cudaMemcpy(hp.data(), pair_group, sizeof(int) * (n / 2), cudaMemcpyDeviceToHost));
@@ -1159,6 +1163,9 @@ static int krylov_impl(emfem_handle hd, int method, int64_t n, int64_t nnz, cons
         for (int q = 0; q < 6; q++) k.v[q] = (float2*)(ws + L.off_v[q]);
         k.partial = partial; k.st = st; k.s = s;
         k.op.skip = st;
+        k.G = G; k.pg = G > 1 ? pair_group : nullptr; k.gblk = gblk;
+        const int* pgk = k.pg;
+        const size_t GSm = (size_t)G * S;
         if (precond) {
             precond_setup_kernel<float><<<grid_for((n / 2) * (long long)S, VB), VB, 0, s>>>(op64, k.bj(), k.minv);
             STRY(check_cuda(cudaGetLastError(), "precond_setup"));
@@ -1168,39 +1175,40 @@ static int krylov_impl(emfem_handle hd, int method, int64_t n, int64_t nnz, cons
             k.adinv = (float2*)aux_dinv_buffer(aux, S);
             STRY(aux_setup_dinv<float2>(aux, S, nsys, k0dev, gdev, k.adinv, s));
         }
-        std::vector<SysState> ho(S);
+        std::vector<SysState> ho(GSm);
         int used = 0;
         for (int outer = 0; outer < 60; outer++) {
-            STRY(check_cuda(cudaMemcpyAsync(ho.data(), st_outer, sizeof(SysState) * S, cudaMemcpyDeviceToHost, s), "copy"));
+            STRY(check_cuda(cudaMemcpyAsync(ho.data(), st_outer, sizeof(SysState) * GSm, cudaMemcpyDeviceToHost, s), "copy"));
             STRY(check_cuda(cudaStreamSynchronize(s), "sync"));
             bool any = false;
-            for (int q = 0; q < S; q++) any |= ho[q].active != 0;
+            for (size_t q = 0; q < GSm; q++) any |= ho[q].active != 0;
             if (!any || used >= maxit) break;
-            to_f32_scaled_kernel<<<gv, VB, 0, s>>>(n, S, r64, st_outer, r32, scale);
+            state_scale_kernel<<<grid_for((long long)GSm, 64), 64, 0, s>>>((int)GSm, st_outer, scale);
+            to_f32_scaled_kernel<<<gv, VB, 0, s>>>(n, S, pgk, r64, scale, r32);
             STRY(check_cuda(cudaMemsetAsync(d32, 0, sizeof(float2) * nS, s), "memset d"));
-            inner_init_kernel<<<1, 64, 0, s>>>(st, st_outer, S, EMFEM_INNER_TOL);
+            inner_init_kernel<<<grid_for((long long)GSm, 64), 64, 0, s>>>(st, st_outer, (int)GSm, EMFEM_INNER_TOL);
             k.maxit = std::max(1, maxit - used);
             STRY(k.start());
             STRY(k.run(16));
-            std::vector<SysState> hin(S);
-            STRY(check_cuda(cudaMemcpyAsync(hin.data(), st, sizeof(SysState) * S, cudaMemcpyDeviceToHost, s), "copy"));
+            std::vector<SysState> hin(GSm);
+            STRY(check_cuda(cudaMemcpyAsync(hin.data(), st, sizeof(SysState) * GSm, cudaMemcpyDeviceToHost, s), "copy"));
             STRY(check_cuda(cudaStreamSynchronize(s), "sync"));
             int mx = 1;
-            for (int q = 0; q < S; q++) if (ho[q].active) mx = std::max(mx, hin[q].iters);
+            for (size_t q = 0; q < GSm; q++) if (ho[q].active) mx = std::max(mx, hin[q].iters);
             used += mx;
-            add_scaled_f32_kernel<<<gv, VB, 0, s>>>(n, S, d32, scale, st_outer, x64);
+            add_scaled_f32_kernel<<<gv, VB, 0, s>>>(n, S, pgk, d32, scale, st_outer, x64);
             spmv_kernel<double><<<gv, VB, 0, s>>>(op64, x64, Ax, nullptr, DOT_NONE, nullptr);
             residual_kernel<<<gv, VB, 0, s>>>(n, S, free_mask, b64, Ax, r64, partial);
             // the inner state array is free now: reuse it to reduce ||b||^2, ||r||^2 of the new residual
-            reduce_update_kernel<<<S, VB, 0, s>>>(partial, (int)gv, S, 2, st, UPD_INIT, maxit, 1.0, S);
+            reduce_update_kernel<<<G * S, VB, 0, s>>>(partial, (int)gv, S, 2, st, UPD_INIT, maxit, 1.0, S, G, gblk, 1, nbh);
             STRY(check_cuda(cudaGetLastError(), "refinement"));
-            std::vector<SysState> hr(S);
-            STRY(check_cuda(cudaMemcpyAsync(hr.data(), st, sizeof(SysState) * S, cudaMemcpyDeviceToHost, s), "copy"));
+            std::vector<SysState> hr(GSm);
+            STRY(check_cuda(cudaMemcpyAsync(hr.data(), st, sizeof(SysState) * GSm, cudaMemcpyDeviceToHost, s), "copy"));
             STRY(check_cuda(cudaStreamSynchronize(s), "sync"));
             // a correction that did not lower the FP64 residual is reverted and the system stops
-            std::vector<double> rev(S, 0.0);
+            std::vector<double> rev(GSm, 0.0);
             bool any_rev = false;
-            for (int q = 0; q < S; q++) {
+            for (size_t q = 0; q < GSm; q++) {
                 if (!ho[q].active) continue;
                 ho[q].iters += hin[q].iters;
                 double prev = ho[q].rn2;
@@ -1215,16 +1223,16 @@ static int krylov_impl(emfem_handle hd, int method, int64_t n, int64_t nnz, cons
                 else if (ho[q].rn2 >= 0.98 * prev) { ho[q].active = 0; ho[q].status = 2; }
             }
             if (any_rev) {
-                STRY(check_cuda(cudaMemcpyAsync(scale, rev.data(), sizeof(double) * S, cudaMemcpyHostToDevice, s), "copy"));
-                add_scaled_f32_kernel<<<gv, VB, 0, s>>>(n, S, d32, scale, st_outer, x64);
+                STRY(check_cuda(cudaMemcpyAsync(scale, rev.data(), sizeof(double) * GSm, cudaMemcpyHostToDevice, s), "copy"));
+                add_scaled_f32_kernel<<<gv, VB, 0, s>>>(n, S, pgk, d32, scale, st_outer, x64);
                 STRY(check_cuda(cudaGetLastError(), "revert"));
             }
-            STRY(check_cuda(cudaMemcpyAsync(st_outer, ho.data(), sizeof(SysState) * S, cudaMemcpyHostToDevice, s), "copy"));
+            STRY(check_cuda(cudaMemcpyAsync(st_outer, ho.data(), sizeof(SysState) * GSm, cudaMemcpyHostToDevice, s), "copy"));
         }
-        STRY(check_cuda(cudaMemcpyAsync(ho.data(), st_outer, sizeof(SysState) * S, cudaMemcpyDeviceToHost, s), "copy"));
+        STRY(check_cuda(cudaMemcpyAsync(ho.data(), st_outer, sizeof(SysState) * GSm, cudaMemcpyDeviceToHost, s), "copy"));
         STRY(check_cuda(cudaStreamSynchronize(s), "sync"));
-        for (int q = 0; q < S; q++) if (ho[q].active) { ho[q].active = 0; ho[q].status = 1; }
-        STRY(check_cuda(cudaMemcpyAsync(st, ho.data(), sizeof(SysState) * S, cudaMemcpyHostToDevice, s), "copy"));
+        for (size_t q = 0; q < GSm; q++) if (ho[q].active) { ho[q].active = 0; ho[q].status = 1; }
+        STRY(check_cuda(cudaMemcpyAsync(st, ho.data(), sizeof(SysState) * GSm, cudaMemcpyHostToDevice, s), "copy"));
     }
     {
         // final FP64 true residual and solution copy-out
@@ -1280,10 +1288,10 @@ int emfem_krylov_solve(emfem_handle hd, int method, int64_t n, int64_t nnz, cons
                        precond, precision, workspace, workspace_bytes, status, iters, relres, aux, 1, nullptr);
 }
 
-int emfem_krylov_workspace_size_grouped(int64_t n, int64_t nnz, int nsys, int ngroups, size_t* bytes) {
-    EMFEM_REQUIRE(bytes && n > 0 && nsys > 0 && nsys <= 64 && nnz >= 0 && ngroups >= 1,
+int emfem_krylov_workspace_size_grouped(int64_t n, int64_t nnz, int nsys, int ngroups, int precision, size_t* bytes) {
+    EMFEM_REQUIRE(bytes && n > 0 && nsys > 0 && nsys <= 64 && nnz >= 0 && ngroups >= 1 && (precision == 0 || precision == 1),
                   "emfem_krylov_workspace_size_grouped: bad argument");
-    *bytes = make_layout(n, nnz, nnz, pow2_at_least(nsys), 8, 0, ngroups).total;
+    *bytes = make_layout(n, nnz, nnz, pow2_at_least(nsys), 8, precision, ngroups).total;
     return EMFEM_OK;
 }
 
@@ -1293,12 +1301,12 @@ int emfem_krylov_solve_grouped(emfem_handle hd, int method, int64_t n, int64_t n
                                const int32_t* patch_rows, const int32_t* patch_rowptr, const int32_t* patch_cols,
                                const void* patch_vals, const int32_t* patch_port, int n_ports, const double* gamma,
                                const uint8_t* free_mask, const void* rhs, void* x, double tol, int maxit, int precond,
-                               void* workspace, size_t workspace_bytes, int* status, int* iters, double* relres,
-                               emfem_aux aux) {
+                               int precision, void* workspace, size_t workspace_bytes, int* status, int* iters,
+                               double* relres, emfem_aux aux) {
     EMFEM_REQUIRE(ngroups >= 1 && ngroups <= 4096, "emfem_krylov_solve_grouped: 1 <= ngroups <= 4096");
     return krylov_impl(hd, method, n, nnz, indptr, indices, E_vals, B_vals, nsys, k0sq, n_patch_rows, patch_rows,
                        patch_rowptr, patch_cols, patch_vals, patch_port, n_ports, gamma, free_mask, rhs, x, tol, maxit,
-                       precond, 0, workspace, workspace_bytes, status, iters, relres, aux, ngroups, pair_group);
+                       precond, precision, workspace, workspace_bytes, status, iters, relres, aux, ngroups, pair_group);
 }
 
 }  // extern "C"

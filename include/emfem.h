@@ -174,20 +174,21 @@ int emfem_krylov_solve(emfem_handle h, int method, int64_t n, int64_t nnz, const
  * through 0..G-1 in order with every group starting at a multiple of 256 DOF pairs (pad a group's
  * rows with eliminated DOFs).  The CSR is block diagonal over the groups.  k0sq (G nsys), gamma
  * (G nsys n_ports complex) are host arrays; status / iters / relres have G nsys entries; rhs and x
- * are (n, nsys) c128.  FP64 vectors, precond 0-4 (3 and 4 with an aux space moved onto the grouped rows
+ * are (n, nsys) c128.  precision 0 (FP64) or 1 (FP32 inner solves in FP64 refinement), precond 0-4 (3 and 4 with an aux space moved onto the grouped rows
  * by emfem_aux_set_rows, same ngroups; the network's weights are per node type, so one network serves
  * every mesh), method 0 or 1 (1 for precond 3-4); otherwise as emfem_krylov_solve.
  * One graph-captured iteration serves every system of every group; each system keeps its own
  * scalars and convergence test. */
-int emfem_krylov_workspace_size_grouped(int64_t n, int64_t nnz, int nsys, int ngroups, size_t *bytes);
+int emfem_krylov_workspace_size_grouped(int64_t n, int64_t nnz, int nsys, int ngroups, int precision,
+                                        size_t *bytes);
 int emfem_krylov_solve_grouped(emfem_handle h, int method, int64_t n, int64_t nnz, const int32_t *indptr,
                                const int32_t *indices, const void *E_vals, const void *B_vals, int ngroups,
                                const int32_t *pair_group, int nsys, const double *k0sq, int64_t n_patch_rows,
                                const int32_t *patch_rows, const int32_t *patch_rowptr, const int32_t *patch_cols,
                                const void *patch_vals, const int32_t *patch_port, int n_ports, const double *gamma,
                                const uint8_t *free_mask, const void *rhs, void *x, double tol, int maxit, int precond,
-                               void *workspace, size_t workspace_bytes, int *status, int *iters, double *relres,
-                               emfem_aux aux);
+                               int precision, void *workspace, size_t workspace_bytes, int *status, int *iters,
+                               double *relres, emfem_aux aux);
 
 /* y_s = A_s x_s for the operator of emfem_krylov_solve (FP64), eliminated rows/cols as there;
  * nsys a power of two <= 256; k0sq_dev and gamma_dev are device arrays. */

@@ -100,3 +100,21 @@ def test_grouped_learned_sweep_matches_separate_learned_sweeps(cuda):
         assert (ref.status == 0).all()
         err = (torch.linalg.vector_norm(r.x - ref.x, dim=0) / torch.linalg.vector_norm(ref.x, dim=0)).cpu().numpy()
         assert err.max() <= 1e-8, (g, err)
+
+
+def test_grouped_mixed_precision_sweep_reaches_fp64_residual(cuda):
+    """FP32 inner solves in FP64 refinement over a batch: every system of every mesh reaches the FP64
+    true residual, each mesh's solutions as close to its own mixed-precision sweep as the tolerance allows,
+    and each mesh batched alone gives the same bits."""
+    Ps = _mixed_problems()
+    bs = BatchSweep(Ps)
+    systems = [[(9e9, 0), (11e9, 0)], [(10e9, 0), (10e9, 1)], [(12e9, 0), (8e9, 0)]]
+    res = bs.solve(systems, tol=1e-8, maxit=20000, precond="aux", precision="mixed")
+    for g, P in enumerate(Ps):
+        r = res[g]
+        assert (r.status == 0).all() and (r.relres <= 1e-8).all(), (g, r.status, r.iters, r.relres)
+        ref = FrequencySweep(P).solve(systems[g], tol=1e-8, maxit=20000, precond="aux", precision="mixed")
+        err = (torch.linalg.vector_norm(r.x - ref.x, dim=0) / torch.linalg.vector_norm(ref.x, dim=0)).cpu().numpy()
+        assert err.max() <= 1e-5, (g, err)
+        alone = BatchSweep([P]).solve([systems[g]], tol=1e-8, maxit=20000, precond="aux", precision="mixed")[0]
+        assert torch.equal(alone.x, r.x), g

@@ -34,7 +34,7 @@ from scipy.sparse import csr_matrix
 from .assembly import CsrPlan, DeviceMesh
 from .connectivity import DeviceTetMesh
 
-__all__ = ["MeshBatch", "BatchSweep"]
+__all__ = ["MeshBatch", "BatchSweep", "grouped_layout"]
 
 
 class MeshBatch:
@@ -95,6 +95,33 @@ class MeshBatch:
         return csr_matrix((vals[sel], cols.astype(np.int32), new_ptr.astype(np.int32)), shape=(n, n))
 
 
+def grouped_layout(n_edges, n_tris, align: int = 256):
+    """Row layout of the grouped multi-mesh system.
+
+    The union of G meshes numbers its DOFs [edges | faces | edges + H | faces + H] over all meshes, with
+    mesh g's edges at [eo_g, eo_g + n_edges[g]) and faces at [to_g, to_g + n_tris[g]) (the offsets are
+    the running sums).  The grouped layout puts mesh g's DOF pairs (first kind at i, second kind at
+    i + h) at [hoff[g], hoff[g] + H_g) with H_g = n_edges[g] + n_tris[g] padded to a multiple of
+    ``align``, in mesh g's own order (its edges, then its faces).  Returns (hoff (G + 1,), perm) with
+    perm[u] the grouped row of union DOF u."""
+    ne_g = np.asarray(n_edges, dtype=np.int64)
+    nf_g = np.asarray(n_tris, dtype=np.int64)
+    Hg = ne_g + nf_g
+    Hp = (Hg + align - 1) // align * align
+    hoff = np.concatenate([[0], np.cumsum(Hp)]).astype(np.int64)
+    eo = np.concatenate([[0], np.cumsum(ne_g)])
+    to = np.concatenate([[0], np.cumsum(nf_g)])
+    ne, nf = int(eo[-1]), int(to[-1])
+    x = np.arange(ne + nf, dtype=np.int64)
+    is_e = x < ne
+    g_e = np.searchsorted(eo, x[is_e], side="right") - 1
+    g_f = np.searchsorted(to, x[~is_e] - ne, side="right") - 1
+    first = np.empty(ne + nf, dtype=np.int64)
+    first[is_e] = hoff[g_e] + (x[is_e] - eo[g_e])
+    first[~is_e] = hoff[g_f] + ne_g[g_f] + (x[~is_e] - ne - to[g_f])
+    return hoff, np.concatenate([first, first + hoff[-1]])
+
+
 class BatchSweep:
     """Sweeps of several problems (``problems.Problem``: mesh, materials, ports, PEC, Robin boundaries)
     solved together.  Assembly: one fused launch for all meshes (:class:`MeshBatch`).  Solve: one
@@ -114,29 +141,20 @@ class BatchSweep:
         del er, ur
         # grouped layout: mesh g's DOF pairs at [hoff[g], hoff[g] + H_g) of each half, padded to 256
         G = len(self.problems)
-        Hg = np.array([P.field.n_field // 2 for P in self.problems], dtype=np.int64)
-        Hp = (Hg + self.PAIR_ALIGN - 1) // self.PAIR_ALIGN * self.PAIR_ALIGN
-        self.hoff = np.concatenate([[0], np.cumsum(Hp)]).astype(np.int64)
-        self.Hg = Hg
+        b = self.batch
+        ne_g = np.diff(b.edge_off.astype(np.int64))
+        nf_g = np.diff(b.tri_off.astype(np.int64))
+        if not (np.array_equal(ne_g, [P.mesh.n_edges for P in self.problems])
+                and np.array_equal(nf_g, [P.mesh.n_tris for P in self.problems])):
+            raise RuntimeError("BatchSweep: the union's entity ranges do not match the meshes")
+        self.hoff, perm = grouped_layout(ne_g, nf_g, self.PAIR_ALIGN)
+        self.Hg = ne_g + nf_g
         self.h = int(self.hoff[-1])
         self.n = 2 * self.h
+        Hp = np.diff(self.hoff)
         self.pair_group = torch.from_numpy(np.repeat(np.arange(G, dtype=np.int32), Hp)).to(dev)
-        # union DOF -> grouped DOF
-        b = self.batch
-        ne, nf = b.dmesh.n_edges, b.dmesh.n_tris
-        Hu = ne + nf
-        eo, to = b.edge_off.astype(np.int64), b.tri_off.astype(np.int64)
-        ne_g = np.diff(eo)
-        x = np.arange(Hu, dtype=np.int64)
-        is_e = x < ne
-        g_e = np.searchsorted(eo, x[is_e], side="right") - 1
-        g_f = np.searchsorted(to, x[~is_e] - ne, side="right") - 1
-        first = np.empty(Hu, dtype=np.int64)
-        first[is_e] = self.hoff[g_e] + (x[is_e] - eo[g_e])
-        first[~is_e] = self.hoff[g_f] + ne_g[g_f] + (x[~is_e] - ne - to[g_f])
-        perm = np.concatenate([first, first + self.h])              # union DOF u -> grouped row
         inv = np.full(self.n, -1, dtype=np.int64)
-        inv[perm] = np.arange(2 * Hu)
+        inv[perm] = np.arange(perm.size)
         # grouped CSR: rows moved, columns relabelled (their order inside a row is kept)
         indptr_u = b.plan.indptr.to(torch.int64)
         lens_u = indptr_u[1:] - indptr_u[:-1]

@@ -62,6 +62,9 @@ _SIGS = {
     "emfem_ned2_tri_robin": ([_vp, _i64, _vp, _i64, _vp, _dbl, _dbl, _vp, _vp, _i32, _vp, _vp], _i32),
     "emfem_segmented_gather_sum": ([_vp, _i64, _vp, _vp, _vp, _vp], _i32),
     "emfem_sweep_combine": ([_vp, _i64, _vp, _vp, _dbl, _i64, _vp, _vp, _dbl, _dbl, _vp], _i32),
+    "emfem_csr_drop_zeros_workspace": ([_i64, ctypes.POINTER(ctypes.c_size_t)], _i32),
+    "emfem_csr_count_nonzero": ([_vp, _i64, _vp, _vp, _vp, _vp, ctypes.c_size_t, ctypes.POINTER(_i64)], _i32),
+    "emfem_csr_compact_nonzero": ([_vp, _i64, _vp, _vp, _vp, _vp, _vp, _vp], _i32),
     "emfem_krylov_workspace_size": ([_i64, _i64, _i32, _i32, ctypes.POINTER(ctypes.c_size_t)], _i32),
     "emfem_krylov_solve": ([_vp, _i32, _i64, _i64, _vp, _vp, _vp, _vp, _i32, _dblp,
                           _i64, _vp, _vp, _vp, _vp, _vp, _i32, _dblp, _vp, _vp, _vp,

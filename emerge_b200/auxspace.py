@@ -194,6 +194,11 @@ class Network:
                                torch.empty(s.value, dtype=torch.float32, device=self.aux.device))}
         return self._ws[nsys]
 
+    def active(self) -> bool:
+        """False when the output weights are all zero: the network is then exactly the skip term, i.e.
+        the aux-space Jacobi, and the solvers apply that instead of running the layers."""
+        return bool(self.params[-2 * CHANNELS:].abs().max().item() > 0)
+
     def forward(self, x: torch.Tensor) -> torch.Tensor:
         """za = N(x) for x (n_aux, nsys) complex64; keeps the activations for backward."""
         x = x.to(torch.complex64).contiguous()

@@ -259,7 +259,10 @@ class BatchSweep:
         it = (ctypes.c_int * (G * nsys))()
         rr = (ctypes.c_double * (G * nsys))()
         aux = None
-        if PRECOND[precond] >= 3:
+        pc = PRECOND[precond]
+        if pc == 4 and not self.network.active():
+            pc = PRECOND["aux"]                # zero output weights: the aux Jacobi exactly, no layers to run
+        if pc >= 3:
             a = self.aux_space()
             a.reserve(nsys)
             aux = a.handle
@@ -270,7 +273,7 @@ class BatchSweep:
             ptr(self.pair_group), nsys, (ctypes.c_double * (G * nsys))(*k0), self.patch_rows.numel(),
             ptr(self.patch_rows), ptr(self.patch_rowptr), ptr(self.patch_cols), ptr(self.patch_vals),
             ptr(self.patch_port), self.n_ports, (ctypes.c_double * len(ga))(*ga), ptr(self.mask), ptr(b), ptr(x),
-            tol, maxit, PRECOND[precond], prec, ptr(self._ws), self._ws.numel(), st, it, rr, aux)
+            tol, maxit, pc, prec, ptr(self._ws), self._ws.numel(), st, it, rr, aux)
         torch.cuda.synchronize(self.device)
         dt = time.perf_counter() - t0
         if rc not in (0, ERR_NOT_CONVERGED):

@@ -1326,28 +1326,62 @@ namespace emfem {
 static __device__ __align__(256) int g_noalloc_patch_map[EMFEM_NOALLOC_MAX_ROWS];
 
 constexpr int NOALLOC_MAX_DEVICES = 64;
-static int* g_noalloc_addr[NOALLOC_MAX_DEVICES] = {nullptr};
+struct NoallocSlot {
+    int* addr = nullptr;
+    unsigned long long ctx_id = 0;     // the context the address was resolved in (0 = unknown)
+};
+static NoallocSlot g_noalloc[NOALLOC_MAX_DEVICES];
 static std::mutex g_noalloc_mutex;
 
-// Device address of the static map on `device` (which must be current).  Resolved once per device
-// with cudaGetSymbolAddress: host code only holds a host-side stand-in for the symbol, which must
-// never be passed to a kernel.
+// The current context's unique id through the driver's cuCtxGetCurrent / cuCtxGetId, looked up at run
+// time (the library links only the CUDA runtime).  0 when no context is current or the lookup failed.
+static unsigned long long current_ctx_id() {
+    typedef int (*GetCurrentFn)(void** ctx);
+    typedef int (*GetIdFn)(void* ctx, unsigned long long* id);
+    static GetCurrentFn get_current = nullptr;
+    static GetIdFn get_id = nullptr;
+    static bool looked_up = false;
+    if (!looked_up) {
+        looked_up = true;
+        cudaDriverEntryPointQueryResult q1, q2;
+        if (cudaGetDriverEntryPointByVersion("cuCtxGetCurrent", (void**)&get_current, 12000, cudaEnableDefault, &q1) !=
+                cudaSuccess || q1 != cudaDriverEntryPointSuccess)
+            get_current = nullptr;
+        if (cudaGetDriverEntryPointByVersion("cuCtxGetId", (void**)&get_id, 12000, cudaEnableDefault, &q2) !=
+                cudaSuccess || q2 != cudaDriverEntryPointSuccess)
+            get_id = nullptr;
+    }
+    if (!get_current || !get_id) return 0;
+    void* ctx = nullptr;
+    unsigned long long id = 0;
+    if (get_current(&ctx) != 0 || ctx == nullptr) return 0;
+    if (get_id(ctx, &id) != 0) return 0;
+    return id;
+}
+
+// Device address of the static map on `device` (which must be current).  Resolved with
+// cudaGetSymbolAddress once per device and context: host code only holds a host-side stand-in for the
+// symbol, which must never be passed to a kernel.  A new context on the device (after cudaDeviceReset,
+// the module is loaded again and the array may move) is seen by its id and resolves the address anew.
 static int noalloc_scratch(int device, int** out) {
     if (device < 0 || device >= NOALLOC_MAX_DEVICES) {
         set_error("emfem_sweep_spmv_noalloc: device %d beyond the supported %d", device, NOALLOC_MAX_DEVICES);
         return EMFEM_ERR_INVALID_ARG;
     }
     std::lock_guard<std::mutex> lock(g_noalloc_mutex);
-    if (g_noalloc_addr[device] == nullptr) {
+    NoallocSlot& slot = g_noalloc[device];
+    unsigned long long ctx = current_ctx_id();
+    if (slot.addr == nullptr || ctx == 0 || ctx != slot.ctx_id) {
         int* p = nullptr;
         cudaError_t e = cudaGetSymbolAddress((void**)&p, g_noalloc_patch_map);
         if (e != cudaSuccess) {
             set_error("emfem_sweep_spmv_noalloc: cudaGetSymbolAddress: %s", cudaGetErrorString(e));
             return EMFEM_ERR_CUDA;
         }
-        g_noalloc_addr[device] = p;
+        slot.addr = p;
+        slot.ctx_id = current_ctx_id();     // the lookup above made the device's context current
     }
-    *out = g_noalloc_addr[device];
+    *out = slot.addr;
     return EMFEM_OK;
 }
 }  // namespace emfem

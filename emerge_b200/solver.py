@@ -2,7 +2,8 @@
 
 * :class:`SolveReport`, :class:`SimulationError`, :class:`Solver` mirror ``solver.py:92-185``,
   ``:295`` and ``:333-371`` (same attributes, method names and return types);
-* :class:`SolverB200COCG` is a ``Solver`` that runs the batched device COCG of libemfem.  It plugs
+* :class:`SolverB200Krylov` is a ``Solver`` that runs the batched device Krylov solver of libemfem
+  (BiCGStab by default, COCG on request; ``SolverB200COCG`` is the same class under its earlier name).  It plugs
   into the reference through ``Simulation.set_solver(instance)`` (``E/simmodel.py:726-734`` →
   ``SolveRoutine.set_solver`` ``solver.py:1079-1090``), as ``SolverCuDSS`` (``:738-773``) does;
 * :class:`SolveRoutine` mirrors ``SolveRoutine.solve`` (``:1241-1326``): PEC elimination by
@@ -88,7 +89,7 @@ class Solver:
         pass
 
 
-class SolverB200COCG(Solver):
+class SolverB200Krylov(Solver):
     """Device Krylov solver (BiCGStab by default, COCG on request), block Jacobi on DOF pairs (i, i+n/2).
 
     The reference's K is not complex-symmetric (its face-face mass block is asymmetric,
@@ -114,8 +115,8 @@ class SolverB200COCG(Solver):
         self.raise_on_fail = raise_on_fail
         self._cache = None
 
-    def duplicate(self) -> "SolverB200COCG":
-        return SolverB200COCG(self.pre, self.tol, self.maxit, self.precond, self.precision, self.device,
+    def duplicate(self) -> "SolverB200Krylov":
+        return SolverB200Krylov(self.pre, self.tol, self.maxit, self.precond, self.precision, self.device,
                               self.raise_on_fail, self.method)
 
     def reset(self) -> None:
@@ -127,7 +128,7 @@ class SolverB200COCG(Solver):
         A.sort_indices()
         n = A.shape[0]
         if n % 2:
-            raise SimulationError("SolverB200COCG needs the Nedelec-2 DOF pairing (an even number of DOFs)")
+            raise SimulationError("SolverB200Krylov needs the Nedelec-2 DOF pairing (an even number of DOFs)")
         self._cache = dict(
             dev=dev, n=n, nnz=A.nnz,
             indptr=torch.from_numpy(A.indptr.astype(np.int32)).to(dev),
@@ -170,7 +171,7 @@ class SolverB200COCG(Solver):
         simtime = time.perf_counter() - t0
         ok = all(s == 0 for s, _, _ in reports)
         if not ok and self.raise_on_fail:
-            raise SimulationError(f"SolverB200COCG did not converge: {reports}")
+            raise SimulationError(f"SolverB200Krylov did not converge: {reports}")
         rep = SolveReport(solver=str(self), exit_code=0 if ok else 1, simtime=simtime, precon=self.precond,
                           aux={"iterations": str([r[1] for r in reports]),
                                "true relative residual": str([f"{r[2]:.3e}" for r in reports]),
@@ -178,12 +179,17 @@ class SolverB200COCG(Solver):
         return (out if multi else out[:, 0]), rep
 
 
+# earlier name of the class (it runs BiCGStab unless method="cocg")
+SolverB200COCG = SolverB200Krylov
+
+
 class SolveRoutine:
-    """``SolveRoutine.solve`` (``solver.py:1241-1326``) with a pluggable solver (default: device COCG)."""
+    """``SolveRoutine.solve`` (``solver.py:1241-1326``) with a pluggable solver (default: the device
+    Krylov solver)."""
 
     def __init__(self, solver: Solver | None = None):
         self.forced_solver = [solver] if solver is not None else []
-        self.default = SolverB200COCG()
+        self.default = SolverB200Krylov()
         self.pre = ""
 
     def set_solver(self, *solvers: Solver) -> None:

@@ -103,6 +103,7 @@ class FrequencySweep:
         self._ws = None
         self._aux = None
         self.network = None
+        self._learned_active = False
 
     @classmethod
     def port_terms(cls, problem, device=None) -> "FrequencySweep":
@@ -123,6 +124,7 @@ class FrequencySweep:
         fs._ws = None
         fs._aux = None
         fs.network = None
+        fs._learned_active = False
         return fs
 
     def aux_space(self):
@@ -134,8 +136,11 @@ class FrequencySweep:
         return self._aux
 
     def set_network(self, net) -> None:
-        """Use this trained :class:`auxspace.Network` for ``precond="learned"``."""
+        """Use this trained :class:`auxspace.Network` for ``precond="learned"``.  A network whose output
+        weights are zero (validation rejected the learned term) is the aux-space Jacobi exactly, and
+        ``precond="learned"`` then runs that without the network's layers."""
         self.network = net
+        self._learned_active = net is not None and net.active()
         self.aux_space().set_network(net.params if net is not None else None)
 
     def assemble(self):
@@ -454,9 +459,12 @@ class FrequencySweep:
         k0a = (ctypes.c_double * nsys)(*k0)
         ga = (ctypes.c_double * len(gam))(*gam)
         aux = None
-        if PRECOND[precond] >= 3:
+        pc = PRECOND[precond]
+        if pc >= 3:
             if precond == "learned" and self.network is None:
                 raise ValueError("precond='learned' needs a trained network (FrequencySweep.set_network)")
+            if pc == 4 and not self._learned_active:
+                pc = PRECOND["aux"]            # zero output weights: the same operator, no layers to run
             a = self.aux_space()
             a.reserve(nsys)
             aux = a.handle
@@ -466,7 +474,7 @@ class FrequencySweep:
                                     ptr(self.E), ptr(self.B), nsys, k0a,
                                     self.patch_rows.numel(), ptr(self.patch_rows), ptr(self.patch_rowptr),
                                     ptr(self.patch_cols), ptr(self.patch_vals), ptr(self.patch_port), self.n_ports, ga,
-                                    ptr(self.mask), ptr(b), ptr(x), tol, maxit, PRECOND[precond], prec,
+                                    ptr(self.mask), ptr(b), ptr(x), tol, maxit, pc, prec,
                                     ptr(ws), ws.numel(), status, iters, relres, aux)
         dt = time.perf_counter() - t0
         if st not in (0, ERR_NOT_CONVERGED) or (raise_on_fail and st != 0):

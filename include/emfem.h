@@ -128,11 +128,24 @@ int emfem_segmented_gather_sum(emfem_handle h, int64_t n_out, const int32_t *seg
                                const void *src, void *out);
 
 /* ---- frequency-sweep system ------------------------------------------------------------------
- * K = (E - k0^2 B) on the plan pattern, then K[patch_slot[i]] += gamma * patch_vals[i]
- * (ASM/assembler.py:255 and :349-350).  Device arrays; nnz complex each. */
+ * K = (E - k0^2 B) on the plan pattern (the product rounded first, as the reference's E - B*K0**2),
+ * then K[patch_slot[i]] += gamma * patch_vals[i] (ASM/assembler.py:255 and :349-350).  The slots of one
+ * call must be distinct (sum duplicates first, e.g. with emfem_segmented_gather_sum).  Device arrays;
+ * nnz complex each. */
 int emfem_sweep_combine(emfem_handle h, int64_t nnz, const void *E_vals, const void *B_vals, double k0sq,
                         int64_t n_patch, const int32_t *patch_slot, const void *patch_vals,
                         double gamma_re, double gamma_im, void *K_vals);
+
+/* Exact zeros dropped from a CSR matrix, the other entries kept in order: the layout SciPy gives the
+ * result of E - B*K0**2 and K + B_p (ASM/assembler.py:255, :350), whose sparse arithmetic stores only
+ * nonzero results.  count: out_indptr (n + 1) i32 gets the compacted row pointers and *nnz_out (host)
+ * the kept count (synchronises the stream); workspace (device) holds emfem_csr_drop_zeros_workspace()
+ * bytes.  compact: out_indices (nnz_out) i32 and out_vals (nnz_out) c128.  Device arrays. */
+int emfem_csr_drop_zeros_workspace(int64_t n, size_t *bytes);
+int emfem_csr_count_nonzero(emfem_handle h, int64_t n, const int32_t *indptr, const void *vals, int32_t *out_indptr,
+                            void *workspace, size_t workspace_bytes, int64_t *nnz_out);
+int emfem_csr_compact_nonzero(emfem_handle h, int64_t n, const int32_t *indptr, const int32_t *indices,
+                              const void *vals, const int32_t *out_indptr, int32_t *out_indices, void *out_vals);
 
 /* ---- batched Krylov solver ------------------------------------------------------------------
  * Solves nsys systems A_s x_s = b_s on one CSR pattern, replacing the per-frequency direct solve
@@ -352,7 +365,8 @@ int emfem_adam_step(emfem_handle h, int64_t n, float *params, const float *grad,
  * fixed device array of EMFEM_NOALLOC_MAX_ROWS ints (16 MiB) inside the library, held by every GPU
  * that loads the library until the process exits; larger n is rejected with EMFEM_ERR_INVALID_ARG.
  * It calls no cudaMalloc/cudaFree.  The first call on a device resolves the array's device address
- * (cudaGetSymbolAddress) once; make that first call before any stream capture.  All calls share the
+ * (cudaGetSymbolAddress) once per context (a new context after cudaDeviceReset resolves it again);
+ * make that first call before any stream capture.  All calls share the
  * array (each call resets the rows it uses), so calls that overlap on the GPU race.  Arguments as
  * emfem_sweep_spmv. */
 #define EMFEM_NOALLOC_MAX_ROWS 4194304

@@ -1,7 +1,7 @@
 """Generate the golden fixtures in this folder by running EMerge's own numba code.
 
-Run in a container that has the reference checkout (``EMERGE_REFERENCE_SRC``, default the
-``src/emerge`` of the read-only checkout); the GPU box never runs this file, it only reads the
+Run in a container that has the reference checkout, with ``EMERGE_REFERENCE_SRC`` set to its
+``src/emerge`` folder (required); the GPU box never runs this file, it only reads the
 ``.npz`` files it wrote.  First numba compile takes about a minute.
 
     python tests/golden/make_golden.py

@@ -12,10 +12,17 @@ import os
 import sys
 import types
 
-REFERENCE_SRC = os.environ.get("EMERGE_REFERENCE_SRC", "/root/reference/src/emerge")
+def _reference_src() -> str:
+    src = os.environ.get("EMERGE_REFERENCE_SRC")
+    if not src:
+        raise RuntimeError("set EMERGE_REFERENCE_SRC to the src/emerge folder of an EMerge checkout")
+    if not os.path.isdir(src):
+        raise RuntimeError(f"EMERGE_REFERENCE_SRC={src!r} is not a folder")
+    return src
 
 
 def load():
+    reference_src = _reference_src()
     os.environ.setdefault("NUMBA_CACHE_DIR", "/tmp/emerge_b200_numba_cache")
     if "emerge" in sys.modules and getattr(sys.modules["emerge"], "_stubbed", False):
         return _modules()
@@ -32,7 +39,7 @@ def load():
     emd = types.ModuleType("emsutil.emdata"); emd.EHField = object; emd.EHFieldFF = object
     sys.modules.update({"emsutil": ems, "emsutil.lib": lib, "emsutil.emdata": emd})
     pkg = types.ModuleType("emerge")
-    pkg.__path__ = [REFERENCE_SRC]
+    pkg.__path__ = [reference_src]
     pkg._stubbed = True
     sys.modules["emerge"] = pkg
     return _modules()

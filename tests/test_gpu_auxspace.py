@@ -158,12 +158,22 @@ def test_training_reduces_correction_loss_and_learned_solve_converges(guide, gol
     for j, key in enumerate(("x1", "x2")):
         gx = g[key]
         assert np.linalg.norm(x[:, j] - gx) / np.linalg.norm(gx) <= 1e-8
-    # what the trained preconditioner gains over the method without it (plain block Jacobi) at a
-    # frequency outside the training set: the same systems to 1e-8 in a fraction of the iterations
+    # what the trained network gains over the method without it: the aux-space Jacobi (the same
+    # preconditioner with the network's output weights at zero), on systems outside the training and
+    # validation sets.  Validation only keeps a learned term that beat the aux Jacobi; when it rejected
+    # the term, precond="learned" is the aux Jacobi exactly and the gain is zero.
     held_sys = [(10.5e9, 0), (10.5e9, 1)]
-    plain = sw.solve(held_sys, tol=1e-8, maxit=40000, precond="block_jacobi")
+    aux_j = sw.solve(held_sys, tol=1e-8, maxit=40000, precond="aux")
     learned = sw.solve(held_sys, tol=1e-8, maxit=40000, precond="learned", fallback=True)
-    assert (plain.status == 0).all() and (learned.status == 0).all()
+    assert (aux_j.status == 0).all() and (learned.status == 0).all()
     assert learned.fallbacks == 0
-    assert learned.iters.max() * 4 < plain.iters.max(), (learned.iters, plain.iters)
+    if rep.accepted:
+        assert learned.iters.sum() <= 1.25 * aux_j.iters.sum(), (learned.iters, aux_j.iters)
+    else:
+        assert (learned.iters == aux_j.iters).all(), (learned.iters, aux_j.iters)
+        assert torch.equal(learned.x, aux_j.x)
+    # and both far below plain block Jacobi: the aux-space structure, not the network, carries that
+    plain = sw.solve(held_sys, tol=1e-8, maxit=40000, precond="block_jacobi")
+    assert (plain.status == 0).all()
+    assert aux_j.iters.max() * 4 < plain.iters.max(), (aux_j.iters, plain.iters)
     sw.set_network(None)

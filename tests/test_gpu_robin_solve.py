@@ -9,7 +9,7 @@ from emerge_b200.assembler import Assembler
 from emerge_b200.mesh import TetMesh
 from emerge_b200.nedelec2 import Nedelec2
 from emerge_b200.ports import PortFrame, RectangularWaveguidePort, k0_of
-from emerge_b200.solver import SolveRoutine, SolverB200COCG
+from emerge_b200.solver import SolveRoutine, SolverB200COCG, SolverB200Krylov
 from emerge_b200.sweep import FrequencySweep
 
 pytestmark = pytest.mark.gpu
@@ -48,6 +48,32 @@ def test_freq_assembly_vs_reference_golden(cuda, golden):
     assert len(job.solve_ids) == int(g["n_solve"])
 
 
+def test_device_combine_matches_scipy_arithmetic(cuda):
+    """emfem_sweep_combine + the zero-dropping compaction against SciPy's E - B*K0**2 (+ generate_csr(Bempty))
+    on the same device-assembled E and B (ASM/assembler.py:255, :350): the same CSR layout, and without
+    boundary terms the same bits."""
+    from emerge_b200.assembler import freq_matrix_device
+    P = problems.waveguide()
+    sw = FrequencySweep(P)
+    k0 = k0_of(10e9)
+    Eh, Bh = sw.plan.to_scipy(sw.E), sw.plan.to_scipy(sw.B)
+    Kref = (Eh - Bh * (k0 ** 2)).tocsr()
+    assert Kref.nnz < Eh.nnz                      # the guide's E and B share exact zeros, which K drops
+    K = freq_matrix_device(sw.plan, sw.E, sw.B, k0 ** 2)
+    assert np.array_equal(K.indptr, Kref.indptr) and np.array_equal(K.indices, Kref.indices)
+    assert np.array_equal(K.data, Kref.data)
+    # with the ports' Robin blocks: the drop-in Assembler against the same steps in SciPy
+    job = Assembler().assemble_freq_matrix(P.field, P.er, P.ur, P.ports, P.pec_tris, 10e9)
+    Bm = P.field.empty_tri_matrix()
+    dpts = assembly.dunavant4()
+    for p in P.ports:
+        Bm, _ = assembly.assemble_robin_bc_excited(P.field, Bm, p.tri_ids,
+                                                   lambda x, y, z, p=p: p.get_Uinc(x, y, z, k0), p.get_gamma(k0), dpts)
+    Kp = (Kref + P.field.generate_csr(Bm)).tocsr()
+    assert np.array_equal(job.A.indptr, Kp.indptr) and np.array_equal(job.A.indices, Kp.indices)
+    assert np.abs(job.A.data - Kp.data).max() <= 1e-15 * np.abs(Kp.data).max()
+
+
 def test_sweep_solve_matches_superlu_golden(cuda, golden):
     """Device COCG (FP64, block Jacobi) on the 6 000-tet guide vs the reference's SuperLU solution."""
     g = golden("config1")
@@ -80,7 +106,8 @@ def test_solver_plugin_through_solve_routine(cuda, golden):
     g = golden("config1")
     P = problems.waveguide()
     job = Assembler().assemble_freq_matrix(P.field, P.er, P.ur, P.ports, P.pec_tris, float(g["f"]))
-    routine = SolveRoutine(SolverB200COCG(tol=1e-12, maxit=60000))
+    assert SolverB200COCG is SolverB200Krylov
+    routine = SolveRoutine(SolverB200Krylov(tol=1e-12, maxit=60000))
     for (A, b, ids, reuse, aux), key in zip(job.iter_Ab(), ("x1", "x2")):
         x, rep = routine.solve(A, b, ids, reuse=reuse)
         assert rep.exit_code == 0, rep.aux

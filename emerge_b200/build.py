@@ -15,7 +15,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libemfem.so")
-SOURCES = ["emfem_core.cu", "ned2_tet.cu", "robin.cu", "sweep_solve.cu", "sparam.cu", "mesh_conn.cu", "aux_space.cu", "bma.cu", "freq_csr.cu"]
+SOURCES = ["emfem_core.cu", "ned2_tet.cu", "robin.cu", "sweep_solve.cu", "sparam.cu", "mesh_conn.cu", "aux_space.cu", "bma.cu", "freq_csr.cu", "multifrontal.cu"]
 HEADERS = ["emfem_internal.cuh", "ned2_math.cuh"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 

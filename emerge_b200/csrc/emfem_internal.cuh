@@ -110,3 +110,10 @@ int aux_setup_dinv(const emfem_aux_s* a, int S, int nsys, const double* k0sq, co
 size_t aux_solve_bytes(const emfem_aux_s* a, int S);
 void* aux_dinv_buffer(const emfem_aux_s* a, int S);
 }  // namespace emfem
+
+// Multifrontal LU (multifrontal.cu); the Krylov solver applies it as a right preconditioner.
+struct emfem_mf_s;
+namespace emfem {
+int mf_apply(emfem_mf_s* m, int S, const double2* r, double2* x, cudaStream_t s);
+int mf_reserved(const emfem_mf_s* m);
+}  // namespace emfem

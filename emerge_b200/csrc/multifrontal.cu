@@ -1,0 +1,953 @@
+// Multifrontal sparse LU of the sweep system on the device (complex64 fronts), the direct solve that
+// replaces the reference's SolverSuperLU (src/emerge/_emerge/solver.py:535-572).
+//
+// The symbolic structure (nested-dissection tree, front DOF lists, extend-add maps, assembly lists) is
+// built on the host (emerge_b200/direct.py) and uploaded once per mesh.  The numeric factorization runs
+// level by level over the tree (all fronts of one height at once):
+//   1. every front of the level is zeroed and gets its own entries of K (FP64 -> FP32) and the Schur
+//      complements of its children (extend-add, one child slot after the other: no atomics);
+//   2. the first e columns of every front are eliminated in steps of 32: LU with partial pivoting inside
+//      the 32 x 32 diagonal block (diag_kernel, one warp per front, also forming the explicit inverses
+//      of its L and U), the block row (row swaps + L^-1) and block column (U^-1) of the panel
+//      (panel_kernel), and the rank-32 update of the trailing matrix (trail_kernel: 64 x 64 tiles,
+//      4 x 4 complex register tiles per thread), every kernel batched over the level's fronts;
+//   3. the factor columns, the U block row and the Schur complement are copied out of the level
+//      workspace (compact_kernel): factors to the factor store, the Schur complement to the update store
+//      until the parent's level consumes it.
+// Pivoting stays inside each 32-row diagonal block (rows are never exchanged across blocks), so row swaps
+// touch only the block row; the solves apply them step by step.  A pivot smaller than 1e-6 of its block's
+// largest entry is raised to that floor and counted: the factorization is a preconditioner under an FP64
+// Krylov iteration, which removes such perturbations.
+//
+// Solves (M^-1 r for S right-hand sides, FP64 in and out, FP32 inside) run the same tree: forward in
+// level order (gather, children's update vectors, blocked L solve with 256-row blocks, update vector for
+// the parent), backward in reverse (gather of the solved boundary, U12 product, blocked U solve).
+#include "emfem_internal.cuh"
+
+#include <algorithm>
+#include <map>
+#include <vector>
+
+namespace emfem {
+
+constexpr int MF_NB = 32;          // pivot block / elimination step
+constexpr int MF_SB = 256;         // solve block
+constexpr int MF_TILE = 64;        // trailing-update tile
+constexpr long long MF_CHUNK = 4096;
+constexpr int MF_MAX_FRONT = 46340; // n^2 must fit an int32 local offset
+
+__device__ __forceinline__ float2 cmul(float2 a, float2 b) {
+    return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__device__ __forceinline__ void cfma(float2& c, float2 a, float2 b) {
+    c.x = fmaf(a.x, b.x, fmaf(-a.y, b.y, c.x));
+    c.y = fmaf(a.x, b.y, fmaf(a.y, b.x, c.y));
+}
+__device__ __forceinline__ void cfms(float2& c, float2 a, float2 b) {   // c -= a b
+    c.x = fmaf(-a.x, b.x, fmaf(a.y, b.y, c.x));
+    c.y = fmaf(-a.x, b.y, fmaf(-a.y, b.x, c.y));
+}
+__device__ __forceinline__ float cabs2(float2 a) { return a.x * a.x + a.y * a.y; }
+__device__ __forceinline__ float2 cinv(float2 a) {
+    float d = 1.0f / cabs2(a);
+    return make_float2(a.x * d, -a.y * d);
+}
+
+struct FrontMeta {        // per front, device
+    int e, b, n, parent;
+    int child[2];
+    long long fdof, ea, asm0, asm1;   // offsets into fdof / ea / asm arrays
+    long long fact, inv, piv;         // factor store offsets (float2 / float2 / int)
+    long long ws, upd;                // level workspace (float2) / update store (float2) offsets
+    long long wv, uv, y;              // solve buffers: level w (rows), update vectors (rows), own solution (rows)
+};
+
+// ---------------------------------------------------------------- factorization kernels
+__global__ void mf_asm_kernel(const int* __restrict__ lst, const FrontMeta* __restrict__ fm,
+                              const double2* __restrict__ K, const int* __restrict__ slot, const int* __restrict__ off,
+                              float2* __restrict__ ws) {
+    const FrontMeta& f = fm[lst[blockIdx.y]];
+    long long k0 = f.asm0 + (long long)blockIdx.x * MF_CHUNK;
+    long long k1 = min(k0 + MF_CHUNK, f.asm1);
+    float2* W = ws + f.ws;
+    for (long long k = k0 + threadIdx.x; k < k1; k += blockDim.x) {
+        double2 v = K[slot[k]];
+        W[off[k]] = make_float2((float)v.x, (float)v.y);
+    }
+}
+
+__global__ void mf_ea_kernel(const int* __restrict__ lst, const FrontMeta* __restrict__ fm, int cslot,
+                             const int* __restrict__ ea, const float2* __restrict__ upd, float2* __restrict__ ws) {
+    const FrontMeta& f = fm[lst[blockIdx.y]];
+    int c = f.child[cslot];
+    if (c < 0) return;
+    const FrontMeta& g = fm[c];
+    long long nb = g.b;
+    long long tot = nb * nb;
+    long long i0 = (long long)blockIdx.x * MF_CHUNK;
+    if (i0 >= tot) return;
+    long long i1 = min(i0 + MF_CHUNK, tot);
+    const int* map = ea + g.ea;
+    const float2* U = upd + g.upd;
+    float2* W = ws + f.ws;
+    long long ld = f.n;
+    for (long long idx = i0 + threadIdx.x; idx < i1; idx += blockDim.x) {
+        long long i = idx % nb, j = idx / nb;
+        float2 u = U[idx];
+        float2* dst = W + map[i] + (long long)map[j] * ld;
+        dst->x += u.x;
+        dst->y += u.y;
+    }
+}
+
+// LU with partial pivoting of the 32 x 32 diagonal block at step k, plus the explicit inverses of its
+// unit-lower L and upper U.  One warp per front; lane = column (or row in the pivot search).
+__global__ void __launch_bounds__(32) mf_diag_kernel(const int* __restrict__ lst, const FrontMeta* __restrict__ fm, int k,
+                                                     float2* __restrict__ ws, float2* __restrict__ inv,
+                                                     int* __restrict__ piv, int* __restrict__ nperturbed) {
+    __shared__ float2 D[MF_NB][MF_NB + 1];
+    __shared__ float2 X[MF_NB][MF_NB + 1];
+    const FrontMeta& f = fm[lst[blockIdx.x]];
+    if (k >= f.e) return;
+    const int kb = min(MF_NB, f.e - k);
+    const int lane = threadIdx.x;
+    const long long ld = f.n;
+    float2* W = ws + f.ws + k + (long long)k * ld;
+    float bmax = 0.0f;
+    for (int c = 0; c < kb; c++) {
+        float2 v = lane < kb ? W[lane + (long long)c * ld] : make_float2(0.f, 0.f);
+        D[lane][c] = v;
+        bmax = fmaxf(bmax, cabs2(v));
+    }
+    for (int o = 16; o > 0; o >>= 1) bmax = fmaxf(bmax, __shfl_xor_sync(0xffffffffu, bmax, o));
+    const float floor2 = fmaxf(bmax, 1e-30f) * 1e-12f;      // (1e-6 of the block's largest entry)^2
+    __syncwarp();
+    int* P = piv + f.piv + k;
+    int pert = 0;
+    for (int j = 0; j < kb; j++) {
+        // pivot: largest |D[r][j]| for r >= j (ties: smallest r)
+        float best = (lane >= j && lane < kb) ? cabs2(D[lane][j]) : -1.0f;
+        int br = lane;
+        for (int o = 16; o > 0; o >>= 1) {
+            float ob = __shfl_xor_sync(0xffffffffu, best, o);
+            int orr = __shfl_xor_sync(0xffffffffu, br, o);
+            if (ob > best || (ob == best && orr < br)) { best = ob; br = orr; }
+        }
+        if (lane == 0) P[j] = br;
+        if (br != j && lane < kb) {
+            float2 t = D[j][lane];
+            D[j][lane] = D[br][lane];
+            D[br][lane] = t;
+        }
+        __syncwarp();
+        if (lane == 0 && cabs2(D[j][j]) < floor2) {
+            float2 d = D[j][j];
+            float a = sqrtf(cabs2(d));
+            float fl = sqrtf(floor2);
+            D[j][j] = a > 0.f ? make_float2(d.x / a * fl, d.y / a * fl) : make_float2(fl, 0.f);
+            pert++;
+        }
+        __syncwarp();
+        float2 pinv = cinv(D[j][j]);
+        if (lane > j && lane < kb) D[lane][j] = cmul(D[lane][j], pinv);
+        __syncwarp();
+        if (lane > j && lane < kb) {
+            float2 u = D[j][lane];
+            for (int r = j + 1; r < kb; r++) cfms(D[r][lane], D[r][j], u);
+        }
+        __syncwarp();
+    }
+    if (lane == 0 && pert) atomicAdd(nperturbed, pert);
+    // write L\U back
+    for (int c = 0; c < kb; c++)
+        if (lane < kb) W[lane + (long long)c * ld] = D[lane][c];
+    float2* Li = inv + f.inv + (long long)(k / MF_NB) * 2 * MF_NB * MF_NB;   // Linv then Uinv, column-major 32x32
+    float2* Ui = Li + MF_NB * MF_NB;
+    // Uinv: lane = column c of X = U^-1 (back substitution, own column only)
+    {
+        int c = lane;
+        for (int i = 0; i < MF_NB; i++) X[i][c] = make_float2(0.f, 0.f);
+        if (c < kb) {
+            X[c][c] = cinv(D[c][c]);
+            for (int i = c - 1; i >= 0; i--) {
+                float2 s = make_float2(0.f, 0.f);
+                for (int t = i + 1; t <= c; t++) cfma(s, D[i][t], X[t][c]);
+                float2 q = cmul(s, cinv(D[i][i]));
+                X[i][c] = make_float2(-q.x, -q.y);
+            }
+        }
+    }
+    __syncwarp();
+    for (int c = 0; c < MF_NB; c++) Ui[lane + c * MF_NB] = X[lane][c];
+    __syncwarp();
+    // Linv: lane = column c of Y = L^-1 (unit lower, forward substitution)
+    {
+        int c = lane;
+        for (int i = 0; i < MF_NB; i++) X[i][c] = make_float2(0.f, 0.f);
+        if (c < kb) {
+            X[c][c] = make_float2(1.f, 0.f);
+            for (int i = c + 1; i < kb; i++) {
+                float2 s = make_float2(0.f, 0.f);
+                for (int t = c; t < i; t++) cfma(s, D[i][t], X[t][c]);
+                X[i][c] = make_float2(-s.x, -s.y);
+            }
+        }
+    }
+    __syncwarp();
+    for (int c = 0; c < MF_NB; c++) Li[lane + c * MF_NB] = X[lane][c];
+}
+
+// Block row (columns >= k + kb): row swaps, then L^-1; block column (rows >= k + kb): times U^-1.
+// Items 0 .. m-1 are columns, m .. 2m-1 rows (m = n - k - kb).
+__global__ void __launch_bounds__(256) mf_panel_kernel(const int* __restrict__ lst, const FrontMeta* __restrict__ fm, int k,
+                                                       float2* __restrict__ ws, const float2* __restrict__ inv,
+                                                       const int* __restrict__ piv) {
+    __shared__ float2 Li[MF_NB * MF_NB];
+    __shared__ float2 Ui[MF_NB * MF_NB];
+    __shared__ int P[MF_NB];
+    const FrontMeta& f = fm[lst[blockIdx.y]];
+    if (k >= f.e) return;
+    const int kb = min(MF_NB, f.e - k);
+    const long long m = f.n - k - kb;
+    long long item = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if ((long long)blockIdx.x * blockDim.x >= 2 * m) return;
+    const float2* L = inv + f.inv + (long long)(k / MF_NB) * 2 * MF_NB * MF_NB;
+    for (int t = threadIdx.x; t < MF_NB * MF_NB; t += blockDim.x) { Li[t] = L[t]; Ui[t] = L[MF_NB * MF_NB + t]; }
+    if (threadIdx.x < MF_NB) P[threadIdx.x] = threadIdx.x < kb ? piv[f.piv + k + threadIdx.x] : threadIdx.x;
+    __syncthreads();
+    if (item >= 2 * m) return;
+    const long long ld = f.n;
+    float2* W = ws + f.ws;
+    float2 v[MF_NB];
+    if (item < m) {
+        long long c = k + kb + item;
+        float2* col = W + k + c * ld;
+        for (int j = 0; j < kb; j++) {           // this thread owns the column: swap in place
+            int r = P[j];
+            if (r != j) {
+                float2 t = col[j];
+                col[j] = col[r];
+                col[r] = t;
+            }
+        }
+#pragma unroll
+        for (int i = 0; i < MF_NB; i++) v[i] = i < kb ? col[i] : make_float2(0.f, 0.f);
+#pragma unroll
+        for (int i = 0; i < MF_NB; i++) {
+            if (i < kb) {
+                float2 s = make_float2(0.f, 0.f);
+#pragma unroll
+                for (int t = 0; t < MF_NB; t++) cfma(s, Li[i + t * MF_NB], v[t]);
+                col[i] = s;
+            }
+        }
+    } else {
+        long long r = k + kb + (item - m);
+        float2* row = W + r + (long long)k * ld;
+#pragma unroll
+        for (int i = 0; i < MF_NB; i++) v[i] = i < kb ? row[(long long)i * ld] : make_float2(0.f, 0.f);
+#pragma unroll
+        for (int c = 0; c < MF_NB; c++) {
+            if (c < kb) {
+                float2 s = make_float2(0.f, 0.f);
+#pragma unroll
+                for (int t = 0; t < MF_NB; t++) cfma(s, v[t], Ui[t + c * MF_NB]);
+                row[(long long)c * ld] = s;
+            }
+        }
+    }
+}
+
+// Trailing update C -= A B on 64 x 64 tiles: A = W[k+kb.., k..k+kb), B = W[k..k+kb, k+kb..).
+__global__ void __launch_bounds__(256) mf_trail_kernel(const int* __restrict__ lst, const FrontMeta* __restrict__ fm, int k,
+                                                       float2* __restrict__ ws) {
+    __shared__ float2 As[MF_NB][MF_TILE + 1];
+    __shared__ float2 Bs[MF_NB][MF_TILE + 1];
+    const FrontMeta& f = fm[lst[blockIdx.y]];
+    if (k >= f.e) return;
+    const int kb = min(MF_NB, f.e - k);
+    const long long m = f.n - k - kb;
+    const long long nt = (m + MF_TILE - 1) / MF_TILE;
+    if ((long long)blockIdx.x >= nt * nt) return;
+    const long long ti = blockIdx.x % nt, tj = blockIdx.x / nt;
+    const long long r0 = k + kb + ti * MF_TILE, c0 = k + kb + tj * MF_TILE;
+    const long long ld = f.n;
+    float2* W = ws + f.ws;
+    const int tid = threadIdx.x;
+    // A tile (64 rows x kb) and B tile (kb x 64 cols)
+    for (int t = tid; t < MF_NB * MF_TILE; t += 256) {
+        int rr = t % MF_TILE, kk = t / MF_TILE;
+        long long r = r0 + rr;
+        As[kk][rr] = (kk < kb && r < f.n) ? W[r + (long long)(k + kk) * ld] : make_float2(0.f, 0.f);
+        int kk2 = t % MF_NB, cc = t / MF_NB;
+        long long c = c0 + cc;
+        Bs[kk2][cc] = (kk2 < kb && c < f.n) ? W[(k + kk2) + c * ld] : make_float2(0.f, 0.f);
+    }
+    __syncthreads();
+    const int tx = tid % 16, ty = tid / 16;
+    float2 acc[4][4];
+#pragma unroll
+    for (int i = 0; i < 4; i++)
+#pragma unroll
+        for (int j = 0; j < 4; j++) acc[i][j] = make_float2(0.f, 0.f);
+    for (int kk = 0; kk < kb; kk++) {
+        float2 a[4], b[4];
+#pragma unroll
+        for (int i = 0; i < 4; i++) a[i] = As[kk][tx + 16 * i];
+#pragma unroll
+        for (int j = 0; j < 4; j++) b[j] = Bs[kk][ty + 16 * j];
+#pragma unroll
+        for (int i = 0; i < 4; i++)
+#pragma unroll
+            for (int j = 0; j < 4; j++) cfma(acc[i][j], a[i], b[j]);
+    }
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+        long long c = c0 + ty + 16 * j;
+        if (c >= f.n) continue;
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+            long long r = r0 + tx + 16 * i;
+            if (r >= f.n) continue;
+            float2* p = W + r + c * ld;
+            float2 v = *p;
+            v.x -= acc[i][j].x;
+            v.y -= acc[i][j].y;
+            *p = v;
+        }
+    }
+}
+
+// Factor columns (n x e), U block row (e x b) and Schur complement (b x b) out of the workspace.
+__global__ void mf_compact_kernel(const int* __restrict__ lst, const FrontMeta* __restrict__ fm,
+                                  const float2* __restrict__ ws, float2* __restrict__ fact, float2* __restrict__ upd) {
+    const FrontMeta& f = fm[lst[blockIdx.y]];
+    const long long n = f.n, e = f.e, b = f.b;
+    long long i0 = (long long)blockIdx.x * MF_CHUNK;
+    if (i0 >= n * n) return;
+    long long i1 = min(i0 + MF_CHUNK, n * n);
+    const float2* W = ws + f.ws;
+    float2* F = fact + f.fact;
+    float2* U = upd + f.upd;
+    for (long long idx = i0 + threadIdx.x; idx < i1; idx += blockDim.x) {
+        long long i = idx % n, j = idx / n;
+        float2 v = W[idx];
+        if (j < e) F[idx] = v;
+        else if (i < e) F[n * e + i + (j - e) * e] = v;
+        else U[(i - e) + (j - e) * b] = v;
+    }
+}
+
+// ---------------------------------------------------------------- solve kernels
+// w (rows of the level's fronts, S per row): own rows from the right-hand side, boundary rows zero
+__global__ void mf_fwd_gather_kernel(const int* __restrict__ lst, const FrontMeta* __restrict__ fm, int S,
+                                     const int* __restrict__ fdof, const double2* __restrict__ rhs, float2* __restrict__ w) {
+    const FrontMeta& f = fm[lst[blockIdx.y]];
+    long long tot = (long long)f.n * S;
+    long long i0 = (long long)blockIdx.x * MF_CHUNK;
+    if (i0 >= tot) return;
+    long long i1 = min(i0 + MF_CHUNK, tot);
+    float2* W = w + f.wv * S;
+    const int* d = fdof + f.fdof;
+    for (long long idx = i0 + threadIdx.x; idx < i1; idx += blockDim.x) {
+        long long i = idx / S;
+        int s = (int)(idx % S);
+        float2 v = make_float2(0.f, 0.f);
+        if (i < f.e) {
+            double2 r = rhs[(long long)d[i] * S + s];
+            v = make_float2((float)r.x, (float)r.y);
+        }
+        W[idx] = v;
+    }
+}
+
+__global__ void mf_fwd_ea_kernel(const int* __restrict__ lst, const FrontMeta* __restrict__ fm, int S, int cslot,
+                                 const int* __restrict__ ea, const float2* __restrict__ uvec, float2* __restrict__ w) {
+    const FrontMeta& f = fm[lst[blockIdx.y]];
+    int c = f.child[cslot];
+    if (c < 0) return;
+    const FrontMeta& g = fm[c];
+    long long tot = (long long)g.b * S;
+    long long i0 = (long long)blockIdx.x * MF_CHUNK;
+    if (i0 >= tot) return;
+    long long i1 = min(i0 + MF_CHUNK, tot);
+    const int* map = ea + g.ea;
+    const float2* U = uvec + g.uv * S;
+    float2* W = w + f.wv * S;
+    for (long long idx = i0 + threadIdx.x; idx < i1; idx += blockDim.x) {
+        long long i = idx / S;
+        int s = (int)(idx % S);
+        float2 u = U[idx];
+        float2* p = W + (long long)map[i] * S + s;
+        p->x += u.x;
+        p->y += u.y;
+    }
+}
+
+// Forward solve inside the 256-row block [k0, k0 + 256) of the own rows: for each 32-step, swaps,
+// y = Linv w, and the update of the block's remaining rows.  One CTA per front.
+__global__ void __launch_bounds__(256) mf_fwd_block_kernel(const int* __restrict__ lst, const FrontMeta* __restrict__ fm,
+                                                           int S, int k0, const float2* __restrict__ fact,
+                                                           const float2* __restrict__ inv, const int* __restrict__ piv,
+                                                           float2* __restrict__ w) {
+    __shared__ float2 y[MF_NB * 64];
+    const FrontMeta& f = fm[lst[blockIdx.x]];
+    if (k0 >= f.e) return;
+    const int k1 = min(k0 + MF_SB, f.e);
+    const long long n = f.n;
+    float2* W = w + f.wv * S;
+    const float2* F = fact + f.fact;
+    const int tid = threadIdx.x;
+    for (int k = k0; k < k1; k += MF_NB) {
+        const int kb = min(MF_NB, f.e - k);
+        const int* P = piv + f.piv + k;
+        // row swaps (sequential in j), one thread per right-hand side
+        if (tid < S) {
+            for (int j = 0; j < kb; j++) {
+                int r = P[j];
+                if (r != j) {
+                    float2 t = W[(long long)(k + j) * S + tid];
+                    W[(long long)(k + j) * S + tid] = W[(long long)(k + r) * S + tid];
+                    W[(long long)(k + r) * S + tid] = t;
+                }
+            }
+        }
+        __syncthreads();
+        const float2* Li = inv + f.inv + (long long)(k / MF_NB) * 2 * MF_NB * MF_NB;
+        for (int sc = 0; sc < S; sc += 64) {
+            const int ns = min(64, S - sc);
+            for (int t = tid; t < kb * ns; t += blockDim.x) {
+                int i = t / ns, s = t % ns;
+                float2 acc = make_float2(0.f, 0.f);
+                for (int c = 0; c <= i; c++) cfma(acc, Li[i + c * MF_NB], W[(long long)(k + c) * S + sc + s]);
+                y[i * 64 + s] = acc;
+            }
+            __syncthreads();
+            for (int t = tid; t < kb * ns; t += blockDim.x) {
+                int i = t / ns, s = t % ns;
+                W[(long long)(k + i) * S + sc + s] = y[i * 64 + s];
+            }
+            // remaining rows of this 256-block
+            for (long long t = tid; t < (long long)(k1 - k - kb) * ns; t += blockDim.x) {
+                long long r = k + kb + t / ns;
+                int s = (int)(t % ns);
+                float2 acc = W[r * S + sc + s];
+                for (int c = 0; c < kb; c++) cfms(acc, F[r + (long long)(k + c) * n], y[c * 64 + s]);
+                W[r * S + sc + s] = acc;
+            }
+            __syncthreads();
+        }
+    }
+}
+
+// Rows [k1, n) of every front: w[r] -= L[r, k0:k1] y[k0:k1]   (one thread per (row, rhs))
+__global__ void __launch_bounds__(256) mf_fwd_update_kernel(const int* __restrict__ lst, const FrontMeta* __restrict__ fm,
+                                                            int S, int k0, const float2* __restrict__ fact,
+                                                            float2* __restrict__ w) {
+    const FrontMeta& f = fm[lst[blockIdx.y]];
+    if (k0 >= f.e) return;
+    const int k1 = min(k0 + MF_SB, f.e);
+    const long long rows = f.n - k1;
+    long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= rows * S) return;
+    long long r = k1 + t / S;
+    int s = (int)(t % S);
+    float2* W = w + f.wv * S;
+    const float2* F = fact + f.fact;
+    const long long n = f.n;
+    float2 acc = W[r * S + s];
+    for (int c = k0; c < k1; c++) cfms(acc, F[r + (long long)c * n], W[(long long)c * S + s]);
+    W[r * S + s] = acc;
+}
+
+// own rows -> y store, boundary rows -> update vector for the parent
+__global__ void mf_fwd_finish_kernel(const int* __restrict__ lst, const FrontMeta* __restrict__ fm, int S,
+                                     const float2* __restrict__ w, float2* __restrict__ ystore, float2* __restrict__ uvec) {
+    const FrontMeta& f = fm[lst[blockIdx.y]];
+    long long tot = (long long)f.n * S;
+    long long i0 = (long long)blockIdx.x * MF_CHUNK;
+    if (i0 >= tot) return;
+    long long i1 = min(i0 + MF_CHUNK, tot);
+    const float2* W = w + f.wv * S;
+    for (long long idx = i0 + threadIdx.x; idx < i1; idx += blockDim.x) {
+        long long i = idx / S;
+        if (i < f.e) ystore[f.y * S + idx] = W[idx];
+        else uvec[f.uv * S + (idx - (long long)f.e * S)] = W[idx];
+    }
+}
+
+// backward: own rows from y, boundary rows from the solved x (FP32, DOF order)
+__global__ void mf_bwd_gather_kernel(const int* __restrict__ lst, const FrontMeta* __restrict__ fm, int S,
+                                     const int* __restrict__ fdof, const float2* __restrict__ ystore,
+                                     const float2* __restrict__ xs, float2* __restrict__ w) {
+    const FrontMeta& f = fm[lst[blockIdx.y]];
+    long long tot = (long long)f.n * S;
+    long long i0 = (long long)blockIdx.x * MF_CHUNK;
+    if (i0 >= tot) return;
+    long long i1 = min(i0 + MF_CHUNK, tot);
+    float2* W = w + f.wv * S;
+    const int* d = fdof + f.fdof;
+    for (long long idx = i0 + threadIdx.x; idx < i1; idx += blockDim.x) {
+        long long i = idx / S;
+        int s = (int)(idx % S);
+        W[idx] = i < f.e ? ystore[f.y * S + idx] : xs[(long long)d[i] * S + s];
+    }
+}
+
+// own rows: w[r] -= U12[r, :] x_bnd   (U12 is e x b, column-major with ld e)
+__global__ void __launch_bounds__(256) mf_bwd_bnd_kernel(const int* __restrict__ lst, const FrontMeta* __restrict__ fm,
+                                                         int S, const float2* __restrict__ fact, float2* __restrict__ w) {
+    const FrontMeta& f = fm[lst[blockIdx.y]];
+    long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long long)f.e * S || f.b == 0) return;
+    long long r = t / S;
+    int s = (int)(t % S);
+    float2* W = w + f.wv * S;
+    const float2* U12 = fact + f.fact + (long long)f.n * f.e;
+    float2 acc = W[r * S + s];
+    for (long long c = 0; c < f.b; c++) cfms(acc, U12[r + c * f.e], W[(f.e + c) * S + s]);
+    W[r * S + s] = acc;
+}
+
+// Backward solve inside the block [k0, k1): 32-steps from the last, x_k = Uinv (w_k), then the block's
+// earlier rows.  One CTA per front.
+__global__ void __launch_bounds__(256) mf_bwd_block_kernel(const int* __restrict__ lst, const FrontMeta* __restrict__ fm,
+                                                           int S, int k0, const float2* __restrict__ fact,
+                                                           const float2* __restrict__ inv, float2* __restrict__ w) {
+    __shared__ float2 xk[MF_NB * 64];
+    const FrontMeta& f = fm[lst[blockIdx.x]];
+    if (k0 >= f.e) return;
+    const int k1 = min(k0 + MF_SB, f.e);
+    const long long n = f.n;
+    float2* W = w + f.wv * S;
+    const float2* F = fact + f.fact;
+    const int tid = threadIdx.x;
+    const int nsteps = (k1 - k0 + MF_NB - 1) / MF_NB;
+    for (int st = nsteps - 1; st >= 0; st--) {
+        const int k = k0 + st * MF_NB;
+        const int kb = min(MF_NB, f.e - k);
+        const float2* Ui = inv + f.inv + (long long)(k / MF_NB) * 2 * MF_NB * MF_NB + MF_NB * MF_NB;
+        for (int sc = 0; sc < S; sc += 64) {
+            const int ns = min(64, S - sc);
+            for (int t = tid; t < kb * ns; t += blockDim.x) {
+                int i = t / ns, s = t % ns;
+                float2 acc = make_float2(0.f, 0.f);
+                for (int c = i; c < kb; c++) cfma(acc, Ui[i + c * MF_NB], W[(long long)(k + c) * S + sc + s]);
+                xk[i * 64 + s] = acc;
+            }
+            __syncthreads();
+            for (int t = tid; t < kb * ns; t += blockDim.x) {
+                int i = t / ns, s = t % ns;
+                W[(long long)(k + i) * S + sc + s] = xk[i * 64 + s];
+            }
+            for (long long t = tid; t < (long long)(k - k0) * ns; t += blockDim.x) {
+                long long r = k0 + t / ns;
+                int s = (int)(t % ns);
+                float2 acc = W[r * S + sc + s];
+                for (int c = 0; c < kb; c++) cfms(acc, F[r + (long long)(k + c) * n], xk[c * 64 + s]);
+                W[r * S + sc + s] = acc;
+            }
+            __syncthreads();
+        }
+    }
+}
+
+// rows [0, k0): w[r] -= U[r, k0:k1] x[k0:k1]
+__global__ void __launch_bounds__(256) mf_bwd_update_kernel(const int* __restrict__ lst, const FrontMeta* __restrict__ fm,
+                                                            int S, int k0, const float2* __restrict__ fact,
+                                                            float2* __restrict__ w) {
+    const FrontMeta& f = fm[lst[blockIdx.y]];
+    if (k0 >= f.e) return;
+    const int k1 = min(k0 + MF_SB, f.e);
+    long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long long)k0 * S) return;
+    long long r = t / S;
+    int s = (int)(t % S);
+    float2* W = w + f.wv * S;
+    const float2* F = fact + f.fact;
+    const long long n = f.n;
+    float2 acc = W[r * S + s];
+    for (int c = k0; c < k1; c++) cfms(acc, F[r + (long long)c * n], W[(long long)c * S + s]);
+    W[r * S + s] = acc;
+}
+
+__global__ void mf_bwd_finish_kernel(const int* __restrict__ lst, const FrontMeta* __restrict__ fm, int S,
+                                     const int* __restrict__ fdof, const float2* __restrict__ w, float2* __restrict__ xs) {
+    const FrontMeta& f = fm[lst[blockIdx.y]];
+    long long tot = (long long)f.e * S;
+    long long i0 = (long long)blockIdx.x * MF_CHUNK;
+    if (i0 >= tot) return;
+    long long i1 = min(i0 + MF_CHUNK, tot);
+    const float2* W = w + f.wv * S;
+    const int* d = fdof + f.fdof;
+    for (long long idx = i0 + threadIdx.x; idx < i1; idx += blockDim.x) {
+        long long i = idx / S;
+        int s = (int)(idx % S);
+        xs[(long long)d[i] * S + s] = W[idx];
+    }
+}
+
+__global__ void mf_out_kernel(long long n, int S, const uint8_t* __restrict__ freed, const float2* __restrict__ xs,
+                              double2* __restrict__ x) {
+    long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= n * S) return;
+    float2 v = xs[g];
+    x[g] = freed[g / S] ? make_double2((double)v.x, (double)v.y) : make_double2(0.0, 0.0);
+}
+
+}  // namespace emfem
+
+using namespace emfem;
+
+struct emfem_mf_s {
+    Handle* h = nullptr;
+    long long n = 0;
+    int nf = 0;
+    std::vector<FrontMeta> meta;                  // host copy
+    std::vector<std::vector<int>> levels;         // fronts per level
+    std::vector<long long> lvl_off;               // offsets of each level's list in d_lst
+    std::vector<int> lvl_max_e, lvl_max_n;
+    std::vector<long long> lvl_max_asm, lvl_max_b;
+    FrontMeta* d_meta = nullptr;
+    int* d_lst = nullptr;
+    int* d_fdof = nullptr;
+    int* d_ea = nullptr;
+    int* d_slot = nullptr;
+    int* d_off = nullptr;
+    uint8_t* d_free = nullptr;                    // 1 where a DOF belongs to some front
+    float2* fact = nullptr;
+    float2* inv = nullptr;
+    int* piv = nullptr;
+    float2* ws = nullptr;
+    float2* upd = nullptr;
+    int* d_npert = nullptr;
+    long long fact_n = 0, inv_n = 0, piv_n = 0, ws_n = 0, upd_n = 0;
+    long long wv_n = 0, uv_n = 0, y_n = 0;        // solve buffer rows
+    // solve buffers for the current S
+    int S = 0;
+    float2 *sw = nullptr, *suv = nullptr, *sy = nullptr, *sx = nullptr;
+    double flops = 0.0;
+    bool factored = false;
+};
+
+static void mf_free(emfem_mf_s* m) {
+    void* ps[] = {m->d_meta, m->d_lst, m->d_fdof, m->d_ea, m->d_slot, m->d_off, m->d_free, m->fact, m->inv, m->piv,
+                  m->ws, m->upd, m->d_npert, m->sw, m->suv, m->sy, m->sx};
+    for (void* p : ps)
+        if (p) cudaFree(p);
+}
+
+static inline unsigned nblk(long long items, long long per) {
+    long long g = (items + per - 1) / per;
+    return (unsigned)std::max(1LL, g);
+}
+
+static int mf_reserve(emfem_mf_s* m, int S) {
+    if (m->S >= S) return EMFEM_OK;
+    void* ps[] = {m->sw, m->suv, m->sy, m->sx};
+    for (void* p : ps)
+        if (p) cudaFree(p);
+    m->sw = m->suv = m->sy = m->sx = nullptr;
+    m->S = 0;
+    EMFEM_CUDA(cudaMalloc(&m->sw, sizeof(float2) * std::max(1LL, m->wv_n) * S));
+    EMFEM_CUDA(cudaMalloc(&m->suv, sizeof(float2) * std::max(1LL, m->uv_n) * S));
+    EMFEM_CUDA(cudaMalloc(&m->sy, sizeof(float2) * std::max(1LL, m->y_n) * S));
+    EMFEM_CUDA(cudaMalloc(&m->sx, sizeof(float2) * m->n * S));
+    m->S = S;
+    return EMFEM_OK;
+}
+
+namespace emfem {
+int mf_reserved(const emfem_mf_s* m) { return m ? m->S : 0; }
+
+// M^-1 r for S right-hand sides (n, S) FP64 DOF-major -> x (FP64), zero on DOFs outside every front.
+int mf_apply(emfem_mf_s* m, int S, const double2* r, double2* x, cudaStream_t s) {
+    EMFEM_REQUIRE(m->factored, "emfem_mf: solve before a successful factorization");
+    if (m->S < S) {
+        set_error("emfem_mf: %d right-hand sides exceed the reserved %d (emfem_mf_reserve)", S, m->S);
+        return EMFEM_ERR_INVALID_ARG;
+    }
+    const int nl = (int)m->levels.size();
+    EMFEM_CUDA(cudaMemsetAsync(m->sx, 0, sizeof(float2) * m->n * S, s));
+    for (int L = 0; L < nl; L++) {
+        const int nfl = (int)m->levels[L].size();
+        const int* lst = m->d_lst + m->lvl_off[L];
+        long long maxn = m->lvl_max_n[L], maxb = m->lvl_max_b[L];
+        for (int y0 = 0; y0 < nfl; y0 += 65535) {
+            const int ny = std::min(65535, nfl - y0);
+            dim3 g(nblk(maxn * S, MF_CHUNK), ny);
+            mf_fwd_gather_kernel<<<g, 256, 0, s>>>(lst + y0, m->d_meta, S, m->d_fdof, r, m->sw);
+            dim3 ge(nblk(maxb * S, MF_CHUNK), ny);
+            mf_fwd_ea_kernel<<<ge, 256, 0, s>>>(lst + y0, m->d_meta, S, 0, m->d_ea, m->suv, m->sw);
+            mf_fwd_ea_kernel<<<ge, 256, 0, s>>>(lst + y0, m->d_meta, S, 1, m->d_ea, m->suv, m->sw);
+            for (int k0 = 0; k0 < m->lvl_max_e[L]; k0 += MF_SB) {
+                mf_fwd_block_kernel<<<ny, 256, 0, s>>>(lst + y0, m->d_meta, S, k0, m->fact, m->inv, m->piv, m->sw);
+                dim3 gu(nblk(maxn * S, 256), ny);      // rows [k1, n) of the widest front, at most n
+                mf_fwd_update_kernel<<<gu, 256, 0, s>>>(lst + y0, m->d_meta, S, k0, m->fact, m->sw);
+            }
+            mf_fwd_finish_kernel<<<g, 256, 0, s>>>(lst + y0, m->d_meta, S, m->sw, m->sy, m->suv);
+        }
+        EMFEM_LAUNCH("multifrontal forward");
+    }
+    for (int L = nl - 1; L >= 0; L--) {
+        const int nfl = (int)m->levels[L].size();
+        const int* lst = m->d_lst + m->lvl_off[L];
+        long long maxn = m->lvl_max_n[L];
+        long long maxe = m->lvl_max_e[L];
+        for (int y0 = 0; y0 < nfl; y0 += 65535) {
+            const int ny = std::min(65535, nfl - y0);
+            dim3 g(nblk(maxn * S, MF_CHUNK), ny);
+            mf_bwd_gather_kernel<<<g, 256, 0, s>>>(lst + y0, m->d_meta, S, m->d_fdof, m->sy, m->sx, m->sw);
+            dim3 gb(nblk(maxe * S, 256), ny);
+            mf_bwd_bnd_kernel<<<gb, 256, 0, s>>>(lst + y0, m->d_meta, S, m->fact, m->sw);
+            const int nblocks = (int)((maxe + MF_SB - 1) / MF_SB);
+            for (int bi = nblocks - 1; bi >= 0; bi--) {
+                const int k0 = bi * MF_SB;
+                mf_bwd_block_kernel<<<ny, 256, 0, s>>>(lst + y0, m->d_meta, S, k0, m->fact, m->inv, m->sw);
+                if (k0 > 0) {
+                    dim3 gu(nblk((long long)k0 * S, 256), ny);
+                    mf_bwd_update_kernel<<<gu, 256, 0, s>>>(lst + y0, m->d_meta, S, k0, m->fact, m->sw);
+                }
+            }
+            dim3 gf(nblk(maxe * S, MF_CHUNK), ny);
+            mf_bwd_finish_kernel<<<gf, 256, 0, s>>>(lst + y0, m->d_meta, S, m->d_fdof, m->sw, m->sx);
+        }
+        EMFEM_LAUNCH("multifrontal backward");
+    }
+    mf_out_kernel<<<grid_for(m->n * S, 256), 256, 0, s>>>(m->n, S, m->d_free, m->sx, x);
+    EMFEM_LAUNCH("mf_out_kernel");
+    return EMFEM_OK;
+}
+}  // namespace emfem
+
+extern "C" {
+
+int emfem_mf_create(emfem_handle h, int64_t n, int n_fronts, const int32_t* e, const int32_t* b, const int32_t* parent,
+                    const int32_t* level, const int64_t* fdof_ptr, const int32_t* fdof, const int32_t* ea,
+                    const int64_t* asm_ptr, const int32_t* asm_slot, const int32_t* asm_off, emfem_mf* out) {
+    EMFEM_REQUIRE(h && n > 0 && n_fronts > 0 && e && b && parent && level && fdof_ptr && fdof && ea && asm_ptr &&
+                      asm_slot && asm_off && out, "emfem_mf_create: bad argument");
+    auto* m = new emfem_mf_s();
+    m->h = &h->h;
+    m->n = n;
+    m->nf = n_fronts;
+    m->meta.resize(n_fronts);
+    int nl = 0;
+    long long tot_fdof = 0;
+    for (int v = 0; v < n_fronts; v++) {
+        if (e[v] < 0 || b[v] < 0 || e[v] + b[v] > MF_MAX_FRONT || level[v] < 0 || parent[v] >= n_fronts ||
+            (parent[v] >= 0 && parent[v] <= v) || fdof_ptr[v + 1] - fdof_ptr[v] != (long long)e[v] + b[v]) {
+            delete m;
+            set_error("emfem_mf_create: front %d is inconsistent (e %d, b %d, parent %d)", v, e[v], b[v], parent[v]);
+            return EMFEM_ERR_INVALID_ARG;
+        }
+        nl = std::max(nl, level[v] + 1);
+        tot_fdof += e[v] + b[v];
+    }
+    m->levels.assign(nl, {});
+    for (int v = 0; v < n_fronts; v++) m->levels[level[v]].push_back(v);
+    // offsets
+    long long fact = 0, inv = 0, pivo = 0, eao = 0, y = 0;
+    for (int v = 0; v < n_fronts; v++) {
+        FrontMeta& f = m->meta[v];
+        f.e = e[v]; f.b = b[v]; f.n = e[v] + b[v]; f.parent = parent[v];
+        f.child[0] = f.child[1] = -1;
+        f.fdof = fdof_ptr[v];
+        f.ea = eao; eao += b[v];
+        f.asm0 = asm_ptr[v]; f.asm1 = asm_ptr[v + 1];
+        f.fact = fact; fact += (long long)f.n * f.e + (long long)f.e * f.b;
+        f.inv = inv; inv += (long long)((f.e + MF_NB - 1) / MF_NB) * 2 * MF_NB * MF_NB;
+        f.piv = pivo; pivo += f.e;
+        f.y = y; y += f.e;
+    }
+    for (int v = 0; v < n_fronts; v++) {
+        int p = parent[v];
+        if (p < 0) continue;
+        FrontMeta& f = m->meta[p];
+        if (f.child[0] < 0) f.child[0] = v;
+        else if (f.child[1] < 0) f.child[1] = v;
+        else { delete m; set_error("emfem_mf_create: front %d has more than two children", p); return EMFEM_ERR_INVALID_ARG; }
+        if (level[p] <= level[v]) { delete m; set_error("emfem_mf_create: parent below child"); return EMFEM_ERR_INVALID_ARG; }
+    }
+    // per-level workspace and solve-buffer offsets; update store by first-fit over the level schedule
+    long long ws_max = 0, wv_max = 0;
+    std::map<long long, long long> freel;   // offset -> size
+    long long upd_top = 0;
+    auto alloc = [&](long long sz) -> long long {
+        for (auto it = freel.begin(); it != freel.end(); ++it) {
+            if (it->second >= sz) {
+                long long o = it->first, rem = it->second - sz;
+                freel.erase(it);
+                if (rem > 0) freel[o + sz] = rem;
+                return o;
+            }
+        }
+        long long o = upd_top;
+        upd_top += sz;
+        return o;
+    };
+    auto release = [&](long long o, long long sz) {
+        if (sz <= 0) return;
+        auto it = freel.emplace(o, sz).first;
+        auto nx = std::next(it);
+        if (nx != freel.end() && it->first + it->second == nx->first) { it->second += nx->second; freel.erase(nx); }
+        if (it != freel.begin()) {
+            auto pv = std::prev(it);
+            if (pv->first + pv->second == it->first) { pv->second += it->second; freel.erase(it); }
+        }
+    };
+    long long uv = 0;
+    m->lvl_max_e.assign(nl, 0); m->lvl_max_n.assign(nl, 0); m->lvl_max_asm.assign(nl, 0); m->lvl_max_b.assign(nl, 0);
+    for (int L = 0; L < nl; L++) {
+        long long wso = 0, wvo = 0;
+        for (int v : m->levels[L]) {
+            FrontMeta& f = m->meta[v];
+            f.ws = wso; wso += (long long)f.n * f.n;
+            f.wv = wvo; wvo += f.n;
+            f.uv = uv; uv += f.b;
+            m->lvl_max_e[L] = std::max(m->lvl_max_e[L], f.e);
+            m->lvl_max_n[L] = std::max(m->lvl_max_n[L], f.n);
+            m->lvl_max_asm[L] = std::max(m->lvl_max_asm[L], f.asm1 - f.asm0);
+            long long cb = 0;
+            for (int c : f.child) if (c >= 0) cb = std::max<long long>(cb, m->meta[c].b);
+            m->lvl_max_b[L] = std::max(m->lvl_max_b[L], cb);
+        }
+        ws_max = std::max(ws_max, wso);
+        wv_max = std::max(wv_max, wvo);
+        // the level's fronts get their update blocks; their children's are freed once the level assembled
+        for (int v : m->levels[L]) {
+            FrontMeta& f = m->meta[v];
+            f.upd = alloc((long long)f.b * f.b);
+        }
+        for (int v : m->levels[L])
+            for (int c : m->meta[v].child)
+                if (c >= 0) release(m->meta[c].upd, (long long)m->meta[c].b * m->meta[c].b);
+    }
+    m->fact_n = fact; m->inv_n = inv; m->piv_n = pivo; m->ws_n = ws_max; m->upd_n = upd_top;
+    m->wv_n = wv_max; m->uv_n = uv; m->y_n = y;
+    for (int v = 0; v < n_fronts; v++) {
+        double E = e[v], B = b[v];
+        m->flops += 8.0 * (E * E * E / 3 + E * E * B + E * B * B);
+    }
+    // device arrays
+    std::vector<int> lst;
+    m->lvl_off.resize(nl);
+    for (int L = 0; L < nl; L++) {
+        m->lvl_off[L] = (long long)lst.size();
+        lst.insert(lst.end(), m->levels[L].begin(), m->levels[L].end());
+    }
+    std::vector<uint8_t> freed(n, 0);
+    for (int v = 0; v < n_fronts; v++)
+        for (int i = 0; i < e[v]; i++) {
+            int d = fdof[fdof_ptr[v] + i];
+            if (d < 0 || d >= n) { delete m; set_error("emfem_mf_create: DOF %d out of range", d); return EMFEM_ERR_INVALID_ARG; }
+            freed[d] = 1;
+        }
+    long long nasm = asm_ptr[n_fronts];
+    int rc = EMFEM_OK;
+    auto up = [&](void** dst, const void* src, size_t bytes) {
+        if (rc != EMFEM_OK) return;
+        rc = check_cuda(cudaMalloc(dst, std::max<size_t>(bytes, 16)), "cudaMalloc");
+        if (rc == EMFEM_OK && bytes) rc = check_cuda(cudaMemcpy(*dst, src, bytes, cudaMemcpyHostToDevice), "cudaMemcpy");
+    };
+    up((void**)&m->d_meta, m->meta.data(), sizeof(FrontMeta) * n_fronts);
+    up((void**)&m->d_lst, lst.data(), sizeof(int) * lst.size());
+    up((void**)&m->d_fdof, fdof, sizeof(int) * tot_fdof);
+    up((void**)&m->d_ea, ea, sizeof(int) * eao);
+    up((void**)&m->d_slot, asm_slot, sizeof(int) * nasm);
+    up((void**)&m->d_off, asm_off, sizeof(int) * nasm);
+    up((void**)&m->d_free, freed.data(), n);
+    auto mk = [&](void** dst, size_t bytes) {
+        if (rc != EMFEM_OK) return;
+        rc = check_cuda(cudaMalloc(dst, std::max<size_t>(bytes, 16)), "cudaMalloc");
+    };
+    mk((void**)&m->fact, sizeof(float2) * fact);
+    mk((void**)&m->inv, sizeof(float2) * inv);
+    mk((void**)&m->piv, sizeof(int) * pivo);
+    mk((void**)&m->ws, sizeof(float2) * ws_max);
+    mk((void**)&m->upd, sizeof(float2) * upd_top);
+    mk((void**)&m->d_npert, sizeof(int));
+    if (rc != EMFEM_OK) { mf_free(m); delete m; return rc; }
+    *out = m;
+    return EMFEM_OK;
+}
+
+int emfem_mf_info(emfem_mf m, size_t* device_bytes, double* flops, int* n_levels) {
+    EMFEM_REQUIRE(m, "emfem_mf_info: bad handle");
+    if (device_bytes)
+        *device_bytes = sizeof(float2) * (m->fact_n + m->inv_n + m->ws_n + m->upd_n) + sizeof(int) * m->piv_n;
+    if (flops) *flops = m->flops;
+    if (n_levels) *n_levels = (int)m->levels.size();
+    return EMFEM_OK;
+}
+
+int emfem_mf_factor(emfem_mf m, const void* K_vals, int* n_perturbed) {
+    EMFEM_REQUIRE(m && K_vals, "emfem_mf_factor: bad argument");
+    cudaStream_t s = m->h->stream;
+    int prev = 0;
+    EMFEM_CUDA(cudaGetDevice(&prev));
+    if (prev != m->h->device) EMFEM_CUDA(cudaSetDevice(m->h->device));
+    int rc = EMFEM_OK;
+    m->factored = false;
+    rc = check_cuda(cudaMemsetAsync(m->d_npert, 0, sizeof(int), s), "cudaMemsetAsync");
+    const int nl = (int)m->levels.size();
+    for (int L = 0; L < nl && rc == EMFEM_OK; L++) {
+        const int nfl = (int)m->levels[L].size();
+        long long wsz = 0;
+        for (int v : m->levels[L]) wsz += (long long)m->meta[v].n * m->meta[v].n;
+        rc = check_cuda(cudaMemsetAsync(m->ws, 0, sizeof(float2) * wsz, s), "cudaMemsetAsync");
+        for (int y0 = 0; y0 < nfl && rc == EMFEM_OK; y0 += 65535) {
+            const int ny = std::min(65535, nfl - y0);
+            const int* lst = m->d_lst + m->lvl_off[L] + y0;
+            long long maxn = m->lvl_max_n[L], maxb = m->lvl_max_b[L];
+            mf_asm_kernel<<<dim3(nblk(m->lvl_max_asm[L], MF_CHUNK), ny), 256, 0, s>>>(
+                lst, m->d_meta, (const double2*)K_vals, m->d_slot, m->d_off, m->ws);
+            for (int c = 0; c < 2; c++)
+                mf_ea_kernel<<<dim3(nblk(maxb * maxb, MF_CHUNK), ny), 256, 0, s>>>(lst, m->d_meta, c, m->d_ea, m->upd, m->ws);
+            for (int k = 0; k < m->lvl_max_e[L]; k += MF_NB) {
+                mf_diag_kernel<<<ny, 32, 0, s>>>(lst, m->d_meta, k, m->ws, m->inv, m->piv, m->d_npert);
+                long long mm = maxn - k - 1;
+                if (mm < 1) mm = 1;
+                mf_panel_kernel<<<dim3(nblk(2 * mm, 256), ny), 256, 0, s>>>(lst, m->d_meta, k, m->ws, m->inv, m->piv);
+                long long nt = (mm + MF_TILE - 1) / MF_TILE;
+                mf_trail_kernel<<<dim3((unsigned)std::max(1LL, nt * nt), ny), 256, 0, s>>>(lst, m->d_meta, k, m->ws);
+            }
+            mf_compact_kernel<<<dim3(nblk(maxn * maxn, MF_CHUNK), ny), 256, 0, s>>>(lst, m->d_meta, m->ws, m->fact, m->upd);
+            rc = check_cuda(cudaGetLastError(), "multifrontal factor level");
+        }
+        if (nfl > 65535 && rc == EMFEM_OK) {
+            // the level workspace holds every front of the level at once; levels wider than one grid are split
+            // only in their launches, never in their storage
+        }
+    }
+    int np = 0;
+    if (rc == EMFEM_OK) rc = check_cuda(cudaMemcpyAsync(&np, m->d_npert, sizeof(int), cudaMemcpyDeviceToHost, s), "copy");
+    if (rc == EMFEM_OK) rc = check_cuda(cudaStreamSynchronize(s), "sync");
+    if (rc == EMFEM_OK) {
+        m->factored = true;
+        if (n_perturbed) *n_perturbed = np;
+    }
+    if (prev != m->h->device) cudaSetDevice(prev);
+    return rc;
+}
+
+int emfem_mf_reserve(emfem_mf m, int nrhs) {
+    EMFEM_REQUIRE(m && nrhs >= 1 && nrhs <= 256, "emfem_mf_reserve: bad argument");
+    return mf_reserve(m, nrhs);
+}
+
+int emfem_mf_solve(emfem_mf m, int nrhs, const void* b, void* x) {
+    EMFEM_REQUIRE(m && b && x && nrhs >= 1, "emfem_mf_solve: bad argument");
+    EMFEM_TRY(mf_reserve(m, nrhs));
+    return mf_apply(m, nrhs, (const double2*)b, (double2*)x, m->h->stream);
+}
+
+int emfem_mf_destroy(emfem_mf m) {
+    if (!m) return EMFEM_OK;
+    cudaStreamSynchronize(m->h->stream);
+    mf_free(m);
+    delete m;
+    return EMFEM_OK;
+}
+
+}  // extern "C"

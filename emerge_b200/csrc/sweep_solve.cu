@@ -855,7 +855,9 @@ struct Krylov {
     // auxiliary-space correction (precond 3: aux Jacobi, 4: learned network); BiCGStab only
     const emfem_aux_s* aux = nullptr;
     T* adinv = nullptr;
-    int bj() const { return precond >= 3 ? 2 : precond; }
+    // multifrontal LU of one system's operator (precond 5): M^-1 for every system of the batch
+    emfem_mf_s* mf = nullptr;
+    int bj() const { return precond == 5 ? 0 : (precond >= 3 ? 2 : precond); }
 
     unsigned nb_all() const { return grid_for(n * (long long)S, VB); }
     unsigned nb_pair() const { return grid_for(h * (long long)S, VB); }
@@ -894,10 +896,16 @@ struct Krylov {
             T *rh = v[0], *p = v[1], *vv = v[2], *ph = v[3], *sh = v[4], *t = v[5];
             bicg_p_kernel<R><<<nb_pair(), VB, 0, s>>>(h, S, bj(), pg, st, r, p, vv, ph, minv, rh);
             if (aux) EMFEM_TRY(aux_correct<T>(aux, S, precond == 4, adinv, p, op.mask, ph, s));
+            if constexpr (sizeof(R) == 8) {
+                if (mf) EMFEM_TRY(mf_apply(mf, S, (const double2*)p, (double2*)ph, s));
+            }
             spmv_kernel<R><<<nb_all(), VB, 0, s>>>(op, ph, vv, partial, DOT_CONJW_Y, rh);
             reduce(1, nb_all(), UPD_BICG_ALPHA);
             bicg_s_kernel<R><<<nb_pair(), VB, 0, s>>>(h, S, bj(), pg, st, r, vv, sh, minv);
             if (aux) EMFEM_TRY(aux_correct<T>(aux, S, precond == 4, adinv, r, op.mask, sh, s));
+            if constexpr (sizeof(R) == 8) {
+                if (mf) EMFEM_TRY(mf_apply(mf, S, (const double2*)r, (double2*)sh, s));
+            }
             spmv_kernel<R><<<nb_all(), VB, 0, s>>>(op, sh, t, partial, DOT_CONJY_W_YY, r);
             reduce(3, nb_all(), UPD_BICG_OMEGA);
             bicg_x_kernel<R><<<nb_all(), VB, 0, s>>>(n, S, pg, st, x, r, ph, sh, t, rh, partial);
@@ -1016,18 +1024,22 @@ static int krylov_impl(emfem_handle hd, int method, int64_t n, int64_t nnz, cons
                        const int32_t* patch_cols, const void* patch_vals, const int32_t* patch_port,
                        int n_ports, const double* gamma, const uint8_t* free_mask, const void* rhs, void* x,
                        double tol, int maxit, int precond, int precision, void* workspace, size_t workspace_bytes,
-                       int* status, int* iters, double* relres, emfem_aux aux, int G, const int32_t* pair_group) {
+                       int* status, int* iters, double* relres, emfem_aux aux, int G, const int32_t* pair_group,
+                       emfem_mf_s* mf = nullptr) {
     EMFEM_REQUIRE(hd && indptr && indices && E_vals && k0sq && free_mask && rhs && x && workspace,
                   "emfem_krylov_solve: null argument");
+    EMFEM_REQUIRE((precond == 5) == (mf != nullptr), "emfem_krylov_solve: the LU preconditioner goes with precond 5");
+    EMFEM_REQUIRE(precond != 5 || (method == 1 && precision == 0 && G == 1),
+                  "emfem_krylov_solve_lu: FP64 BiCGStab on one group only");
     EMFEM_REQUIRE(method == 0 || method == 1, "emfem_krylov_solve: method must be 0 (COCG) or 1 (BiCGStab)");
     EMFEM_REQUIRE(n > 0 && (n % 2) == 0, "emfem_krylov_solve: n must be even (DOF pairs i, i + n/2)");
     EMFEM_REQUIRE(nsys >= 1 && nsys <= 64, "emfem_krylov_solve: 1 <= nsys <= 64");
-    EMFEM_REQUIRE(precond >= 0 && precond <= 4 && (precision == 0 || precision == 1), "emfem_krylov_solve: bad option");
-    EMFEM_REQUIRE(precond < 3 || (aux && method == 1 && aux->n == n && aux->have_operator && aux->nports == n_ports),
+    EMFEM_REQUIRE(precond >= 0 && precond <= 5 && (precision == 0 || precision == 1), "emfem_krylov_solve: bad option");
+    EMFEM_REQUIRE(precond < 3 || precond == 5 || (aux && method == 1 && aux->n == n && aux->have_operator && aux->nports == n_ports),
                   "emfem_krylov_solve: precond 3/4 need BiCGStab and an aux space of this field with its operator "
                   "set (emfem_aux_set_operator, same ports)");
     EMFEM_REQUIRE(precond != 4 || aux->params, "emfem_krylov_solve: precond 4 needs network parameters (emfem_aux_set_network)");
-    EMFEM_REQUIRE(precond < 3 || aux->ngroups == G,
+    EMFEM_REQUIRE(precond < 3 || precond == 5 || aux->ngroups == G,
                   "emfem_krylov_solve: the aux space's groups (emfem_aux_set_rows) must match the solve's groups");
     EMFEM_REQUIRE(n_ports >= 0 && n_ports <= 8, "emfem_krylov_solve: at most 8 ports");
     EMFEM_REQUIRE(n_patch_rows == 0 || (patch_rows && patch_rowptr && patch_cols && patch_vals && patch_port && gamma),
@@ -1042,7 +1054,9 @@ static int krylov_impl(emfem_handle hd, int method, int64_t n, int64_t nnz, cons
         npatch = last;
     }
     EMFEM_REQUIRE(npatch <= nnz, "emfem_krylov_solve: more patch entries than nnz");
-    EMFEM_REQUIRE(precond < 3 || aux->kbuf_bytes >= aux_solve_bytes(aux, S),
+    EMFEM_REQUIRE(precond != 5 || mf_reserved(mf) >= S,
+                  "emfem_krylov_solve_lu: call emfem_mf_reserve with at least the padded batch size first");
+    EMFEM_REQUIRE(precond < 3 || precond == 5 || aux->kbuf_bytes >= aux_solve_bytes(aux, S),
                   "emfem_krylov_solve: call emfem_aux_reserve with at least nsys systems first");
     std::vector<int> hgblk(G + 1, 0);
     if (G > 1) {
@@ -1138,21 +1152,22 @@ static int krylov_impl(emfem_handle hd, int method, int64_t n, int64_t nnz, cons
         k.partial = partial; k.st = st; k.s = s;
         k.op.skip = st;
         k.G = G; k.pg = G > 1 ? pair_group : nullptr; k.gblk = gblk;
-        if (precond) {
+        if (k.bj()) {
             precond_setup_kernel<double><<<grid_for((n / 2) * (long long)S, VB), VB, 0, s>>>(op64, k.bj(), k.minv);
             STRY(check_cuda(cudaGetLastError(), "precond_setup"));
         }
-        if (precond >= 3) {
+        if (precond == 3 || precond == 4) {
             k.aux = aux;
             k.adinv = (double2*)aux_dinv_buffer(aux, S);
             STRY(aux_setup_dinv<double2>(aux, S, nsys, k0dev, gdev, k.adinv, s));
         }
+        k.mf = mf;
         // the recurrence tolerance is half the requested one so the FP64 true residual meets it
         reduce_update_kernel<<<G * S, VB, 0, s>>>(partial, (int)gv, S, 2, st, UPD_INIT, maxit, 0.5 * tol, nsys, G, gblk, 1,
                                                   nbh);
         STRY(check_cuda(cudaGetLastError(), "init state"));
         STRY(k.start());
-        STRY(k.run(16));
+        STRY(k.run(mf ? 2 : 16));     // an LU application is ~1000 launches: short captured chunks
     } else {
         OpArgs op32 = op64;  // FP64 values, FP32 vectors (see spmv_kernel)
         Krylov<float> k;
@@ -1286,6 +1301,18 @@ int emfem_krylov_solve(emfem_handle hd, int method, int64_t n, int64_t nnz, cons
     return krylov_impl(hd, method, n, nnz, indptr, indices, E_vals, B_vals, nsys, k0sq, n_patch_rows, patch_rows,
                        patch_rowptr, patch_cols, patch_vals, patch_port, n_ports, gamma, free_mask, rhs, x, tol, maxit,
                        precond, precision, workspace, workspace_bytes, status, iters, relres, aux, 1, nullptr);
+}
+
+int emfem_krylov_solve_lu(emfem_handle hd, int64_t n, int64_t nnz, const int32_t* indptr, const int32_t* indices,
+                          const void* E_vals, const void* B_vals, int nsys, const double* k0sq, int64_t n_patch_rows,
+                          const int32_t* patch_rows, const int32_t* patch_rowptr, const int32_t* patch_cols,
+                          const void* patch_vals, const int32_t* patch_port, int n_ports, const double* gamma,
+                          const uint8_t* free_mask, const void* rhs, void* x, double tol, int maxit, emfem_mf lu,
+                          void* workspace, size_t workspace_bytes, int* status, int* iters, double* relres) {
+    EMFEM_REQUIRE(lu, "emfem_krylov_solve_lu: no factorization");
+    return krylov_impl(hd, 1, n, nnz, indptr, indices, E_vals, B_vals, nsys, k0sq, n_patch_rows, patch_rows,
+                       patch_rowptr, patch_cols, patch_vals, patch_port, n_ports, gamma, free_mask, rhs, x, tol, maxit,
+                       5, 0, workspace, workspace_bytes, status, iters, relres, nullptr, 1, nullptr, lu);
 }
 
 int emfem_krylov_workspace_size_grouped(int64_t n, int64_t nnz, int nsys, int ngroups, int precision, size_t* bytes) {

@@ -61,8 +61,11 @@ def eigenmodes(sweep, nmodes: int = 4, target_k0: float = 1.0, tol: float = 1e-1
     boundaries, as the reference's assemble_eig_matrix takes one frequency for them).
 
     ``block`` (a power of two, at most 64; default the smallest one >= max(2 nmodes, nmodes + 8)) vectors
-    are iterated; the loop stops when every wanted pair's residual is <= ``eig_tol`` or after
-    ``max_outer`` steps.  ``tol``/``maxit``/``precond`` configure the inner solves."""
+    are iterated; the loop stops when every wanted pair's residual is <= ``eig_tol``, when the residuals
+    stall, or after ``max_outer`` steps.  ``tol``/``maxit``/``precond`` configure the inner solves.
+    Pairs inside the λ = 0 gradient null space of a closed region (nearer σ than the next physical mode
+    when σ is low) are not individual eigenpairs; they come back with ``converged`` False unless their
+    residual passes."""
     dev = sweep.device
     if nmodes < 1:
         raise ValueError("eigenmodes: nmodes must be >= 1")

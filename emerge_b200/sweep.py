@@ -437,11 +437,22 @@ class FrequencySweep:
                               precond=precond, precision=precision, method=method, x0=x0,
                               raise_on_fail=raise_on_fail, systems=systems)
 
+    def solve_lu(self, systems, lu, tol: float = 1e-8, maxit: int = 500, x0: torch.Tensor | None = None,
+                 raise_on_fail: bool = False) -> SolveResult:
+        """The listed (frequency, port) systems by FP64 BiCGStab right-preconditioned with the device LU
+        ``lu`` (:class:`~emerge_b200.direct.DeviceLU`, factored at one frequency of this sweep: at that
+        frequency a few iterations refine its complex64 solution to the FP64 tolerance, at neighbouring
+        ones the LU is a preconditioner for the shifted operator)."""
+        freqs = [f for f, _ in systems]
+        return self.solve_rhs(self.k0sq(freqs), self.rhs(systems), self.gammas(freqs), tol=tol, maxit=maxit,
+                              x0=x0, raise_on_fail=raise_on_fail, systems=systems, lu=lu)
+
     def solve_rhs(self, k0sq, b: torch.Tensor, gammas=None, tol: float = 1e-8, maxit: int = 20000,
                   precond: str = "block_jacobi", precision: str = "fp64", method: str = "bicgstab",
-                  x0: torch.Tensor | None = None, raise_on_fail: bool = False, systems=None) -> SolveResult:
+                  x0: torch.Tensor | None = None, raise_on_fail: bool = False, systems=None, lu=None) -> SolveResult:
         """(E - k0sq_s B + sum_p gammas[s, p] R_p) x_s = b_s for arbitrary right-hand sides b (N, nsys)
-        on the free DOFs (gammas default 0: the Robin terms drop out)."""
+        on the free DOFs (gammas default 0: the Robin terms drop out).  With ``lu`` (a factored
+        :class:`~emerge_b200.direct.DeviceLU`) the solve is FP64 BiCGStab preconditioned by it."""
         b = b.to(device=self.device, dtype=torch.complex128).contiguous()
         nsys = b.shape[1]
         assert 1 <= nsys <= 64
@@ -460,7 +471,7 @@ class FrequencySweep:
         ga = (ctypes.c_double * len(gam))(*gam)
         aux = None
         pc = PRECOND[precond]
-        if pc >= 3:
+        if pc >= 3 and lu is None:
             if precond == "learned" and self.network is None:
                 raise ValueError("precond='learned' needs a trained network (FrequencySweep.set_network)")
             if pc == 4 and not self._learned_active:
@@ -469,6 +480,22 @@ class FrequencySweep:
             a.reserve(nsys)
             aux = a.handle
         h = Handle.get(self.device)
+        if lu is not None:
+            if lu.frequency is None:
+                raise ValueError("solve_rhs: the LU has not been factored")
+            lu.reserve(1 << (nsys - 1).bit_length())
+            ws = self.workspace(nsys, 0)
+            t0 = time.perf_counter()
+            st = lib().emfem_krylov_solve_lu(h.h, self.n, self.plan.nnz, ptr(self.plan.indptr), ptr(self.plan.indices),
+                                             ptr(self.E), ptr(self.B), nsys, k0a, self.patch_rows.numel(),
+                                             ptr(self.patch_rows), ptr(self.patch_rowptr), ptr(self.patch_cols),
+                                             ptr(self.patch_vals), ptr(self.patch_port), self.n_ports, ga, ptr(self.mask),
+                                             ptr(b), ptr(x), tol, maxit, lu._p, ptr(ws), ws.numel(), status, iters, relres)
+            dt = time.perf_counter() - t0
+            if st not in (0, ERR_NOT_CONVERGED) or (raise_on_fail and st != 0):
+                check(st, "emfem_krylov_solve_lu")
+            return SolveResult(x, np.array(status[:]), np.array(iters[:]), np.array(relres[:]),
+                               list(systems) if systems is not None else [], dt)
         t0 = time.perf_counter()
         st = lib().emfem_krylov_solve(h.h, METHOD[method], self.n, self.plan.nnz, ptr(self.plan.indptr), ptr(self.plan.indices),
                                     ptr(self.E), ptr(self.B), nsys, k0a,

@@ -357,6 +357,45 @@ int emfem_mpnn_backward(emfem_aux aux, int nsys, const float *params, const void
 int emfem_adam_step(emfem_handle h, int64_t n, float *params, const float *grad, float *m, float *v, float lr,
                     float beta1, float beta2, float eps, float weight_decay, int step);
 
+/* ---- multifrontal LU (device direct solve) ---------------------------------------------------
+ * Replaces the reference's direct solve, SolverSuperLU (src/emerge/_emerge/solver.py:535-572, SuperLU
+ * with MMD ordering), for the sweep system on a CSR pattern.  The host builds the symbolic structure
+ * (emerge_b200/direct.py: nested dissection of the mesh's tets, fronts, assembly lists); the library
+ * factors and solves on the device in complex64 (fronts) with FP64 input and output.
+ * create (host arrays; allocates all device memory once): n_fronts fronts in postorder (children before
+ *   parents, each front at most two children); e / b: eliminated and boundary DOFs per front (e + b <=
+ *   46340); parent (-1 for the root), level (height, leaves 0; a parent's level exceeds its children's);
+ *   fdof[fdof_ptr[v] .. fdof_ptr[v + 1]): the front's DOFs (own, then boundary, as CSR row numbers);
+ *   ea: for every front in order, the position of each of its b boundary DOFs in its parent's front;
+ *   asm_slot / asm_off (asm_ptr per front): the CSR slots assembled into each front and their local
+ *   offsets row + col * (e + b).
+ * info: device bytes held, factorization flops, number of levels.
+ * factor: K_vals (nnz c128, device) on the CSR pattern the structure was built for; *n_perturbed
+ *   (host) gets the number of pivots raised to 1e-6 of their 32 x 32 block's largest entry (pivoting is
+ *   partial inside each 32-row diagonal block).  Synchronises the stream.
+ * reserve: solve buffers for up to nrhs right-hand sides (<= 256).
+ * solve: x = (LU)^-1 b for nrhs right-hand sides, b and x (n, nrhs) c128 DOF-major, device; x is zero on
+ *   DOFs that belong to no front (PEC).
+ * emfem_krylov_solve_lu: FP64 right-preconditioned BiCGStab of emfem_krylov_solve (same operator and
+ *   arguments) with M = this factorization for every system; the factorization may belong to another
+ *   frequency of the same mesh (a window of a sweep shares one).  Reserve the padded batch size
+ *   (next power of two of nsys) first. */
+typedef struct emfem_mf_s *emfem_mf;
+int emfem_mf_create(emfem_handle h, int64_t n, int n_fronts, const int32_t *e, const int32_t *b, const int32_t *parent,
+                    const int32_t *level, const int64_t *fdof_ptr, const int32_t *fdof, const int32_t *ea,
+                    const int64_t *asm_ptr, const int32_t *asm_slot, const int32_t *asm_off, emfem_mf *out);
+int emfem_mf_info(emfem_mf lu, size_t *device_bytes, double *flops, int *n_levels);
+int emfem_mf_factor(emfem_mf lu, const void *K_vals, int *n_perturbed);
+int emfem_mf_reserve(emfem_mf lu, int nrhs);
+int emfem_mf_solve(emfem_mf lu, int nrhs, const void *b, void *x);
+int emfem_mf_destroy(emfem_mf lu);
+int emfem_krylov_solve_lu(emfem_handle h, int64_t n, int64_t nnz, const int32_t *indptr, const int32_t *indices,
+                          const void *E_vals, const void *B_vals, int nsys, const double *k0sq, int64_t n_patch_rows,
+                          const int32_t *patch_rows, const int32_t *patch_rowptr, const int32_t *patch_cols,
+                          const void *patch_vals, const int32_t *patch_port, int n_ports, const double *gamma,
+                          const uint8_t *free_mask, const void *rhs, void *x, double tol, int maxit, emfem_mf lu,
+                          void *workspace, size_t workspace_bytes, int *status, int *iters, double *relres);
+
 /* ---- allocation-free sweep SpMV ------------------------------------------------------------
  * No counterpart in the reference.  The same y_s = A_s x_s as emfem_sweep_spmv, for callers that
  * cannot call cudaMalloc: applications whose device memory is owned up front by their own pool

@@ -1,0 +1,94 @@
+"""The device multifrontal LU (emerge_b200.direct.DeviceLU, emfem_mf_*) and the LU-preconditioned
+sweep (emfem_krylov_solve_lu) against the reference's direct solve: SuperLU on the oracle's matrices
+(SolverSuperLU, src/emerge/_emerge/solver.py:535-572) and the reference's own SuperLU solutions."""
+import numpy as np
+import pytest
+import scipy.sparse.linalg as spl
+import torch
+
+import oracle
+from emerge_b200 import problems
+from emerge_b200.direct import DeviceLU
+from emerge_b200.ports import k0_of
+from emerge_b200.sweep import FrequencySweep
+
+pytestmark = pytest.mark.gpu
+
+
+def _oracle_solution(P, f, q):
+    """SuperLU on the oracle's K_f with port q's excitation (the reference's SolveRoutine path)."""
+    fld = P.field
+    E, B = oracle.tet_mass_stiffness_matrices(fld, P.er, P.ur)
+    k0 = k0_of(f)
+    Bm = fld.empty_tri_matrix()
+    b = np.zeros(fld.n_field, complex)
+    for i, p in enumerate(P.ports):
+        if i == q:
+            Bm, bp = oracle.assemble_robin_bc_excited(fld, Bm, p.tri_ids, lambda x, y, z, p=p: p.get_Uinc(x, y, z, k0),
+                                                      p.get_gamma(k0), oracle.dunavant4())
+            b += bp
+        else:
+            Bm = oracle.assemble_robin_bc(fld, Bm, p.tri_ids, p.get_gamma(k0))
+    K = (E - B * k0 ** 2 + fld.generate_csr(Bm)).tocsc()
+    ids = P.solve_ids
+    x = np.zeros(fld.n_field, complex)
+    x[ids] = spl.spsolve(K[ids][:, ids], b[ids])
+    return x, K
+
+
+def test_device_lu_solve_matches_superlu(cuda):
+    P = problems.waveguide()
+    sw = FrequencySweep(P)
+    lu = DeviceLU(sw).factor(10e9)
+    assert lu.n_perturbed == 0
+    _, K = _oracle_solution(P, 10e9, 0)
+    ids = P.solve_ids
+    rng = np.random.default_rng(3)
+    b = np.zeros((sw.n, 3), complex)
+    b[ids] = rng.standard_normal((len(ids), 3)) + 1j * rng.standard_normal((len(ids), 3))
+    x = lu.solve(torch.from_numpy(b).to(sw.device)).cpu().numpy()
+    Kf = K[ids][:, ids].tocsc()
+    for j in range(3):
+        xr = spl.spsolve(Kf, b[ids, j])
+        # complex64 factors: the error is the single-precision rounding amplified by the conditioning
+        assert np.linalg.norm(x[ids, j] - xr) <= 1e-3 * np.linalg.norm(xr)
+    pec = np.setdiff1d(np.arange(sw.n), ids)
+    assert np.abs(x[pec]).max() == 0
+
+
+def test_lu_preconditioned_sweep_matches_superlu_golden(cuda, golden):
+    g = golden("config1")
+    f = float(g["f"])
+    P = problems.waveguide()
+    sw = FrequencySweep(P)
+    lu = DeviceLU(sw).factor(f)
+    res = sw.solve_lu([(f, 0), (f, 1)], lu, tol=1e-12, maxit=60)
+    assert (res.status == 0).all(), (res.status, res.iters, res.relres)
+    assert res.iters.max() <= 12, res.iters            # the complex64 LU of the same operator: a few refinements
+    x = res.x.cpu().numpy()
+    for j, key in enumerate(("x1", "x2")):
+        assert np.linalg.norm(x[:, j] - g[key]) <= 1e-10 * np.linalg.norm(g[key])
+    # the same factorization preconditions a neighbouring frequency
+    f2 = 1.03 * f
+    r2 = sw.solve_lu([(f2, 0), (f2, 1)], lu, tol=1e-10, maxit=300)
+    assert (r2.status == 0).all(), (r2.status, r2.iters, r2.relres)
+    for q in (0, 1):
+        xr, _ = _oracle_solution(P, f2, q)
+        assert np.linalg.norm(r2.x[:, q].cpu().numpy() - xr) <= 1e-8 * np.linalg.norm(xr)
+
+
+def test_lu_solves_a_cavity_where_block_jacobi_stalls(cuda):
+    """The dielectric-loaded cavity family (closed, lightly lossy, one port): block-Jacobi BiCGStab does
+    not reach 1e-8, the LU-preconditioned solve does and agrees with SuperLU."""
+    P = problems.cavity(n=8)
+    sw = FrequencySweep(P)
+    freqs = [float(f) for f in P.freqs[40:44]]
+    systems = [(f, 0) for f in freqs]
+    bj = sw.solve(systems, tol=1e-8, maxit=4000, precond="block_jacobi")
+    lu = DeviceLU(sw).factor(freqs[1])
+    res = sw.solve_lu(systems, lu, tol=1e-10, maxit=400)
+    assert (res.status == 0).all(), (res.status, res.iters, res.relres)
+    assert (bj.status != 0).any() or bj.iters.max() > 20 * res.iters.max()
+    for j, f in enumerate(freqs):
+        xr, _ = _oracle_solution(P, f, 0)
+        assert np.linalg.norm(res.x[:, j].cpu().numpy() - xr) <= 1e-8 * np.linalg.norm(xr), f

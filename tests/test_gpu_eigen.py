@@ -27,7 +27,13 @@ def test_pec_cavity_eigenmodes_match_direct_arpack_and_te101(cuda):
     Bf = B[ids][:, ids].tocsc()
     vo, _ = eigs(Ef, k=3, M=Bf, sigma=sigma, which="LM")
     vo = vo[np.argsort(np.abs(vo - sigma))]
-    assert np.abs(res.k0sq - vo).max() <= 1e-8 * np.abs(vo).max(), (res.k0sq, vo)
+    # the physical mode nearest the shift agrees with the direct solve
+    assert abs(res.k0sq[0] - vo[0]) <= 1e-8 * abs(vo[0]), (res.k0sq, vo)
+    # the next nearest eigenvalues of this closed box are the lambda = 0 gradient fields (a null space of
+    # E with thousands of members, nearer sigma than TE102); both solvers return values there, which are
+    # not individual eigenpairs: ours flag them unless their residual passes
+    assert np.abs(vo[1:]).max() <= 1e-6 * abs(vo[0])
+    assert np.abs(res.k0sq[1:]).max() <= 1e-2 * abs(vo[0]), res.k0sq
     # the mode nearest the target is TE101, within the discretisation error
     assert abs(res.k0sq[0].real - k101 ** 2) <= 5e-3 * k101 ** 2, (res.k0sq[0], k101 ** 2)
     assert abs(res.k0sq[0].imag) <= 1e-9 * abs(res.k0sq[0])
@@ -37,7 +43,11 @@ def test_pec_cavity_eigenmodes_match_direct_arpack_and_te101(cuda):
     assert np.abs(x[pec]).max() == 0
     r = Ef @ x[ids] - res.k0sq[0] * (Bf @ x[ids])
     assert np.linalg.norm(r) <= 1e-7 * np.linalg.norm(Ef @ x[ids])
-    assert res.inner_solves > 0 and res.converged.all()
+    assert res.inner_solves > 0 and res.converged[0]
+    for j in np.flatnonzero(res.converged):          # every pair reported as converged is an eigenpair
+        xj = res.modes[ids, j]
+        rj = Ef @ xj - res.k0sq[j] * (Bf @ xj)
+        assert np.linalg.norm(rj) <= 1e-6 * (np.linalg.norm(Ef @ xj) + sigma * np.linalg.norm(Bf @ xj)), j
 
 
 def test_eigenmodes_with_ports_match_direct_arpack(cuda):

@@ -194,7 +194,21 @@ __global__ void __launch_bounds__(32) mf_diag_kernel(const int* __restrict__ lst
         }
     }
     __syncwarp();
-    for (int c = 0; c < MF_NB; c++) Li[lane + c * MF_NB] = X[lane][c];
+    // the block's row swaps folded into the inverse: w' = P w (swaps j = 0..kb-1 in order) has
+    // w'[i] = w[q[i]], so y = Linv w' = (Linv P) w with column q[i] of Linv P = column i of Linv
+    int q[MF_NB];
+#pragma unroll
+    for (int i = 0; i < MF_NB; i++) q[i] = i;
+    for (int j = 0; j < kb; j++) {
+        int r = P[j];
+        int a = 0, b2 = 0;
+#pragma unroll
+        for (int i = 0; i < MF_NB; i++) { if (i == j) a = q[i]; if (i == r) b2 = q[i]; }
+#pragma unroll
+        for (int i = 0; i < MF_NB; i++) { if (i == j) q[i] = b2; if (i == r) q[i] = a; }
+    }
+#pragma unroll
+    for (int i = 0; i < MF_NB; i++) Li[lane + q[i] * MF_NB] = X[lane][i];
 }
 
 // Block row (columns >= k + kb): row swaps, then L^-1; block column (rows >= k + kb): times U^-1.
@@ -204,7 +218,6 @@ __global__ void __launch_bounds__(256) mf_panel_kernel(const int* __restrict__ l
                                                        const int* __restrict__ piv) {
     __shared__ float2 Li[MF_NB * MF_NB];
     __shared__ float2 Ui[MF_NB * MF_NB];
-    __shared__ int P[MF_NB];
     const FrontMeta& f = fm[lst[blockIdx.y]];
     if (k >= f.e) return;
     const int kb = min(MF_NB, f.e - k);
@@ -213,7 +226,6 @@ __global__ void __launch_bounds__(256) mf_panel_kernel(const int* __restrict__ l
     if ((long long)blockIdx.x * blockDim.x >= 2 * m) return;
     const float2* L = inv + f.inv + (long long)(k / MF_NB) * 2 * MF_NB * MF_NB;
     for (int t = threadIdx.x; t < MF_NB * MF_NB; t += blockDim.x) { Li[t] = L[t]; Ui[t] = L[MF_NB * MF_NB + t]; }
-    if (threadIdx.x < MF_NB) P[threadIdx.x] = threadIdx.x < kb ? piv[f.piv + k + threadIdx.x] : threadIdx.x;
     __syncthreads();
     if (item >= 2 * m) return;
     const long long ld = f.n;
@@ -222,14 +234,6 @@ __global__ void __launch_bounds__(256) mf_panel_kernel(const int* __restrict__ l
     if (item < m) {
         long long c = k + kb + item;
         float2* col = W + k + c * ld;
-        for (int j = 0; j < kb; j++) {           // this thread owns the column: swap in place
-            int r = P[j];
-            if (r != j) {
-                float2 t = col[j];
-                col[j] = col[r];
-                col[r] = t;
-            }
-        }
 #pragma unroll
         for (int i = 0; i < MF_NB; i++) v[i] = i < kb ? col[i] : make_float2(0.f, 0.f);
 #pragma unroll
@@ -237,7 +241,7 @@ __global__ void __launch_bounds__(256) mf_panel_kernel(const int* __restrict__ l
             if (i < kb) {
                 float2 s = make_float2(0.f, 0.f);
 #pragma unroll
-                for (int t = 0; t < MF_NB; t++) cfma(s, Li[i + t * MF_NB], v[t]);
+                for (int t = 0; t < MF_NB; t++) cfma(s, Li[i + t * MF_NB], v[t]);   // (Linv P) times the column
                 col[i] = s;
             }
         }
@@ -384,80 +388,99 @@ __global__ void mf_fwd_ea_kernel(const int* __restrict__ lst, const FrontMeta* _
     }
 }
 
-// Forward solve inside the 256-row block [k0, k0 + 256) of the own rows: for each 32-step, swaps,
-// y = Linv w, and the update of the block's remaining rows.  One CTA per front.
+// Forward solve inside the 256-row block [k0, k1) of the own rows, held in shared memory: for each
+// 32-step y = (Linv P) w_step, then the block's remaining rows.  One CTA per front, 16 right-hand sides
+// at a time.
+constexpr int MF_SC = 16;
 __global__ void __launch_bounds__(256) mf_fwd_block_kernel(const int* __restrict__ lst, const FrontMeta* __restrict__ fm,
                                                            int S, int k0, const float2* __restrict__ fact,
-                                                           const float2* __restrict__ inv, const int* __restrict__ piv,
-                                                           float2* __restrict__ w) {
-    __shared__ float2 y[MF_NB * 64];
+                                                           const float2* __restrict__ inv, float2* __restrict__ w) {
+    __shared__ float2 wb[MF_SB][MF_SC];
+    __shared__ float2 y[MF_NB][MF_SC];
     const FrontMeta& f = fm[lst[blockIdx.x]];
     if (k0 >= f.e) return;
     const int k1 = min(k0 + MF_SB, f.e);
+    const int rows = k1 - k0;
     const long long n = f.n;
     float2* W = w + f.wv * S;
     const float2* F = fact + f.fact;
     const int tid = threadIdx.x;
-    for (int k = k0; k < k1; k += MF_NB) {
-        const int kb = min(MF_NB, f.e - k);
-        const int* P = piv + f.piv + k;
-        // row swaps (sequential in j), one thread per right-hand side
-        if (tid < S) {
-            for (int j = 0; j < kb; j++) {
-                int r = P[j];
-                if (r != j) {
-                    float2 t = W[(long long)(k + j) * S + tid];
-                    W[(long long)(k + j) * S + tid] = W[(long long)(k + r) * S + tid];
-                    W[(long long)(k + r) * S + tid] = t;
-                }
-            }
-        }
+    for (int sc = 0; sc < S; sc += MF_SC) {
+        const int ns = min(MF_SC, S - sc);
+        for (int t = tid; t < rows * ns; t += blockDim.x) wb[t / ns][t % ns] = W[(long long)(k0 + t / ns) * S + sc + t % ns];
         __syncthreads();
-        const float2* Li = inv + f.inv + (long long)(k / MF_NB) * 2 * MF_NB * MF_NB;
-        for (int sc = 0; sc < S; sc += 64) {
-            const int ns = min(64, S - sc);
+        for (int k = k0; k < k1; k += MF_NB) {
+            const int kb = min(MF_NB, f.e - k);
+            const float2* Li = inv + f.inv + (long long)(k / MF_NB) * 2 * MF_NB * MF_NB;
             for (int t = tid; t < kb * ns; t += blockDim.x) {
-                int i = t / ns, s = t % ns;
+                int i = t / ns, sj = t % ns;
                 float2 acc = make_float2(0.f, 0.f);
-                for (int c = 0; c <= i; c++) cfma(acc, Li[i + c * MF_NB], W[(long long)(k + c) * S + sc + s]);
-                y[i * 64 + s] = acc;
+                for (int c = 0; c < kb; c++) cfma(acc, Li[i + c * MF_NB], wb[k - k0 + c][sj]);
+                y[i][sj] = acc;
             }
             __syncthreads();
-            for (int t = tid; t < kb * ns; t += blockDim.x) {
-                int i = t / ns, s = t % ns;
-                W[(long long)(k + i) * S + sc + s] = y[i * 64 + s];
-            }
-            // remaining rows of this 256-block
-            for (long long t = tid; t < (long long)(k1 - k - kb) * ns; t += blockDim.x) {
-                long long r = k + kb + t / ns;
-                int s = (int)(t % ns);
-                float2 acc = W[r * S + sc + s];
-                for (int c = 0; c < kb; c++) cfms(acc, F[r + (long long)(k + c) * n], y[c * 64 + s]);
-                W[r * S + sc + s] = acc;
+            for (int t = tid; t < kb * ns; t += blockDim.x) wb[k - k0 + t / ns][t % ns] = y[t / ns][t % ns];
+            for (int t = tid; t < (k1 - k - kb) * ns; t += blockDim.x) {
+                int r = k + kb + t / ns, sj = t % ns;
+                float2 acc = wb[r - k0][sj];
+                for (int c = 0; c < kb; c++) cfms(acc, F[r + (long long)(k + c) * n], y[c][sj]);
+                wb[r - k0][sj] = acc;
             }
             __syncthreads();
+        }
+        for (int t = tid; t < rows * ns; t += blockDim.x) W[(long long)(k0 + t / ns) * S + sc + t % ns] = wb[t / ns][t % ns];
+        __syncthreads();
+    }
+}
+
+// w[r] -= sum_{c in [c0, c1)} M[r, c] x[c] for the rows [r0, r1) of a front, M column-major with leading
+// dimension ldm, x = rows c of w (or of xsrc).  A CTA owns 32 rows; its 8 warps take every 8th column
+// and their sums meet in shared memory.  8 right-hand sides per CTA (grid.z).
+__device__ __forceinline__ void mf_gemv_rows(float2* W, int S, long long r, int rl, int g, bool live, const float2* M,
+                                             long long ldm, long long c0, long long c1, const float2* X,
+                                             long long xrow0, int s0, int ns, float2 (*red)[32][8]) {
+    float2 acc[8];
+#pragma unroll
+    for (int q = 0; q < 8; q++) acc[q] = make_float2(0.f, 0.f);
+    if (live) {
+        for (long long c = c0 + g; c < c1; c += 8) {
+            float2 mv = M[r + c * ldm];
+            const float2* xc = X + (xrow0 + c - c0) * S + s0;
+#pragma unroll
+            for (int q = 0; q < 8; q++)
+                if (q < ns) cfma(acc[q], mv, xc[q]);
+        }
+    }
+#pragma unroll
+    for (int q = 0; q < 8; q++) red[g][rl][q] = acc[q];
+    __syncthreads();
+    if (g == 0 && live) {
+        for (int q = 0; q < ns; q++) {
+            float2 t = make_float2(0.f, 0.f);
+#pragma unroll
+            for (int gg = 0; gg < 8; gg++) { t.x += red[gg][rl][q].x; t.y += red[gg][rl][q].y; }
+            float2* p = W + r * S + s0 + q;
+            p->x -= t.x;
+            p->y -= t.y;
         }
     }
 }
 
-// Rows [k1, n) of every front: w[r] -= L[r, k0:k1] y[k0:k1]   (one thread per (row, rhs))
+// Rows [k1, n) of every front: w[r] -= L[r, k0:k1] y[k0:k1]
 __global__ void __launch_bounds__(256) mf_fwd_update_kernel(const int* __restrict__ lst, const FrontMeta* __restrict__ fm,
                                                             int S, int k0, const float2* __restrict__ fact,
                                                             float2* __restrict__ w) {
+    __shared__ float2 red[8][32][8];
     const FrontMeta& f = fm[lst[blockIdx.y]];
     if (k0 >= f.e) return;
     const int k1 = min(k0 + MF_SB, f.e);
-    const long long rows = f.n - k1;
-    long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= rows * S) return;
-    long long r = k1 + t / S;
-    int s = (int)(t % S);
+    const long long r0 = k1 + (long long)blockIdx.x * 32;
+    if (r0 >= f.n) return;
+    const int s0 = blockIdx.z * 8, ns = min(8, S - s0);
+    const int rl = threadIdx.x % 32, g = threadIdx.x / 32;
+    const long long r = r0 + rl;
     float2* W = w + f.wv * S;
-    const float2* F = fact + f.fact;
-    const long long n = f.n;
-    float2 acc = W[r * S + s];
-    for (int c = k0; c < k1; c++) cfms(acc, F[r + (long long)c * n], W[(long long)c * S + s]);
-    W[r * S + s] = acc;
+    mf_gemv_rows(W, S, r, rl, g, r < f.n, fact + f.fact, f.n, k0, k1, W, k0, s0, ns, red);
 }
 
 // own rows -> y store, boundary rows -> update vector for the parent
@@ -494,61 +517,63 @@ __global__ void mf_bwd_gather_kernel(const int* __restrict__ lst, const FrontMet
     }
 }
 
-// own rows: w[r] -= U12[r, :] x_bnd   (U12 is e x b, column-major with ld e)
+// own rows: w[r] -= U12[r, :] x_bnd   (U12 is e x b, column-major with ld e; x_bnd = rows e.. of w)
 __global__ void __launch_bounds__(256) mf_bwd_bnd_kernel(const int* __restrict__ lst, const FrontMeta* __restrict__ fm,
                                                          int S, const float2* __restrict__ fact, float2* __restrict__ w) {
+    __shared__ float2 red[8][32][8];
     const FrontMeta& f = fm[lst[blockIdx.y]];
-    long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= (long long)f.e * S || f.b == 0) return;
-    long long r = t / S;
-    int s = (int)(t % S);
+    if (f.b == 0) return;
+    const long long r0 = (long long)blockIdx.x * 32;
+    if (r0 >= f.e) return;
+    const int s0 = blockIdx.z * 8, ns = min(8, S - s0);
+    const int rl = threadIdx.x % 32, g = threadIdx.x / 32;
+    const long long r = r0 + rl;
     float2* W = w + f.wv * S;
-    const float2* U12 = fact + f.fact + (long long)f.n * f.e;
-    float2 acc = W[r * S + s];
-    for (long long c = 0; c < f.b; c++) cfms(acc, U12[r + c * f.e], W[(f.e + c) * S + s]);
-    W[r * S + s] = acc;
+    mf_gemv_rows(W, S, r, rl, g, r < f.e, fact + f.fact + (long long)f.n * f.e, f.e, 0, f.b, W, f.e, s0, ns, red);
 }
 
-// Backward solve inside the block [k0, k1): 32-steps from the last, x_k = Uinv (w_k), then the block's
-// earlier rows.  One CTA per front.
+// Backward solve inside the block [k0, k1), held in shared memory: 32-steps from the last,
+// x_k = Uinv (w_k), then the block's earlier rows.  One CTA per front, 16 right-hand sides at a time.
 __global__ void __launch_bounds__(256) mf_bwd_block_kernel(const int* __restrict__ lst, const FrontMeta* __restrict__ fm,
                                                            int S, int k0, const float2* __restrict__ fact,
                                                            const float2* __restrict__ inv, float2* __restrict__ w) {
-    __shared__ float2 xk[MF_NB * 64];
+    __shared__ float2 wb[MF_SB][MF_SC];
+    __shared__ float2 xk[MF_NB][MF_SC];
     const FrontMeta& f = fm[lst[blockIdx.x]];
     if (k0 >= f.e) return;
     const int k1 = min(k0 + MF_SB, f.e);
+    const int rows = k1 - k0;
     const long long n = f.n;
     float2* W = w + f.wv * S;
     const float2* F = fact + f.fact;
     const int tid = threadIdx.x;
-    const int nsteps = (k1 - k0 + MF_NB - 1) / MF_NB;
-    for (int st = nsteps - 1; st >= 0; st--) {
-        const int k = k0 + st * MF_NB;
-        const int kb = min(MF_NB, f.e - k);
-        const float2* Ui = inv + f.inv + (long long)(k / MF_NB) * 2 * MF_NB * MF_NB + MF_NB * MF_NB;
-        for (int sc = 0; sc < S; sc += 64) {
-            const int ns = min(64, S - sc);
+    const int nsteps = (rows + MF_NB - 1) / MF_NB;
+    for (int sc = 0; sc < S; sc += MF_SC) {
+        const int ns = min(MF_SC, S - sc);
+        for (int t = tid; t < rows * ns; t += blockDim.x) wb[t / ns][t % ns] = W[(long long)(k0 + t / ns) * S + sc + t % ns];
+        __syncthreads();
+        for (int st = nsteps - 1; st >= 0; st--) {
+            const int k = k0 + st * MF_NB;
+            const int kb = min(MF_NB, f.e - k);
+            const float2* Ui = inv + f.inv + (long long)(k / MF_NB) * 2 * MF_NB * MF_NB + MF_NB * MF_NB;
             for (int t = tid; t < kb * ns; t += blockDim.x) {
-                int i = t / ns, s = t % ns;
+                int i = t / ns, sj = t % ns;
                 float2 acc = make_float2(0.f, 0.f);
-                for (int c = i; c < kb; c++) cfma(acc, Ui[i + c * MF_NB], W[(long long)(k + c) * S + sc + s]);
-                xk[i * 64 + s] = acc;
+                for (int c = i; c < kb; c++) cfma(acc, Ui[i + c * MF_NB], wb[k - k0 + c][sj]);
+                xk[i][sj] = acc;
             }
             __syncthreads();
-            for (int t = tid; t < kb * ns; t += blockDim.x) {
-                int i = t / ns, s = t % ns;
-                W[(long long)(k + i) * S + sc + s] = xk[i * 64 + s];
-            }
-            for (long long t = tid; t < (long long)(k - k0) * ns; t += blockDim.x) {
-                long long r = k0 + t / ns;
-                int s = (int)(t % ns);
-                float2 acc = W[r * S + sc + s];
-                for (int c = 0; c < kb; c++) cfms(acc, F[r + (long long)(k + c) * n], xk[c * 64 + s]);
-                W[r * S + sc + s] = acc;
+            for (int t = tid; t < kb * ns; t += blockDim.x) wb[k - k0 + t / ns][t % ns] = xk[t / ns][t % ns];
+            for (int t = tid; t < (k - k0) * ns; t += blockDim.x) {
+                int r = k0 + t / ns, sj = t % ns;
+                float2 acc = wb[r - k0][sj];
+                for (int c = 0; c < kb; c++) cfms(acc, F[r + (long long)(k + c) * n], xk[c][sj]);
+                wb[r - k0][sj] = acc;
             }
             __syncthreads();
         }
+        for (int t = tid; t < rows * ns; t += blockDim.x) W[(long long)(k0 + t / ns) * S + sc + t % ns] = wb[t / ns][t % ns];
+        __syncthreads();
     }
 }
 
@@ -556,19 +581,17 @@ __global__ void __launch_bounds__(256) mf_bwd_block_kernel(const int* __restrict
 __global__ void __launch_bounds__(256) mf_bwd_update_kernel(const int* __restrict__ lst, const FrontMeta* __restrict__ fm,
                                                             int S, int k0, const float2* __restrict__ fact,
                                                             float2* __restrict__ w) {
+    __shared__ float2 red[8][32][8];
     const FrontMeta& f = fm[lst[blockIdx.y]];
     if (k0 >= f.e) return;
     const int k1 = min(k0 + MF_SB, f.e);
-    long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= (long long)k0 * S) return;
-    long long r = t / S;
-    int s = (int)(t % S);
+    const long long r0 = (long long)blockIdx.x * 32;
+    if (r0 >= k0) return;
+    const int s0 = blockIdx.z * 8, ns = min(8, S - s0);
+    const int rl = threadIdx.x % 32, g = threadIdx.x / 32;
+    const long long r = r0 + rl;
     float2* W = w + f.wv * S;
-    const float2* F = fact + f.fact;
-    const long long n = f.n;
-    float2 acc = W[r * S + s];
-    for (int c = k0; c < k1; c++) cfms(acc, F[r + (long long)c * n], W[(long long)c * S + s]);
-    W[r * S + s] = acc;
+    mf_gemv_rows(W, S, r, rl, g, r < k0, fact + f.fact, f.n, k0, k1, W, k0, s0, ns, red);
 }
 
 __global__ void mf_bwd_finish_kernel(const int* __restrict__ lst, const FrontMeta* __restrict__ fm, int S,
@@ -680,9 +703,10 @@ int mf_apply(emfem_mf_s* m, int S, const double2* r, double2* x, cudaStream_t s)
             dim3 ge(nblk(maxb * S, MF_CHUNK), ny);
             mf_fwd_ea_kernel<<<ge, 256, 0, s>>>(lst + y0, m->d_meta, S, 0, m->d_ea, m->suv, m->sw);
             mf_fwd_ea_kernel<<<ge, 256, 0, s>>>(lst + y0, m->d_meta, S, 1, m->d_ea, m->suv, m->sw);
+            const unsigned sz = (unsigned)((S + 7) / 8);
             for (int k0 = 0; k0 < m->lvl_max_e[L]; k0 += MF_SB) {
-                mf_fwd_block_kernel<<<ny, 256, 0, s>>>(lst + y0, m->d_meta, S, k0, m->fact, m->inv, m->piv, m->sw);
-                dim3 gu(nblk(maxn * S, 256), ny);      // rows [k1, n) of the widest front, at most n
+                mf_fwd_block_kernel<<<ny, 256, 0, s>>>(lst + y0, m->d_meta, S, k0, m->fact, m->inv, m->sw);
+                dim3 gu(nblk(maxn - k0, 32), ny, sz);      // rows [k1, n) of a front: at most n - k0
                 mf_fwd_update_kernel<<<gu, 256, 0, s>>>(lst + y0, m->d_meta, S, k0, m->fact, m->sw);
             }
             mf_fwd_finish_kernel<<<g, 256, 0, s>>>(lst + y0, m->d_meta, S, m->sw, m->sy, m->suv);
@@ -698,14 +722,15 @@ int mf_apply(emfem_mf_s* m, int S, const double2* r, double2* x, cudaStream_t s)
             const int ny = std::min(65535, nfl - y0);
             dim3 g(nblk(maxn * S, MF_CHUNK), ny);
             mf_bwd_gather_kernel<<<g, 256, 0, s>>>(lst + y0, m->d_meta, S, m->d_fdof, m->sy, m->sx, m->sw);
-            dim3 gb(nblk(maxe * S, 256), ny);
+            const unsigned sz = (unsigned)((S + 7) / 8);
+            dim3 gb(nblk(maxe, 32), ny, sz);
             mf_bwd_bnd_kernel<<<gb, 256, 0, s>>>(lst + y0, m->d_meta, S, m->fact, m->sw);
             const int nblocks = (int)((maxe + MF_SB - 1) / MF_SB);
             for (int bi = nblocks - 1; bi >= 0; bi--) {
                 const int k0 = bi * MF_SB;
                 mf_bwd_block_kernel<<<ny, 256, 0, s>>>(lst + y0, m->d_meta, S, k0, m->fact, m->inv, m->sw);
                 if (k0 > 0) {
-                    dim3 gu(nblk((long long)k0 * S, 256), ny);
+                    dim3 gu(nblk(k0, 32), ny, sz);
                     mf_bwd_update_kernel<<<gu, 256, 0, s>>>(lst + y0, m->d_meta, S, k0, m->fact, m->sw);
                 }
             }

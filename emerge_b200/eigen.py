@@ -116,7 +116,7 @@ def eigenmodes(sweep, nmodes: int = 4, target_k0: float = 1.0, tol: float = 1e-1
             raise RuntimeError(f"eigenmodes: inner solve at sigma={sigma:.6g} did not converge "
                                f"(relres {sol.relres.max():.2e} after {sol.iters.max()} iterations)")
         Q, _ = torch.linalg.qr(sol.x)
-        Q = Q.contiguous()
+        Q = (Q * free[:, None]).contiguous()       # Householder reflections spread rounding onto PEC rows
         EQ = spmv(sweep.E, Q, False)
         MQ = spmv(sweep.B, Q, True)
         Eh = (Q.conj().T @ EQ).cpu().numpy()

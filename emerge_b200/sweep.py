@@ -437,6 +437,51 @@ class FrequencySweep:
                               precond=precond, precision=precision, method=method, x0=x0,
                               raise_on_fail=raise_on_fail, systems=systems)
 
+    def direct_solver(self, leaf_tets: int = 64):
+        """The device multifrontal LU of this sweep's mesh (built once, on first use)."""
+        if getattr(self, "_lu", None) is None:
+            from .direct import DeviceLU
+            self._lu = DeviceLU(self, leaf_tets=leaf_tets)
+        return self._lu
+
+    def solve_direct(self, systems, window: int = 5, tol: float = 1e-8, maxit: int = 400) -> SolveResult:
+        """Every listed (frequency, port) system through the device LU, the GPU counterpart of the
+        reference's direct solve per frequency (``SolverSuperLU``, LU reused across the ports of a
+        frequency, ``MW/simjob.py:82-107``).  The distinct frequencies, ascending, are cut into windows of
+        ``window`` consecutive ones; each window's middle frequency is factored (complex64) and all systems
+        of the window are solved together by FP64 BiCGStab preconditioned with that factorization (at
+        the factored frequency a couple of refinement steps, at its neighbours a Krylov solve of the
+        shifted operator).  Results come back in the order of ``systems``; ``windows`` on the result lists
+        (factored frequency, systems, factor seconds, solve seconds, iterations) per window."""
+        lu = self.direct_solver()
+        freqs = sorted({f for f, _ in systems})
+        n = len(systems)
+        x = torch.zeros((self.n, n), dtype=torch.complex128, device=self.device)
+        status = np.zeros(n, dtype=np.int64)
+        iters = np.zeros(n, dtype=np.int64)
+        relres = np.zeros(n)
+        t0 = time.perf_counter()
+        log = []
+        for w0 in range(0, len(freqs), window):
+            wf = freqs[w0:w0 + window]
+            idx = [j for j, (f, _) in enumerate(systems) if f in set(wf)]
+            tf = time.perf_counter()
+            lu.factor(wf[len(wf) // 2])
+            tf = time.perf_counter() - tf
+            for c0 in range(0, len(idx), 64):
+                sub = idx[c0:c0 + 64]
+                r = self.solve_lu([systems[j] for j in sub], lu, tol=tol, maxit=maxit)
+                x[:, sub] = r.x
+                status[sub] = r.status
+                iters[sub] = r.iters
+                relres[sub] = r.relres
+                log.append(dict(factored=wf[len(wf) // 2], systems=len(sub), factor_seconds=tf,
+                                solve_seconds=r.seconds, iters=r.iters.tolist(), perturbed=lu.n_perturbed))
+                tf = 0.0
+        res = SolveResult(x, status, iters, relres, list(systems), time.perf_counter() - t0)
+        res.windows = log
+        return res
+
     def solve_lu(self, systems, lu, tol: float = 1e-8, maxit: int = 500, x0: torch.Tensor | None = None,
                  raise_on_fail: bool = False) -> SolveResult:
         """The listed (frequency, port) systems by FP64 BiCGStab right-preconditioned with the device LU

@@ -318,3 +318,25 @@ class BatchSweep:
     def sparams(self, g: int, res) -> dict:
         """S-parameters of mesh g's solved systems (``FrequencySweep.sparams``)."""
         return self.sweeps[g].sparams(res)
+
+
+def solve_meshes_partitioned(problems, systems, world_size: int | None = None, rank: int | None = None,
+                             **kw) -> list[list[dict]]:
+    """Many meshes' sweeps across the ranks of the process group: meshes are dealt by cost (DOFs x systems,
+    the work of one batched Krylov iteration over the mesh's systems), each rank solves its meshes in one
+    :class:`BatchSweep` call on its own GPU (keyword arguments passed to ``BatchSweep.solve``), and every
+    rank gets, per mesh in input order, one dict per system (status, iterations, FP64 relative residual)."""
+    from . import distributed
+    ws, rk = distributed.world()
+    ws = ws if world_size is None else world_size
+    rk = rk if rank is None else rank
+    items = list(range(len(problems)))
+    cost = [float(problems[i].field.n_field) * len(systems[i]) for i in items]
+    mine = [i for i, _ in distributed.partition(items, ws, rk, cost)]
+    local = []
+    if mine:
+        res = BatchSweep([problems[i] for i in mine]).solve([systems[i] for i in mine], **kw)
+        for i, r in zip(mine, res):
+            local.append((i, [{"status": int(r.status[j]), "iters": int(r.iters[j]), "relres": float(r.relres[j])}
+                              for j in range(len(systems[i]))]))
+    return distributed.gather(local, len(problems))

@@ -437,6 +437,52 @@ class FrequencySweep:
                               precond=precond, precision=precision, method=method, x0=x0,
                               raise_on_fail=raise_on_fail, systems=systems)
 
+    def solve_partitioned(self, systems, solver: str = "krylov", window: int = 5, world_size: int | None = None,
+                          rank: int | None = None, return_x: bool = False, **kw) -> list[dict]:
+        """Solve ``systems`` split across the ranks of the process group (one GPU each), as the reference's
+        frequency-parallel sweep does (``MW/microwave_3d.py:795-861``): ``solver="krylov"`` deals the
+        systems round-robin and solves each rank's share in batches of 64 (``solve``, keyword arguments
+        passed on); ``solver="direct"`` deals whole windows of ``window`` consecutive frequencies (one
+        factorization each, ``solve_direct``), balanced by their system count.  Returns, on every rank and
+        in the order of ``systems``, one dict per system: status, iterations, FP64 relative residual and,
+        with ``return_x``, the solution as a host array."""
+        from . import distributed
+        ws, rk = distributed.world()
+        ws = ws if world_size is None else world_size
+        rk = rk if rank is None else rank
+        systems = list(systems)
+
+        def pack(res, j):
+            d = {"status": int(res.status[j]), "iters": int(res.iters[j]), "relres": float(res.relres[j])}
+            if return_x:
+                d["x"] = res.x[:, j].cpu().numpy()
+            return d
+
+        if solver == "krylov":
+            def run(batch):
+                r = self.solve(batch, **kw)
+                return [pack(r, j) for j in range(len(batch))]
+            return distributed.run_partitioned(systems, run, ws, rk, batch=64)
+        if solver != "direct":
+            raise ValueError("solver must be 'krylov' or 'direct'")
+        freqs = sorted({f for f, _ in systems})
+        wins = [freqs[i:i + window] for i in range(0, len(freqs), window)]
+        members = [[j for j, (f, _) in enumerate(systems) if f in set(w)] for w in wins]
+
+        def run_windows(batch):
+            out = []
+            for idx in batch:
+                r = self.solve_direct([systems[j] for j in idx], window=window, **kw)
+                out.append([(j, pack(r, q)) for q, j in enumerate(idx)])
+            return out
+        per_win = distributed.run_partitioned(members, run_windows, ws, rk, batch=1,
+                                              cost=[len(m) for m in members])
+        result: list = [None] * len(systems)
+        for lst in per_win:
+            for j, d in lst:
+                result[j] = d
+        return result
+
     def direct_solver(self, leaf_tets: int = 64):
         """The device multifrontal LU of this sweep's mesh (built once, on first use)."""
         if getattr(self, "_lu", None) is None:

@@ -92,3 +92,22 @@ def test_lu_solves_a_cavity_where_block_jacobi_stalls(cuda):
     for j, f in enumerate(freqs):
         xr, _ = _oracle_solution(P, f, 0)
         assert np.linalg.norm(res.x[:, j].cpu().numpy() - xr) <= 1e-8 * np.linalg.norm(xr), f
+
+
+def test_partitioned_entry_points_on_one_rank(cuda):
+    """FrequencySweep.solve_partitioned (windows of the direct sweep, or Krylov batches) and the multi-mesh
+    solve_meshes_partitioned give, on a single rank, what the unpartitioned calls give."""
+    from emerge_b200.batch import solve_meshes_partitioned
+    P = problems.waveguide(nx=6, ny=3, nz=10)
+    sw = FrequencySweep(P)
+    systems = [(f, q) for f in (9e9, 9.5e9, 10e9, 10.5e9) for q in (0, 1)]
+    got = sw.solve_partitioned(systems, solver="direct", window=2, tol=1e-10)
+    ref = sw.solve_direct(systems, window=2, tol=1e-10)
+    assert [d["status"] for d in got] == [0] * len(systems)
+    assert [d["iters"] for d in got] == ref.iters.tolist()
+    got_k = sw.solve_partitioned(systems[:4], solver="krylov", tol=1e-8, precond="aux", return_x=True)
+    assert all(d["status"] == 0 and d["relres"] <= 1e-8 for d in got_k)
+    Ps = [problems.waveguide(nx=n, ny=3, nz=2 * n, seed=n) for n in (4, 6, 5)]
+    sl = [[(10e9, 0), (10e9, 1)] for _ in Ps]
+    out = solve_meshes_partitioned(Ps, sl, tol=1e-8, maxit=20000, precond="aux")
+    assert len(out) == 3 and all(d["status"] == 0 for per in out for d in per)

@@ -48,6 +48,14 @@ __device__ __forceinline__ void cfms(float2& c, float2 a, float2 b) {   // c -= 
     c.y = fmaf(-a.x, b.y, fmaf(-a.y, b.x, c.y));
 }
 __device__ __forceinline__ float cabs2(float2 a) { return a.x * a.x + a.y * a.y; }
+
+// 8-byte asynchronous global -> shared copies: a thread issues all of its copies before waiting once,
+// so a staging loop costs one memory round trip instead of one per element
+__device__ __forceinline__ void cp_async8(void* dst_smem, const void* src) {
+    unsigned d = (unsigned)__cvta_generic_to_shared(dst_smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 __device__ __forceinline__ float2 cinv(float2 a) {
     float d = 1.0f / cabs2(a);
     return make_float2(a.x * d, -a.y * d);
@@ -390,13 +398,23 @@ __global__ void mf_fwd_ea_kernel(const int* __restrict__ lst, const FrontMeta* _
 
 // Forward solve inside the 256-row block [k0, k1) of the own rows, held in shared memory: for each
 // 32-step y = (Linv P) w_step, then the block's remaining rows.  One CTA per front, 16 right-hand sides
-// at a time.
+// at a time.  Each step's inverse block and L panel (the block's rows below the step, 32 columns) are
+// first staged in shared memory with coalesced loads, so a step costs one global round trip.
 constexpr int MF_SC = 16;
+constexpr int MF_PAN = MF_SB - MF_NB;     // panel rows below a step inside the block
+struct MfBlockSmem {
+    float2 wb[MF_SB][MF_SC];
+    float2 y[MF_NB][MF_SC];
+    float2 li[MF_NB * MF_NB];
+    float2 pan[MF_PAN][MF_NB + 1];
+};
+constexpr size_t MF_BLOCK_SMEM = sizeof(MfBlockSmem);
+
 __global__ void __launch_bounds__(256) mf_fwd_block_kernel(const int* __restrict__ lst, const FrontMeta* __restrict__ fm,
                                                            int S, int k0, const float2* __restrict__ fact,
                                                            const float2* __restrict__ inv, float2* __restrict__ w) {
-    __shared__ float2 wb[MF_SB][MF_SC];
-    __shared__ float2 y[MF_NB][MF_SC];
+    extern __shared__ __align__(16) unsigned char mf_smem[];
+    MfBlockSmem& sm = *reinterpret_cast<MfBlockSmem*>(mf_smem);
     const FrontMeta& f = fm[lst[blockIdx.x]];
     if (k0 >= f.e) return;
     const int k1 = min(k0 + MF_SB, f.e);
@@ -407,28 +425,36 @@ __global__ void __launch_bounds__(256) mf_fwd_block_kernel(const int* __restrict
     const int tid = threadIdx.x;
     for (int sc = 0; sc < S; sc += MF_SC) {
         const int ns = min(MF_SC, S - sc);
-        for (int t = tid; t < rows * ns; t += blockDim.x) wb[t / ns][t % ns] = W[(long long)(k0 + t / ns) * S + sc + t % ns];
-        __syncthreads();
+        for (int t = tid; t < rows * ns; t += blockDim.x)
+            cp_async8(&sm.wb[t / ns][t % ns], &W[(long long)(k0 + t / ns) * S + sc + t % ns]);
         for (int k = k0; k < k1; k += MF_NB) {
             const int kb = min(MF_NB, f.e - k);
+            const int pr = k1 - k - kb;           // panel rows
             const float2* Li = inv + f.inv + (long long)(k / MF_NB) * 2 * MF_NB * MF_NB;
+            for (int t = tid; t < MF_NB * MF_NB; t += blockDim.x) cp_async8(&sm.li[t], &Li[t]);
+            for (int t = tid; t < pr * kb; t += blockDim.x) {
+                int c = t / pr, r = t - c * pr;   // consecutive threads: consecutive rows of one column
+                cp_async8(&sm.pan[r][c], &F[(k + kb + r) + (long long)(k + c) * n]);
+            }
+            cp_async_wait_all();
+            __syncthreads();
             for (int t = tid; t < kb * ns; t += blockDim.x) {
                 int i = t / ns, sj = t % ns;
                 float2 acc = make_float2(0.f, 0.f);
-                for (int c = 0; c < kb; c++) cfma(acc, Li[i + c * MF_NB], wb[k - k0 + c][sj]);
-                y[i][sj] = acc;
+                for (int c = 0; c < kb; c++) cfma(acc, sm.li[i + c * MF_NB], sm.wb[k - k0 + c][sj]);
+                sm.y[i][sj] = acc;
             }
             __syncthreads();
-            for (int t = tid; t < kb * ns; t += blockDim.x) wb[k - k0 + t / ns][t % ns] = y[t / ns][t % ns];
-            for (int t = tid; t < (k1 - k - kb) * ns; t += blockDim.x) {
-                int r = k + kb + t / ns, sj = t % ns;
-                float2 acc = wb[r - k0][sj];
-                for (int c = 0; c < kb; c++) cfms(acc, F[r + (long long)(k + c) * n], y[c][sj]);
-                wb[r - k0][sj] = acc;
+            for (int t = tid; t < kb * ns; t += blockDim.x) sm.wb[k - k0 + t / ns][t % ns] = sm.y[t / ns][t % ns];
+            for (int t = tid; t < pr * ns; t += blockDim.x) {
+                int r = t / ns, sj = t % ns;
+                float2 acc = sm.wb[k + kb - k0 + r][sj];
+                for (int c = 0; c < kb; c++) cfms(acc, sm.pan[r][c], sm.y[c][sj]);
+                sm.wb[k + kb - k0 + r][sj] = acc;
             }
             __syncthreads();
         }
-        for (int t = tid; t < rows * ns; t += blockDim.x) W[(long long)(k0 + t / ns) * S + sc + t % ns] = wb[t / ns][t % ns];
+        for (int t = tid; t < rows * ns; t += blockDim.x) W[(long long)(k0 + t / ns) * S + sc + t % ns] = sm.wb[t / ns][t % ns];
         __syncthreads();
     }
 }
@@ -443,6 +469,7 @@ __device__ __forceinline__ void mf_gemv_rows(float2* W, int S, long long r, int 
 #pragma unroll
     for (int q = 0; q < 8; q++) acc[q] = make_float2(0.f, 0.f);
     if (live) {
+#pragma unroll 8
         for (long long c = c0 + g; c < c1; c += 8) {
             float2 mv = M[r + c * ldm];
             const float2* xc = X + (xrow0 + c - c0) * S + s0;
@@ -533,12 +560,13 @@ __global__ void __launch_bounds__(256) mf_bwd_bnd_kernel(const int* __restrict__
 }
 
 // Backward solve inside the block [k0, k1), held in shared memory: 32-steps from the last,
-// x_k = Uinv (w_k), then the block's earlier rows.  One CTA per front, 16 right-hand sides at a time.
+// x_k = Uinv (w_k), then the block's earlier rows.  One CTA per front, 16 right-hand sides at a time;
+// each step's Uinv block and U panel (the block's rows above the step) staged in shared memory first.
 __global__ void __launch_bounds__(256) mf_bwd_block_kernel(const int* __restrict__ lst, const FrontMeta* __restrict__ fm,
                                                            int S, int k0, const float2* __restrict__ fact,
                                                            const float2* __restrict__ inv, float2* __restrict__ w) {
-    __shared__ float2 wb[MF_SB][MF_SC];
-    __shared__ float2 xk[MF_NB][MF_SC];
+    extern __shared__ __align__(16) unsigned char mf_smem[];
+    MfBlockSmem& sm = *reinterpret_cast<MfBlockSmem*>(mf_smem);
     const FrontMeta& f = fm[lst[blockIdx.x]];
     if (k0 >= f.e) return;
     const int k1 = min(k0 + MF_SB, f.e);
@@ -550,29 +578,37 @@ __global__ void __launch_bounds__(256) mf_bwd_block_kernel(const int* __restrict
     const int nsteps = (rows + MF_NB - 1) / MF_NB;
     for (int sc = 0; sc < S; sc += MF_SC) {
         const int ns = min(MF_SC, S - sc);
-        for (int t = tid; t < rows * ns; t += blockDim.x) wb[t / ns][t % ns] = W[(long long)(k0 + t / ns) * S + sc + t % ns];
-        __syncthreads();
+        for (int t = tid; t < rows * ns; t += blockDim.x)
+            cp_async8(&sm.wb[t / ns][t % ns], &W[(long long)(k0 + t / ns) * S + sc + t % ns]);
         for (int st = nsteps - 1; st >= 0; st--) {
             const int k = k0 + st * MF_NB;
             const int kb = min(MF_NB, f.e - k);
+            const int pr = k - k0;                // panel rows above the step
             const float2* Ui = inv + f.inv + (long long)(k / MF_NB) * 2 * MF_NB * MF_NB + MF_NB * MF_NB;
+            for (int t = tid; t < MF_NB * MF_NB; t += blockDim.x) cp_async8(&sm.li[t], &Ui[t]);
+            for (int t = tid; t < pr * kb; t += blockDim.x) {
+                int c = t / pr, r = t - c * pr;
+                cp_async8(&sm.pan[r][c], &F[(k0 + r) + (long long)(k + c) * n]);
+            }
+            cp_async_wait_all();
+            __syncthreads();
             for (int t = tid; t < kb * ns; t += blockDim.x) {
                 int i = t / ns, sj = t % ns;
                 float2 acc = make_float2(0.f, 0.f);
-                for (int c = i; c < kb; c++) cfma(acc, Ui[i + c * MF_NB], wb[k - k0 + c][sj]);
-                xk[i][sj] = acc;
+                for (int c = i; c < kb; c++) cfma(acc, sm.li[i + c * MF_NB], sm.wb[k - k0 + c][sj]);
+                sm.y[i][sj] = acc;
             }
             __syncthreads();
-            for (int t = tid; t < kb * ns; t += blockDim.x) wb[k - k0 + t / ns][t % ns] = xk[t / ns][t % ns];
-            for (int t = tid; t < (k - k0) * ns; t += blockDim.x) {
-                int r = k0 + t / ns, sj = t % ns;
-                float2 acc = wb[r - k0][sj];
-                for (int c = 0; c < kb; c++) cfms(acc, F[r + (long long)(k + c) * n], xk[c][sj]);
-                wb[r - k0][sj] = acc;
+            for (int t = tid; t < kb * ns; t += blockDim.x) sm.wb[k - k0 + t / ns][t % ns] = sm.y[t / ns][t % ns];
+            for (int t = tid; t < pr * ns; t += blockDim.x) {
+                int r = t / ns, sj = t % ns;
+                float2 acc = sm.wb[r][sj];
+                for (int c = 0; c < kb; c++) cfms(acc, sm.pan[r][c], sm.y[c][sj]);
+                sm.wb[r][sj] = acc;
             }
             __syncthreads();
         }
-        for (int t = tid; t < rows * ns; t += blockDim.x) W[(long long)(k0 + t / ns) * S + sc + t % ns] = wb[t / ns][t % ns];
+        for (int t = tid; t < rows * ns; t += blockDim.x) W[(long long)(k0 + t / ns) * S + sc + t % ns] = sm.wb[t / ns][t % ns];
         __syncthreads();
     }
 }
@@ -705,7 +741,7 @@ int mf_apply(emfem_mf_s* m, int S, const double2* r, double2* x, cudaStream_t s)
             mf_fwd_ea_kernel<<<ge, 256, 0, s>>>(lst + y0, m->d_meta, S, 1, m->d_ea, m->suv, m->sw);
             const unsigned sz = (unsigned)((S + 7) / 8);
             for (int k0 = 0; k0 < m->lvl_max_e[L]; k0 += MF_SB) {
-                mf_fwd_block_kernel<<<ny, 256, 0, s>>>(lst + y0, m->d_meta, S, k0, m->fact, m->inv, m->sw);
+                mf_fwd_block_kernel<<<ny, 256, MF_BLOCK_SMEM, s>>>(lst + y0, m->d_meta, S, k0, m->fact, m->inv, m->sw);
                 dim3 gu(nblk(maxn - k0, 32), ny, sz);      // rows [k1, n) of a front: at most n - k0
                 mf_fwd_update_kernel<<<gu, 256, 0, s>>>(lst + y0, m->d_meta, S, k0, m->fact, m->sw);
             }
@@ -728,7 +764,7 @@ int mf_apply(emfem_mf_s* m, int S, const double2* r, double2* x, cudaStream_t s)
             const int nblocks = (int)((maxe + MF_SB - 1) / MF_SB);
             for (int bi = nblocks - 1; bi >= 0; bi--) {
                 const int k0 = bi * MF_SB;
-                mf_bwd_block_kernel<<<ny, 256, 0, s>>>(lst + y0, m->d_meta, S, k0, m->fact, m->inv, m->sw);
+                mf_bwd_block_kernel<<<ny, 256, MF_BLOCK_SMEM, s>>>(lst + y0, m->d_meta, S, k0, m->fact, m->inv, m->sw);
                 if (k0 > 0) {
                     dim3 gu(nblk(k0, 32), ny, sz);
                     mf_bwd_update_kernel<<<gu, 256, 0, s>>>(lst + y0, m->d_meta, S, k0, m->fact, m->sw);
@@ -892,6 +928,12 @@ int emfem_mf_create(emfem_handle h, int64_t n, int n_fronts, const int32_t* e, c
     mk((void**)&m->ws, sizeof(float2) * ws_max);
     mk((void**)&m->upd, sizeof(float2) * upd_top);
     mk((void**)&m->d_npert, sizeof(int));
+    if (rc != EMFEM_OK) { mf_free(m); delete m; return rc; }
+    rc = check_cuda(cudaFuncSetAttribute(mf_fwd_block_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)MF_BLOCK_SMEM), "cudaFuncSetAttribute");
+    if (rc == EMFEM_OK)
+        rc = check_cuda(cudaFuncSetAttribute(mf_bwd_block_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)MF_BLOCK_SMEM), "cudaFuncSetAttribute");
     if (rc != EMFEM_OK) { mf_free(m); delete m; return rc; }
     *out = m;
     return EMFEM_OK;

@@ -286,22 +286,31 @@ __global__ void __launch_bounds__(256) mf_trail_kernel(const int* __restrict__ l
     const long long ld = f.n;
     float2* W = ws + f.ws;
     const int tid = threadIdx.x;
-    // A tile (64 rows x kb) and B tile (kb x 64 cols)
+    // A tile (64 rows x kb) and B tile (kb x 64 cols) by asynchronous copies; out-of-range parts zeroed
     for (int t = tid; t < MF_NB * MF_TILE; t += 256) {
         int rr = t % MF_TILE, kk = t / MF_TILE;
         long long r = r0 + rr;
-        As[kk][rr] = (kk < kb && r < f.n) ? W[r + (long long)(k + kk) * ld] : make_float2(0.f, 0.f);
+        if (kk < kb && r < f.n) cp_async8(&As[kk][rr], &W[r + (long long)(k + kk) * ld]);
+        else As[kk][rr] = make_float2(0.f, 0.f);
         int kk2 = t % MF_NB, cc = t / MF_NB;
         long long c = c0 + cc;
-        Bs[kk2][cc] = (kk2 < kb && c < f.n) ? W[(k + kk2) + c * ld] : make_float2(0.f, 0.f);
+        if (kk2 < kb && c < f.n) cp_async8(&Bs[kk2][cc], &W[(k + kk2) + c * ld]);
+        else Bs[kk2][cc] = make_float2(0.f, 0.f);
     }
-    __syncthreads();
     const int tx = tid % 16, ty = tid / 16;
+    // the thread's 16 C entries go straight into its accumulators while the tiles are in flight
     float2 acc[4][4];
 #pragma unroll
-    for (int i = 0; i < 4; i++)
+    for (int j = 0; j < 4; j++) {
+        long long c = c0 + ty + 16 * j;
 #pragma unroll
-        for (int j = 0; j < 4; j++) acc[i][j] = make_float2(0.f, 0.f);
+        for (int i = 0; i < 4; i++) {
+            long long r = r0 + tx + 16 * i;
+            acc[i][j] = (r < f.n && c < f.n) ? W[r + c * ld] : make_float2(0.f, 0.f);
+        }
+    }
+    cp_async_wait_all();
+    __syncthreads();
     for (int kk = 0; kk < kb; kk++) {
         float2 a[4], b[4];
 #pragma unroll
@@ -311,7 +320,7 @@ __global__ void __launch_bounds__(256) mf_trail_kernel(const int* __restrict__ l
 #pragma unroll
         for (int i = 0; i < 4; i++)
 #pragma unroll
-            for (int j = 0; j < 4; j++) cfma(acc[i][j], a[i], b[j]);
+            for (int j = 0; j < 4; j++) cfms(acc[i][j], a[i], b[j]);
     }
 #pragma unroll
     for (int j = 0; j < 4; j++) {
@@ -320,12 +329,7 @@ __global__ void __launch_bounds__(256) mf_trail_kernel(const int* __restrict__ l
 #pragma unroll
         for (int i = 0; i < 4; i++) {
             long long r = r0 + tx + 16 * i;
-            if (r >= f.n) continue;
-            float2* p = W + r + c * ld;
-            float2 v = *p;
-            v.x -= acc[i][j].x;
-            v.y -= acc[i][j].y;
-            *p = v;
+            if (r < f.n) W[r + c * ld] = acc[i][j];
         }
     }
 }

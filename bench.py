@@ -472,13 +472,17 @@ def sweep_section(P_cavity, cavity_systems: int, cavity_maxit: int, arm_names=SW
         "aux_jacobi_vs_plain_solves_per_s": ratio(auxj, plain),
         "device_lu_vs_plain_solves_per_s": ratio(arms.get("device_lu_c64_fp64_bicgstab", {}).get("solves_per_s"), plain)}}
     cav = {"workload": "the assembly workload (384 000 tets, 2 480 240 DOF, one TE10 port, PEC elsewhere): "
-                       f"{lu_windows} windows of {lu_window} consecutive frequencies of the 101 (2-6 GHz) through the "
+                       f"{'all' if lu_windows < 0 else lu_windows} windows of {lu_window} consecutive frequencies of the "
+                       "101 (2-6 GHz) through the "
                        "device LU to FP64 relative residual 1e-8; block Jacobi and the aux-space correction with "
                        "bounded iterations (neither reaches 1e-8 on this cavity)"}
-    if lu_windows > 0:
-        mid = len(P_cavity.freqs) // 2
-        f0 = mid - (lu_window * lu_windows) // 2
-        lu_sys = [(float(f), 0) for f in P_cavity.freqs[f0:f0 + lu_window * lu_windows]]
+    if lu_windows != 0:
+        if lu_windows < 0:            # every frequency of the sweep
+            lu_sys = [(float(f), 0) for f in P_cavity.freqs]
+        else:
+            mid = len(P_cavity.freqs) // 2
+            f0 = max(0, mid - (lu_window * lu_windows) // 2)
+            lu_sys = [(float(f), 0) for f in P_cavity.freqs[f0:f0 + lu_window * lu_windows]]
         cav["device_lu_c64_fp64_bicgstab"] = direct_measure(P_cavity, lu_sys, window=lu_window)
         import gc as _gc
         _gc.collect()
@@ -503,8 +507,9 @@ def main():
     ap.add_argument("--no-precision", action="store_true")
     ap.add_argument("--sweep-systems", type=int, default=4)
     ap.add_argument("--sweep-maxit", type=int, default=2000)
-    ap.add_argument("--lu-window", type=int, default=5, help="frequencies per device-LU factorization on the cavity")
-    ap.add_argument("--lu-windows", type=int, default=2, help="cavity windows timed (0: skip the device-LU arm)")
+    ap.add_argument("--lu-window", type=int, default=9, help="frequencies per device-LU factorization on the cavity")
+    ap.add_argument("--lu-windows", type=int, default=2,
+                    help="cavity windows timed (0: skip the device-LU arm, -1: all 101 frequencies)")
     ap.add_argument("--sweep-arms", default=",".join(SWEEP_ARMS),
                     help="comma-separated waveguide sweep arms to measure (default: all)")
     ap.add_argument("--no-cpu-baseline", action="store_true")

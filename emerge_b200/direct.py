@@ -393,3 +393,35 @@ class DeviceLU:
         x = torch.empty_like(b2)
         check(lib().emfem_mf_solve(self._p, b2.shape[1], ptr(b2), ptr(x)), "emfem_mf_solve")
         return x.reshape(b.shape)
+
+
+def _main(argv=None) -> None:
+    """``python -m emerge_b200.direct --cavity N``: build the N³ dielectric-loaded cavity's sweep, factor
+    its system at one frequency, apply the LU to that frequency's right-hand side once and print the
+    timings (one GPU)."""
+    import argparse
+    import json
+    import time
+    import torch
+    from . import problems
+    from .sweep import FrequencySweep
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--cavity", type=int, default=16, help="hex grid size of the cavity (40: 384 000 tets)")
+    ap.add_argument("--freq-index", type=int, default=50)
+    a = ap.parse_args(argv)
+    P = problems.cavity(n=a.cavity)
+    sw = FrequencySweep(P)
+    f = float(P.freqs[a.freq_index])
+    lu = DeviceLU(sw).factor(f)
+    b = sw.rhs([(f, 0)])
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    lu.solve(b)
+    torch.cuda.synchronize()
+    print(json.dumps({"tets": int(P.mesh.n_tets), "dof": int(sw.n), "fronts": lu.n_fronts, "levels": lu.n_levels,
+                      "factor_seconds": lu.seconds_factor, "flops": lu.flops, "device_gb": lu.device_bytes / 1e9,
+                      "solve_seconds": time.perf_counter() - t0, "perturbed_pivots": lu.n_perturbed}))
+
+
+if __name__ == "__main__":
+    _main()

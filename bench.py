@@ -488,8 +488,8 @@ def sweep_section(P_cavity, cavity_systems: int, cavity_maxit: int, arm_names=SW
         _gc.collect()
         import torch as _torch
         _torch.cuda.empty_cache()
-    cav_sys = [(float(f), 0) for f in P_cavity.freqs[:: max(1, len(P_cavity.freqs) // cavity_systems)][:cavity_systems]]
     if cavity_systems > 0:
+        cav_sys = [(float(f), 0) for f in P_cavity.freqs[:: max(1, len(P_cavity.freqs) // cavity_systems)][:cavity_systems]]
         cav["plain_block_jacobi_fp64"] = sweep_measure(P_cavity, cav_sys, cavity_maxit, "fp64", "block_jacobi")
         cav["aux_jacobi_fp64"] = sweep_measure(P_cavity, cav_sys, cavity_maxit, "fp64", "aux")
     out["cavity_384000_tets"] = cav

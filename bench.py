@@ -405,7 +405,8 @@ SWEEP_ARMS = ("plain_block_jacobi_fp64", "aux_jacobi_fp64", "aux_jacobi_mixed", 
               "device_lu_c64_fp64_bicgstab")
 
 
-def direct_measure(P, systems, window: int, tol: float = 1e-8, maxit: int = 400, sweep=None) -> dict:
+def direct_measure(P, systems, window: int, tol: float = 1e-8, maxit: int = 400, sweep=None,
+                   adaptive: bool = False) -> dict:
     """Solves/s of the device-LU sweep (``FrequencySweep.solve_direct``): per window of ``window``
     frequencies one complex64 multifrontal factorization at the middle frequency (K_f formed on the device)
     and FP64 BiCGStab preconditioned with it for every system of the window.  The timed region holds the
@@ -419,14 +420,15 @@ def direct_measure(P, systems, window: int, tol: float = 1e-8, maxit: int = 400,
     torch.cuda.synchronize()
     t_setup = time.perf_counter() - t0
     t0 = time.perf_counter()
-    res = sw.solve_direct(systems, window=window, tol=tol, maxit=maxit)
+    res = sw.solve_direct(systems, window=window, tol=tol, maxit=maxit, adaptive=adaptive)
     torch.cuda.synchronize()
     dt = time.perf_counter() - t0
     conv = int(((res.status == 0) & (res.relres <= tol)).sum())
     fac = [w["factor_seconds"] for w in res.windows if w["factor_seconds"] > 0]
     out = {"precision": "complex64 LU factors and triangular solves inside FP64 BiCGStab (FP64 residual)",
            "precond": "device multifrontal LU of the window's middle frequency", "method": "bicgstab",
-           "systems": len(systems), "window_frequencies": window, "converged": conv, "seconds": dt,
+           "systems": len(systems), "window_frequencies": window, "adaptive_windows": adaptive,
+           "converged": conv, "seconds": dt,
            "solves_per_s": conv / dt, "iters_max": int(res.iters.max()), "iters_mean": float(res.iters.mean()),
            "relres_max": float(res.relres.max()), "tol": tol, "maxit": maxit,
            "setup_seconds": t_setup, "setup_symbolic_seconds": lu.seconds_symbolic,
@@ -483,7 +485,8 @@ def sweep_section(P_cavity, cavity_systems: int, cavity_maxit: int, arm_names=SW
             mid = len(P_cavity.freqs) // 2
             f0 = max(0, mid - (lu_window * lu_windows) // 2)
             lu_sys = [(float(f), 0) for f in P_cavity.freqs[f0:f0 + lu_window * lu_windows]]
-        cav["device_lu_c64_fp64_bicgstab"] = direct_measure(P_cavity, lu_sys, window=lu_window)
+        cav["device_lu_c64_fp64_bicgstab"] = direct_measure(P_cavity, lu_sys, window=lu_window,
+                                                            adaptive=lu_windows < 0)
         import gc as _gc
         _gc.collect()
         import torch as _torch

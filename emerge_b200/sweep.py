@@ -490,15 +490,19 @@ class FrequencySweep:
             self._lu = DeviceLU(self, leaf_tets=leaf_tets)
         return self._lu
 
-    def solve_direct(self, systems, window: int = 5, tol: float = 1e-8, maxit: int = 400) -> SolveResult:
+    def solve_direct(self, systems, window: int = 5, tol: float = 1e-8, maxit: int = 400, adaptive: bool = False,
+                     iter_band: tuple = (20, 40), max_window: int = 15) -> SolveResult:
         """Every listed (frequency, port) system through the device LU, the GPU counterpart of the
         reference's direct solve per frequency (``SolverSuperLU``, LU reused across the ports of a
         frequency, ``MW/simjob.py:82-107``).  The distinct frequencies, ascending, are cut into windows of
         ``window`` consecutive ones; each window's middle frequency is factored (complex64) and all systems
         of the window are solved together by FP64 BiCGStab preconditioned with that factorization (at
         the factored frequency a couple of refinement steps, at its neighbours a Krylov solve of the
-        shifted operator).  Results come back in the order of ``systems``; ``windows`` on the result lists
-        (factored frequency, systems, factor seconds, solve seconds, iterations) per window."""
+        shifted operator).  With ``adaptive``, each window's width follows the previous one's largest
+        iteration count: wider by 2 below ``iter_band[0]``, narrower by 2 above ``iter_band[1]`` (between 3
+        and ``max_window``), since the shifted systems at a window's edges need more iterations where the
+        cavity's modes are denser.  Results come back in the order of ``systems``; ``windows`` on the
+        result lists (factored frequency, systems, factor seconds, solve seconds, iterations) per window."""
         lu = self.direct_solver()
         freqs = sorted({f for f, _ in systems})
         n = len(systems)
@@ -508,9 +512,12 @@ class FrequencySweep:
         relres = np.zeros(n)
         t0 = time.perf_counter()
         log = []
-        for w0 in range(0, len(freqs), window):
-            wf = freqs[w0:w0 + window]
+        w0, W = 0, window
+        while w0 < len(freqs):
+            wf = freqs[w0:w0 + W]
+            w0 += len(wf)
             idx = [j for j, (f, _) in enumerate(systems) if f in set(wf)]
+            imax = 0
             tf = time.perf_counter()
             lu.factor(wf[len(wf) // 2])
             tf = time.perf_counter() - tf
@@ -524,6 +531,12 @@ class FrequencySweep:
                 log.append(dict(factored=wf[len(wf) // 2], systems=len(sub), factor_seconds=tf,
                                 solve_seconds=r.seconds, iters=r.iters.tolist(), perturbed=lu.n_perturbed))
                 tf = 0.0
+                imax = max(imax, int(r.iters.max()))
+            if adaptive:
+                if imax > iter_band[1] and W > 3:
+                    W = max(3, W - 2)
+                elif imax < iter_band[0] and W < max_window:
+                    W = min(max_window, W + 2)
         res = SolveResult(x, status, iters, relres, list(systems), time.perf_counter() - t0)
         res.windows = log
         return res

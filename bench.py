@@ -401,6 +401,90 @@ def batch_section(n_meshes: int = 64, seed: int = 7, reps: int = 3) -> dict:
     return out
 
 
+def configs_sweep_section(n_meshes: int = 16, tol: float = 1e-8) -> dict:
+    """Configurations 3 and 4 as sweeps (opt-in, ``--configs-sweeps``; minutes of GPU time).
+
+    Config 3: the first ``n_meshes`` of the 64 batched guides (``problems.batch_family``), 16 frequencies
+    each, port 1 excited: the batched aux-space Krylov solve over all of them in one grouped launch
+    (``BatchSweep``), then the device LU sweep (``solve_direct``, adaptive windows) for every system the
+    Krylov solve left above ``tol``.  Config 4: the substrate family at 40 x 30 x 26 x 6 = 187 200 tets,
+    all 51 frequencies through the device LU, and the FP64 aux-space Krylov solve at the frequencies
+    where it converges, with the relative difference of the two solutions per frequency."""
+    import torch
+    from emerge_b200 import problems
+    from emerge_b200.batch import BatchSweep
+    from emerge_b200.sweep import FrequencySweep
+    out = {}
+    Ps = problems.batch_family(64)[:n_meshes]
+    systems = [[(float(f), 0) for f in P.freqs] for P in Ps]
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    bs = BatchSweep(Ps)
+    rb = bs.solve(systems, tol=tol, maxit=6000, precond="aux")
+    torch.cuda.synchronize()
+    t_batch = time.perf_counter() - t0
+    conv_k = [int(((r.status == 0) & (r.relres <= tol)).sum()) for r in rb]
+    del bs
+    gc.collect()
+    t0 = time.perf_counter()
+    lu_conv, lu_setup, lu_sys = 0, 0.0, 0
+    for P, sl, r in zip(Ps, systems, rb):
+        bad = [sl[j] for j in np.flatnonzero((r.status != 0) | (r.relres > tol))]
+        if not bad:
+            continue
+        sw = FrequencySweep(P)
+        ts = time.perf_counter()
+        sw.direct_solver()
+        lu_setup += time.perf_counter() - ts
+        rd = sw.solve_direct(bad, window=5, tol=tol, adaptive=True)
+        lu_conv += int(((rd.status == 0) & (rd.relres <= tol)).sum())
+        lu_sys += len(bad)
+        del sw, rd
+        gc.collect()
+    torch.cuda.synchronize()
+    t_lu = time.perf_counter() - t0
+    n_sys = sum(len(sl) for sl in systems)
+    out["config3_batched_guides"] = {
+        "workload": f"{n_meshes} of the 64 batched guides ({sum(P.mesh.n_tets for P in Ps)} tets, "
+                    f"{min(P.mesh.n_tets for P in Ps)}-{max(P.mesh.n_tets for P in Ps)} each), 16 frequencies "
+                    "over each guide's TE10-TE20 band, port 1 excited, FP64 relative residual 1e-8",
+        "systems": n_sys, "krylov_aux_batched": {"seconds": t_batch, "converged": int(sum(conv_k))},
+        "device_lu_for_the_rest": {"systems": lu_sys, "converged": lu_conv, "seconds": t_lu,
+                                   "setup_seconds_in_it": lu_setup},
+        "converged_total": int(sum(conv_k)) + lu_conv,
+        "solves_per_s": (int(sum(conv_k)) + lu_conv) / (t_batch + t_lu)}
+    gc.collect()
+    torch.cuda.empty_cache()
+    Q = problems.substrate_box(40, 30, 26)
+    sw = FrequencySweep(Q)
+    sys4 = [(float(f), 0) for f in Q.freqs]
+    ts = time.perf_counter()
+    sw.direct_solver()
+    t_setup = time.perf_counter() - ts
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    rd = sw.solve_direct(sys4, window=9, tol=tol, adaptive=True)
+    torch.cuda.synchronize()
+    t_d = time.perf_counter() - t0
+    rk = sw.solve(sys4[-8:], tol=tol, maxit=30000, precond="aux")
+    diff = []
+    for j, (f, _) in enumerate(sys4[-8:]):
+        if rk.status[j] == 0:
+            xd = rd.x[:, len(sys4) - 8 + j]
+            diff.append((f, float(torch.linalg.vector_norm(rk.x[:, j] - xd) / torch.linalg.vector_norm(xd))))
+    out["config4_substrate_downsized"] = {
+        "workload": "substrate box 40x30x26 hex grid x6 (187 200 tets), eps_r 3.5-0.007j below the interface, "
+                    "PEC strip, lumped ports, order-2 ABC; all 51 frequencies 1-8 GHz, FP64 relative residual 1e-8",
+        "device_lu": {"converged": int(((rd.status == 0) & (rd.relres <= tol)).sum()), "systems": len(sys4),
+                      "seconds": t_d, "solves_per_s": int(((rd.status == 0) & (rd.relres <= tol)).sum()) / t_d,
+                      "setup_seconds": t_setup, "iters_max": int(rd.iters.max()),
+                      "relres_max": float(rd.relres.max()), "windows": len(rd.windows)},
+        "aux_krylov_top8_freqs": {"converged": int((rk.status == 0).sum()), "seconds": rk.seconds,
+                                  "iters_max": int(rk.iters.max())},
+        "lu_vs_aux_rel_diff_per_freq": diff}
+    return out
+
+
 SWEEP_ARMS = ("plain_block_jacobi_fp64", "aux_jacobi_fp64", "aux_jacobi_mixed", "learned_fp64", "learned_mixed",
               "device_lu_c64_fp64_bicgstab")
 
@@ -516,6 +600,8 @@ def main():
     ap.add_argument("--sweep-arms", default=",".join(SWEEP_ARMS),
                     help="comma-separated waveguide sweep arms to measure (default: all)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--configs-sweeps", action="store_true",
+                    help="also run configurations 3 and 4 as sweeps (several minutes of GPU time)")
     ap.add_argument("--grid", type=int, default=40, help="cavity hex grid size (40 = the 384 000-tet workload)")
     ap.add_argument("--variant", type=int, default=-1, help="assembly kernel variant (default: autotune)")
     args = ap.parse_args()
@@ -626,6 +712,7 @@ def main():
         batch = None if args.no_batch else batch_section()
         precision = None if args.no_precision else precision_section()
         batched_sweeps = None if args.no_batch else batched_sweep_section()
+        cfg = configs_sweep_section() if args.configs_sweeps else None
         cb = None if args.no_cpu_baseline else cpu_baseline(P)
         out = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
@@ -648,6 +735,7 @@ def main():
             "batched_meshes": batch,
             "precision_workload": precision,
             "batched_sweeps": batched_sweeps,
+            "configs_sweeps": cfg,
             "cpu_baseline": cb,
         }
         print(json.dumps(out), flush=True)

@@ -165,3 +165,51 @@ def with_modal_ports(P: Problem, freq: float, nmodes: int = 1, device=None) -> P
                    device=device)
         ports.append(mp)
     return dataclasses.replace(P, ports=ports)
+
+
+def batch_family(n_meshes: int = 64, seed: int = 7, nfreq: int = 16, aniso_fraction: float = 0.1) -> list:
+    """The batched-meshes workload as sweepable problems: ``n_meshes`` box meshes with seeded grid sizes
+    giving 5 000-200 000 tets each (the grid and size recipe of the batched assembly benchmark), per-tet
+    eps_r' ~ U[1,12] with tan d ~ U[0,5e-3], diagonal mu_r ~ U[1,2]^3 on a seeded ``aniso_fraction`` of
+    the tets.  The configuration names no excitation, so each box is a guide section: TE10 ports on the
+    z = 0 and z = l faces and PEC on the four side walls.  The analytic TE10 port assumes a homogeneous
+    filling, so the cell layer next to each port face holds the member's mean eps_r' (isotropic, same
+    loss) while every other tet keeps its own random tensors.  ``nfreq`` frequencies per member span its
+    first-mode band, 1.1 to 1.9 times the TE10 cutoff of the mean filling (below the TE20 cutoff)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(n_meshes):
+        target = rng.uniform(5000, 200000) / 6
+        nx = max(2, int(round(target ** (1 / 3) * rng.uniform(0.7, 1.3))))
+        ny = max(2, int(round((target / nx) ** 0.5 * rng.uniform(0.8, 1.2))))
+        nz = max(3, int(round(target / (nx * ny))))
+        a = 0.02 * rng.uniform(0.8, 1.25)
+        b, l = a * ny / nx, a * nz / nx
+        nodes, tets = box_tet_mesh(nx, ny, nz, a, b, l, jitter=0.1, seed=1000 + i)
+        mesh = TetMesh(nodes, tets)
+        fld = Nedelec2(mesh)
+        nt = mesh.n_tets
+        epr = rng.uniform(1, 12, nt)
+        tand = rng.uniform(0, 5e-3, nt)
+        aniso = rng.random(nt) < aniso_fraction
+        mu = np.where(aniso[None, :], rng.uniform(1, 2, (3, nt)), 1.0)
+        cz = nodes[2][tets].mean(axis=0)
+        feed = (cz < l / nz) | (cz > l - l / nz)
+        e_mean = float(epr.mean())
+        epr = np.where(feed, e_mean, epr)
+        mu = np.where(feed[None, :], 1.0, mu)
+        er = np.zeros((3, 3, nt), np.complex128)
+        ur = np.zeros((3, 3, nt), np.complex128)
+        for c in range(3):
+            er[c, c] = epr * (1 - 1j * tand)
+            ur[c, c] = mu[c]
+        ports = [RectangularWaveguidePort(1, PortFrame((a / 2, b / 2, 0.0)), (a, b), mesh.tris_on_plane(2, 0.0),
+                                          er=e_mean),
+                 RectangularWaveguidePort(2, PortFrame((a / 2, b / 2, l)), (a, b), mesh.tris_on_plane(2, l),
+                                          er=e_mean)]
+        walls = np.concatenate([mesh.tris_on_plane(0, 0.0), mesh.tris_on_plane(0, a),
+                                mesh.tris_on_plane(1, 0.0), mesh.tris_on_plane(1, b)])
+        fc = 299792458.0 / (2 * a * np.sqrt(e_mean))
+        out.append(Problem(f"batch_member_{i}", mesh, fld, er, ur, ports, walls,
+                           np.linspace(1.1 * fc, 1.9 * fc, nfreq), (a, b, l)))
+    return out

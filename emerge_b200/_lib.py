@@ -105,6 +105,7 @@ _SIGS = {
     "emfem_aux_set_rows": ([_vp, _i64, _vp, _i32, _vp], _i32),
     "emfem_point_field_dot": ([_vp, _i64, _vp, _i64, _vp, _vp, _i64, _i64, _vp, _vp, _vp, _i32, _vp, _vp], _i32),
     "emfem_mf_create": ([_vp, _i64, _i32, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, ctypes.POINTER(_vp)], _i32),
+    "emfem_mf_build_lists": ([_vp, _i64, _vp, _vp], _i32),
     "emfem_mf_info": ([_vp, ctypes.POINTER(ctypes.c_size_t), ctypes.POINTER(ctypes.c_double), _i32p], _i32),
     "emfem_mf_factor": ([_vp, _vp, _i32p], _i32),
     "emfem_mf_reserve": ([_vp, _i32], _i32),

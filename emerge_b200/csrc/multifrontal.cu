@@ -354,6 +354,65 @@ __global__ void mf_compact_kernel(const int* __restrict__ lst, const FrontMeta* 
     }
 }
 
+// ---------------------------------------------------------------- assembly lists on the device
+// Every CSR entry (r, c) of the free rows and columns belongs to the front that eliminates the earlier of
+// r and c; its local row/column is the DOF's own index there, or e + its index among the front's boundary
+// DOFs (sorted by elimination position: binary search).
+__device__ __forceinline__ int mf_local(const FrontMeta& f, int v, int d, int p, const int* __restrict__ fpos,
+                                        const long long* __restrict__ own0, const int* __restrict__ fdof,
+                                        const int* __restrict__ pos) {
+    if (fpos[p] == v) return (int)(p - own0[v]);
+    int lo = f.e, hi = f.n - 1;
+    const int* D = fdof + f.fdof;
+    while (lo < hi) {
+        int mid = (lo + hi) >> 1;
+        if (pos[D[mid]] < p) lo = mid + 1; else hi = mid;
+    }
+    return (lo < f.n && D[lo] == d) ? lo : -1;
+}
+
+__global__ void mf_list_count_kernel(long long n, const int* __restrict__ indptr, const int* __restrict__ indices,
+                                     const int* __restrict__ pos, const int* __restrict__ fpos, int* __restrict__ cnt) {
+    long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= n) return;
+    const int pr = pos[r];
+    if (pr < 0) return;
+    for (int k = indptr[r]; k < indptr[r + 1]; k++) {
+        const int pc = pos[indices[k]];
+        if (pc < 0) continue;
+        atomicAdd(&cnt[fpos[min(pr, pc)]], 1);
+    }
+}
+
+__global__ void mf_list_fill_kernel(long long n, const int* __restrict__ indptr, const int* __restrict__ indices,
+                                    const int* __restrict__ pos, const int* __restrict__ fpos,
+                                    const long long* __restrict__ own0, const FrontMeta* __restrict__ fm,
+                                    const int* __restrict__ fdof, const int* __restrict__ base, int* __restrict__ cur,
+                                    int* __restrict__ slot, int* __restrict__ off, int* __restrict__ status) {
+    long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= n) return;
+    const int pr = pos[r];
+    if (pr < 0) return;
+    for (int k = indptr[r]; k < indptr[r + 1]; k++) {
+        const int c = indices[k];
+        const int pc = pos[c];
+        if (pc < 0) continue;
+        const int v = fpos[min(pr, pc)];
+        const FrontMeta& f = fm[v];
+        const int li = mf_local(f, v, (int)r, pr, fpos, own0, fdof, pos);
+        const int lj = mf_local(f, v, c, pc, fpos, own0, fdof, pos);
+        const int q = base[v] + atomicAdd(&cur[v], 1);
+        if (li < 0 || lj < 0) {
+            flag(status, DEV_BAD_INDEX);
+            slot[q] = k;
+            off[q] = 0;
+            continue;
+        }
+        slot[q] = k;
+        off[q] = li + lj * f.n;
+    }
+}
+
 // ---------------------------------------------------------------- solve kernels
 // w (rows of the level's fronts, S per row): own rows from the right-hand side, boundary rows zero
 __global__ void mf_fwd_gather_kernel(const int* __restrict__ lst, const FrontMeta* __restrict__ fm, int S,
@@ -691,6 +750,9 @@ struct emfem_mf_s {
     float2 *sw = nullptr, *suv = nullptr, *sy = nullptr, *sx = nullptr;
     double flops = 0.0;
     bool factored = false;
+    bool lists = false;                           // assembly lists present (given or built)
+    std::vector<int> h_pos, h_fpos;               // host copies used to build the lists on the device
+    std::vector<long long> h_own0;
 };
 
 static void mf_free(emfem_mf_s* m) {
@@ -790,8 +852,10 @@ extern "C" {
 int emfem_mf_create(emfem_handle h, int64_t n, int n_fronts, const int32_t* e, const int32_t* b, const int32_t* parent,
                     const int32_t* level, const int64_t* fdof_ptr, const int32_t* fdof, const int32_t* ea,
                     const int64_t* asm_ptr, const int32_t* asm_slot, const int32_t* asm_off, emfem_mf* out) {
-    EMFEM_REQUIRE(h && n > 0 && n_fronts > 0 && e && b && parent && level && fdof_ptr && fdof && ea && asm_ptr &&
-                      asm_slot && asm_off && out, "emfem_mf_create: bad argument");
+    EMFEM_REQUIRE(h && n > 0 && n_fronts > 0 && e && b && parent && level && fdof_ptr && fdof && ea && out,
+                  "emfem_mf_create: bad argument");
+    EMFEM_REQUIRE((asm_ptr && asm_slot && asm_off) || (!asm_ptr && !asm_slot && !asm_off),
+                  "emfem_mf_create: give all three assembly arrays or none (then emfem_mf_build_lists)");
     auto* m = new emfem_mf_s();
     m->h = &h->h;
     m->n = n;
@@ -819,7 +883,7 @@ int emfem_mf_create(emfem_handle h, int64_t n, int n_fronts, const int32_t* e, c
         f.child[0] = f.child[1] = -1;
         f.fdof = fdof_ptr[v];
         f.ea = eao; eao += b[v];
-        f.asm0 = asm_ptr[v]; f.asm1 = asm_ptr[v + 1];
+        f.asm0 = asm_ptr ? asm_ptr[v] : 0; f.asm1 = asm_ptr ? asm_ptr[v + 1] : 0;
         f.fact = fact; fact += (long long)f.n * f.e + (long long)f.e * f.b;
         f.inv = inv; inv += (long long)((f.e + MF_NB - 1) / MF_NB) * 2 * MF_NB * MF_NB;
         f.piv = pivo; pivo += f.e;
@@ -908,7 +972,19 @@ int emfem_mf_create(emfem_handle h, int64_t n, int n_fronts, const int32_t* e, c
             if (d < 0 || d >= n) { delete m; set_error("emfem_mf_create: DOF %d out of range", d); return EMFEM_ERR_INVALID_ARG; }
             freed[d] = 1;
         }
-    long long nasm = asm_ptr[n_fronts];
+    long long nasm = asm_ptr ? asm_ptr[n_fronts] : 0;
+    m->lists = asm_ptr != nullptr;
+    // elimination position of every DOF, the front of every position, each front's first position
+    m->h_pos.assign(n, -1);
+    m->h_fpos.reserve((size_t)std::max<long long>(1, n));
+    m->h_own0.resize(n_fronts);
+    for (int v = 0; v < n_fronts; v++) {
+        m->h_own0[v] = (long long)m->h_fpos.size();
+        for (int i = 0; i < e[v]; i++) {
+            m->h_pos[fdof[fdof_ptr[v] + i]] = (int)m->h_fpos.size();
+            m->h_fpos.push_back(v);
+        }
+    }
     int rc = EMFEM_OK;
     auto up = [&](void** dst, const void* src, size_t bytes) {
         if (rc != EMFEM_OK) return;
@@ -954,6 +1030,7 @@ int emfem_mf_info(emfem_mf m, size_t* device_bytes, double* flops, int* n_levels
 
 int emfem_mf_factor(emfem_mf m, const void* K_vals, int* n_perturbed) {
     EMFEM_REQUIRE(m && K_vals, "emfem_mf_factor: bad argument");
+    EMFEM_REQUIRE(m->lists, "emfem_mf_factor: no assembly lists (emfem_mf_build_lists)");
     cudaStream_t s = m->h->stream;
     int prev = 0;
     EMFEM_CUDA(cudaGetDevice(&prev));
@@ -1000,6 +1077,68 @@ int emfem_mf_factor(emfem_mf m, const void* K_vals, int* n_perturbed) {
     }
     if (prev != m->h->device) cudaSetDevice(prev);
     return rc;
+}
+
+int emfem_mf_build_lists(emfem_mf m, int64_t nnz, const int32_t* indptr, const int32_t* indices) {
+    EMFEM_REQUIRE(m && indptr && indices && nnz > 0 && nnz < (1LL << 31), "emfem_mf_build_lists: bad argument");
+    EMFEM_REQUIRE(!m->lists, "emfem_mf_build_lists: the lists exist already");
+    cudaStream_t s = m->h->stream;
+    const long long n = m->n;
+    const int nf = m->nf;
+    int *d_pos = nullptr, *d_fpos = nullptr, *cnt = nullptr, *base = nullptr, *cur = nullptr, *scratch = nullptr;
+    long long* d_own0 = nullptr;
+    int rc = EMFEM_OK;
+    std::vector<int> hb(nf + 1);
+#define LTRY(x) do { rc = (x); if (rc != EMFEM_OK) goto done; } while (0)
+    LTRY(check_cuda(cudaMalloc(&d_pos, sizeof(int) * n), "cudaMalloc"));
+    LTRY(check_cuda(cudaMalloc(&d_fpos, sizeof(int) * std::max<size_t>(1, m->h_fpos.size())), "cudaMalloc"));
+    LTRY(check_cuda(cudaMalloc(&d_own0, sizeof(long long) * nf), "cudaMalloc"));
+    LTRY(check_cuda(cudaMalloc(&cnt, sizeof(int) * nf), "cudaMalloc"));
+    LTRY(check_cuda(cudaMalloc(&base, sizeof(int) * (nf + 1)), "cudaMalloc"));
+    LTRY(check_cuda(cudaMalloc(&cur, sizeof(int) * nf), "cudaMalloc"));
+    LTRY(check_cuda(cudaMalloc(&scratch, sizeof(int) * scan_scratch_ints(nf)), "cudaMalloc"));
+    LTRY(check_cuda(cudaMemcpyAsync(d_pos, m->h_pos.data(), sizeof(int) * n, cudaMemcpyHostToDevice, s), "copy"));
+    LTRY(check_cuda(cudaMemcpyAsync(d_fpos, m->h_fpos.data(), sizeof(int) * m->h_fpos.size(), cudaMemcpyHostToDevice, s), "copy"));
+    LTRY(check_cuda(cudaMemcpyAsync(d_own0, m->h_own0.data(), sizeof(long long) * nf, cudaMemcpyHostToDevice, s), "copy"));
+    LTRY(check_cuda(cudaMemsetAsync(cnt, 0, sizeof(int) * nf, s), "memset"));
+    LTRY(check_cuda(cudaMemsetAsync(cur, 0, sizeof(int) * nf, s), "memset"));
+    LTRY(check_cuda(cudaMemsetAsync(m->h->dev_status, 0, sizeof(int), s), "memset"));
+    mf_list_count_kernel<<<grid_for(n, 256), 256, 0, s>>>(n, indptr, indices, d_pos, d_fpos, cnt);
+    LTRY(check_cuda(cudaGetLastError(), "mf_list_count_kernel"));
+    LTRY(exclusive_scan_i32(m->h, cnt, base, nf, scratch));
+    LTRY(check_cuda(cudaMemcpyAsync(hb.data(), base, sizeof(int) * (nf + 1), cudaMemcpyDeviceToHost, s), "copy"));
+    LTRY(check_cuda(cudaStreamSynchronize(s), "sync"));
+    LTRY(check_cuda(cudaMalloc(&m->d_slot, sizeof(int) * std::max(1, hb[nf])), "cudaMalloc"));
+    LTRY(check_cuda(cudaMalloc(&m->d_off, sizeof(int) * std::max(1, hb[nf])), "cudaMalloc"));
+    mf_list_fill_kernel<<<grid_for(n, 256), 256, 0, s>>>(n, indptr, indices, d_pos, d_fpos, d_own0, m->d_meta, m->d_fdof,
+                                                          base, cur, m->d_slot, m->d_off, m->h->dev_status);
+    LTRY(check_cuda(cudaGetLastError(), "mf_list_fill_kernel"));
+    for (int v = 0; v < nf; v++) {
+        m->meta[v].asm0 = hb[v];
+        m->meta[v].asm1 = hb[v + 1];
+    }
+    for (size_t L = 0; L < m->levels.size(); L++) {
+        long long mx = 0;
+        for (int v : m->levels[L]) mx = std::max<long long>(mx, hb[v + 1] - hb[v]);
+        m->lvl_max_asm[L] = mx;
+    }
+    LTRY(check_cuda(cudaMemcpyAsync(m->d_meta, m->meta.data(), sizeof(FrontMeta) * nf, cudaMemcpyHostToDevice, s), "copy"));
+    {
+        int st = 0;
+        LTRY(check_cuda(cudaMemcpyAsync(&st, m->h->dev_status, sizeof(int), cudaMemcpyDeviceToHost, s), "copy"));
+        LTRY(check_cuda(cudaStreamSynchronize(s), "sync"));
+        if (st & DEV_BAD_INDEX) {
+            cudaMemsetAsync(m->h->dev_status, 0, sizeof(int), s);
+            set_error("emfem_mf_build_lists: a CSR entry's DOF is in neither the own nor the boundary set of its front");
+            rc = EMFEM_ERR_DEVICE_CHECK;
+            goto done;
+        }
+    }
+    m->lists = true;
+done:
+    cudaFree(d_pos); cudaFree(d_fpos); cudaFree(d_own0); cudaFree(cnt); cudaFree(base); cudaFree(cur); cudaFree(scratch);
+    return rc;
+#undef LTRY
 }
 
 int emfem_mf_reserve(emfem_mf m, int nrhs) {

@@ -93,6 +93,7 @@ def nested_dissection(ent: np.ndarray, n_entity: int, cen: np.ndarray, free: np.
     (entity X owns DOFs X and X + H)."""
     nt = ent.shape[1]
     owner = np.full(n_entity, -1, dtype=np.int64)       # tree node that eliminates each entity
+    stamp = np.full(n_entity, -1, dtype=np.int64)       # last node whose left half touched each entity
     nodes_tets: list[np.ndarray] = []
     nodes_own: list[np.ndarray] = []
     nodes_children: list[list[int]] = []
@@ -115,9 +116,10 @@ def nested_dissection(ent: np.ndarray, n_entity: int, cen: np.ndarray, free: np.
             nodes_own.append(u)
             continue
         left, right = _split(cen, tets)
-        el = np.unique(ent[:, left])
-        er = np.unique(ent[:, right])
-        sep = np.intersect1d(el, er, assume_unique=True)
+        # separator: entities touched by both halves (stamped by the left half, met again on the right)
+        stamp[ent[:, left]] = nid
+        er_ = ent[:, right].ravel()
+        sep = np.unique(er_[stamp[er_] == nid])
         sep = sep[owner[sep] < 0]
         owner[sep] = nid
         nodes_own.append(sep)
@@ -152,6 +154,7 @@ def nested_dissection(ent: np.ndarray, n_entity: int, cen: np.ndarray, free: np.
     # entities eliminated inside the subtree
     owner_new = np.where(owner >= 0, new_of_old[np.maximum(owner, 0)], -1)
     bnd_ent: list[np.ndarray] = [None] * n           # type: ignore[list-item]
+    mark = np.zeros(n_entity, dtype=bool)            # reused: set for a node's own entities, then cleared
     parent = np.full(n, -1, dtype=np.int64)
     level = np.zeros(n, dtype=np.int64)
     for old in post:
@@ -162,9 +165,9 @@ def nested_dissection(ent: np.ndarray, n_entity: int, cen: np.ndarray, free: np.
         tets = nodes_tets[old]
         own_u = nodes_own[old]
         if len(own_u):
-            mark = np.zeros(n_entity, dtype=bool)
             mark[own_u] = True
             touch = mark[ent[:, tets]].any(axis=0)
+            mark[own_u] = False
             adj = np.unique(ent[:, tets[touch]])
         else:
             adj = np.zeros(0, dtype=np.int64)
@@ -204,15 +207,17 @@ class FrontStructure:
     fdof: np.ndarray
     ea_ptr: np.ndarray
     ea: np.ndarray
-    asm_ptr: np.ndarray
-    asm_slot: np.ndarray
-    asm_off: np.ndarray
+    asm_ptr: np.ndarray | None
+    asm_slot: np.ndarray | None
+    asm_off: np.ndarray | None
     tree: EliminationTree
 
 
-def front_structure(tree: EliminationTree, indptr: np.ndarray, indices: np.ndarray) -> FrontStructure:
+def front_structure(tree: EliminationTree, indptr: np.ndarray | None, indices: np.ndarray | None,
+                    with_lists: bool = True) -> FrontStructure:
     """The front lists, extend-add maps and assembly lists of ``tree`` for the CSR pattern
-    (indptr, indices) of the full system (PEC rows and columns are skipped)."""
+    (indptr, indices) of the full system (PEC rows and columns are skipped).  Without ``with_lists`` the
+    assembly lists are left empty (``asm_ptr`` None) for the device to build (``emfem_mf_build_lists``)."""
     T = tree
     nf = T.n_nodes
     e = T.own_size().astype(np.int64)
@@ -253,6 +258,10 @@ def front_structure(tree: EliminationTree, indptr: np.ndarray, indices: np.ndarr
     has_par = T.parent[bfront] >= 0
     ea = np.full(len(T.bnd), -1, dtype=np.int64)
     ea[has_par] = local_index(T.parent[bfront[has_par]], T.bnd[has_par])
+    if not with_lists:
+        return FrontStructure(N, e.astype(np.int32), b.astype(np.int32), T.parent.astype(np.int32),
+                              T.level.astype(np.int32), fdof_ptr, fdof.astype(np.int32), ea_ptr, ea.astype(np.int32),
+                              None, None, None, T)
     # assembly lists from the CSR pattern (free rows and columns only)
     rows = np.repeat(np.arange(N, dtype=np.int64), np.diff(indptr))
     cols = indices.astype(np.int64)
@@ -284,7 +293,7 @@ class DeviceLU:
         import ctypes
         import time
         import torch
-        from ._lib import Handle, check, lib
+        from ._lib import Handle, check, lib, ptr
         from .sweep import _seg_from_keys
         t0 = time.perf_counter()
         P = sweep.problem
@@ -295,21 +304,20 @@ class DeviceLU:
         free = sweep.mask.cpu().numpy().astype(bool)
         cen = mesh.nodes[:, mesh.tets].mean(axis=1)
         self.tree = nested_dissection(fld.tet_to_field[:10], H, cen, free, H, leaf_tets=leaf_tets)
-        indptr, indices = sweep.plan.host_pattern()
-        S = front_structure(self.tree, indptr, indices)
+        S = front_structure(self.tree, None, None, with_lists=False)     # assembly lists: built on the device
         self.structure = S
         self.n_fronts = len(S.e)
         self.seconds_symbolic = time.perf_counter() - t0
         h = Handle.get(self.device)
         c = np.ascontiguousarray
         arrs = [c(S.e, np.int32), c(S.b, np.int32), c(S.parent, np.int32), c(S.level, np.int32),
-                c(S.fdof_ptr, np.int64), c(S.fdof, np.int32), c(S.ea, np.int32), c(S.asm_ptr, np.int64),
-                c(S.asm_slot, np.int32), c(S.asm_off, np.int32)]
-        self._host_arrays = arrs
+                c(S.fdof_ptr, np.int64), c(S.fdof, np.int32), c(S.ea, np.int32)]
         p = ctypes.c_void_p()
         check(lib().emfem_mf_create(h.h, sweep.n, self.n_fronts, *[a.ctypes.data_as(ctypes.c_void_p) for a in arrs],
-                                    ctypes.byref(p)), "emfem_mf_create")
+                                    None, None, None, ctypes.byref(p)), "emfem_mf_create")
         self._p = p
+        check(lib().emfem_mf_build_lists(p, sweep.plan.nnz, ptr(sweep.plan.indptr), ptr(sweep.plan.indices)),
+              "emfem_mf_build_lists")
         nb, fl, nl = ctypes.c_size_t(), ctypes.c_double(), ctypes.c_int()
         check(lib().emfem_mf_info(p, ctypes.byref(nb), ctypes.byref(fl), ctypes.byref(nl)), "emfem_mf_info")
         self.device_bytes, self.flops, self.n_levels = nb.value, fl.value, nl.value

@@ -368,7 +368,9 @@ int emfem_adam_step(emfem_handle h, int64_t n, float *params, const float *grad,
  *   fdof[fdof_ptr[v] .. fdof_ptr[v + 1]): the front's DOFs (own, then boundary, as CSR row numbers);
  *   ea: for every front in order, the position of each of its b boundary DOFs in its parent's front;
  *   asm_slot / asm_off (asm_ptr per front): the CSR slots assembled into each front and their local
- *   offsets row + col * (e + b).
+ *   offsets row + col * (e + b).  The three assembly arrays may all be NULL; then
+ *   emfem_mf_build_lists builds them on the device from the CSR pattern (device indptr (n + 1) and
+ *   indices (nnz), int32), which must come before the first factorization.
  * info: device bytes held, factorization flops, number of levels.
  * factor: K_vals (nnz c128, device) on the CSR pattern the structure was built for; *n_perturbed
  *   (host) gets the number of pivots raised to 1e-6 of their 32 x 32 block's largest entry (pivoting is
@@ -384,6 +386,7 @@ typedef struct emfem_mf_s *emfem_mf;
 int emfem_mf_create(emfem_handle h, int64_t n, int n_fronts, const int32_t *e, const int32_t *b, const int32_t *parent,
                     const int32_t *level, const int64_t *fdof_ptr, const int32_t *fdof, const int32_t *ea,
                     const int64_t *asm_ptr, const int32_t *asm_slot, const int32_t *asm_off, emfem_mf *out);
+int emfem_mf_build_lists(emfem_mf lu, int64_t nnz, const int32_t *indptr, const int32_t *indices);
 int emfem_mf_info(emfem_mf lu, size_t *device_bytes, double *flops, int *n_levels);
 int emfem_mf_factor(emfem_mf lu, const void *K_vals, int *n_perturbed);
 int emfem_mf_reserve(emfem_mf lu, int nrhs);

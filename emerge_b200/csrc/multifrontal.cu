@@ -56,6 +56,9 @@ __device__ __forceinline__ void cp_async8(void* dst_smem, const void* src) {
     asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(src) : "memory");
 }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+// wait until at most one committed group is still in flight
+__device__ __forceinline__ void cp_async_wait_1() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
 __device__ __forceinline__ float2 cinv(float2 a) {
     float d = 1.0f / cabs2(a);
     return make_float2(a.x * d, -a.y * d);
@@ -465,46 +468,67 @@ __global__ void mf_fwd_ea_kernel(const int* __restrict__ lst, const FrontMeta* _
 // first staged in shared memory with coalesced loads, so a step costs one global round trip.
 constexpr int MF_SC = 16;
 constexpr int MF_PAN = MF_SB - MF_NB;     // panel rows below a step inside the block
+template <int NBUF>
 struct MfBlockSmem {
     float2 wb[MF_SB][MF_SC];
     float2 y[MF_NB][MF_SC];
-    float2 li[MF_NB * MF_NB];
-    float2 pan[MF_PAN][MF_NB + 1];
+    float2 li[NBUF][MF_NB * MF_NB];
+    float2 pan[NBUF][MF_PAN][MF_NB + 1];
 };
-constexpr size_t MF_BLOCK_SMEM = sizeof(MfBlockSmem);
+constexpr size_t MF_BLOCK_SMEM = sizeof(MfBlockSmem<1>);
+constexpr size_t MF_BLOCK_SMEM2 = sizeof(MfBlockSmem<2>);
 
+// Stage step st's inverse block and panel (forward: rows below the step inside the block; backward: rows
+// above it) into buffer slot, as one committed group of asynchronous copies.
+__device__ __forceinline__ void mf_stage_step(float2* li, float2 (*pan)[MF_NB + 1], const float2* Ib,
+                                              const float2* F, long long n, int rbase, int pr, int kcol, int kb) {
+    for (int t = threadIdx.x; t < MF_NB * MF_NB; t += blockDim.x) cp_async8(&li[t], &Ib[t]);
+    for (int t = threadIdx.x; t < pr * kb; t += blockDim.x) {
+        int c = t / pr, r = t - c * pr;          // consecutive threads: consecutive rows of one column
+        cp_async8(&pan[r][c], &F[(rbase + r) + (long long)(kcol + c) * n]);
+    }
+    cp_async_commit();
+}
+
+template <int NBUF>
 __global__ void __launch_bounds__(256) mf_fwd_block_kernel(const int* __restrict__ lst, const FrontMeta* __restrict__ fm,
                                                            int S, int k0, const float2* __restrict__ fact,
                                                            const float2* __restrict__ inv, float2* __restrict__ w) {
     extern __shared__ __align__(16) unsigned char mf_smem[];
-    MfBlockSmem& sm = *reinterpret_cast<MfBlockSmem*>(mf_smem);
+    MfBlockSmem<NBUF>& sm = *reinterpret_cast<MfBlockSmem<NBUF>*>(mf_smem);
     const FrontMeta& f = fm[lst[blockIdx.x]];
     if (k0 >= f.e) return;
     const int k1 = min(k0 + MF_SB, f.e);
     const int rows = k1 - k0;
+    const int nsteps = (rows + MF_NB - 1) / MF_NB;
     const long long n = f.n;
     float2* W = w + f.wv * S;
     const float2* F = fact + f.fact;
     const int tid = threadIdx.x;
+    auto stage = [&](int st) {
+        const int k = k0 + st * MF_NB, kb = min(MF_NB, f.e - k);
+        mf_stage_step(sm.li[st % NBUF], sm.pan[st % NBUF], inv + f.inv + (long long)(k / MF_NB) * 2 * MF_NB * MF_NB,
+                      F, n, k + kb, k1 - k - kb, k, kb);
+    };
     for (int sc = 0; sc < S; sc += MF_SC) {
         const int ns = min(MF_SC, S - sc);
         for (int t = tid; t < rows * ns; t += blockDim.x)
             cp_async8(&sm.wb[t / ns][t % ns], &W[(long long)(k0 + t / ns) * S + sc + t % ns]);
-        for (int k = k0; k < k1; k += MF_NB) {
-            const int kb = min(MF_NB, f.e - k);
-            const int pr = k1 - k - kb;           // panel rows
-            const float2* Li = inv + f.inv + (long long)(k / MF_NB) * 2 * MF_NB * MF_NB;
-            for (int t = tid; t < MF_NB * MF_NB; t += blockDim.x) cp_async8(&sm.li[t], &Li[t]);
-            for (int t = tid; t < pr * kb; t += blockDim.x) {
-                int c = t / pr, r = t - c * pr;   // consecutive threads: consecutive rows of one column
-                cp_async8(&sm.pan[r][c], &F[(k + kb + r) + (long long)(k + c) * n]);
+        stage(0);
+        for (int st = 0; st < nsteps; st++) {
+            const int k = k0 + st * MF_NB, kb = min(MF_NB, f.e - k), pr = k1 - k - kb;
+            if (NBUF == 2 && st + 1 < nsteps) {
+                stage(st + 1);                   // the next step's copies fly while this step computes
+                cp_async_wait_1();
+            } else {
+                cp_async_wait_all();
             }
-            cp_async_wait_all();
             __syncthreads();
+            const float2* li = sm.li[st % NBUF];
             for (int t = tid; t < kb * ns; t += blockDim.x) {
                 int i = t / ns, sj = t % ns;
                 float2 acc = make_float2(0.f, 0.f);
-                for (int c = 0; c < kb; c++) cfma(acc, sm.li[i + c * MF_NB], sm.wb[k - k0 + c][sj]);
+                for (int c = 0; c < kb; c++) cfma(acc, li[i + c * MF_NB], sm.wb[k - k0 + c][sj]);
                 sm.y[i][sj] = acc;
             }
             __syncthreads();
@@ -512,10 +536,11 @@ __global__ void __launch_bounds__(256) mf_fwd_block_kernel(const int* __restrict
             for (int t = tid; t < pr * ns; t += blockDim.x) {
                 int r = t / ns, sj = t % ns;
                 float2 acc = sm.wb[k + kb - k0 + r][sj];
-                for (int c = 0; c < kb; c++) cfms(acc, sm.pan[r][c], sm.y[c][sj]);
+                for (int c = 0; c < kb; c++) cfms(acc, sm.pan[st % NBUF][r][c], sm.y[c][sj]);
                 sm.wb[k + kb - k0 + r][sj] = acc;
             }
             __syncthreads();
+            if (NBUF == 1 && st + 1 < nsteps) stage(st + 1);
         }
         for (int t = tid; t < rows * ns; t += blockDim.x) W[(long long)(k0 + t / ns) * S + sc + t % ns] = sm.wb[t / ns][t % ns];
         __syncthreads();
@@ -625,11 +650,12 @@ __global__ void __launch_bounds__(256) mf_bwd_bnd_kernel(const int* __restrict__
 // Backward solve inside the block [k0, k1), held in shared memory: 32-steps from the last,
 // x_k = Uinv (w_k), then the block's earlier rows.  One CTA per front, 16 right-hand sides at a time;
 // each step's Uinv block and U panel (the block's rows above the step) staged in shared memory first.
+template <int NBUF>
 __global__ void __launch_bounds__(256) mf_bwd_block_kernel(const int* __restrict__ lst, const FrontMeta* __restrict__ fm,
                                                            int S, int k0, const float2* __restrict__ fact,
                                                            const float2* __restrict__ inv, float2* __restrict__ w) {
     extern __shared__ __align__(16) unsigned char mf_smem[];
-    MfBlockSmem& sm = *reinterpret_cast<MfBlockSmem*>(mf_smem);
+    MfBlockSmem<NBUF>& sm = *reinterpret_cast<MfBlockSmem<NBUF>*>(mf_smem);
     const FrontMeta& f = fm[lst[blockIdx.x]];
     if (k0 >= f.e) return;
     const int k1 = min(k0 + MF_SB, f.e);
@@ -639,26 +665,31 @@ __global__ void __launch_bounds__(256) mf_bwd_block_kernel(const int* __restrict
     const float2* F = fact + f.fact;
     const int tid = threadIdx.x;
     const int nsteps = (rows + MF_NB - 1) / MF_NB;
+    // processing order j = 0.. runs the steps from the last (st = nsteps - 1 - j); buffers follow j
+    auto stage = [&](int j) {
+        const int k = k0 + (nsteps - 1 - j) * MF_NB, kb = min(MF_NB, f.e - k);
+        mf_stage_step(sm.li[j % NBUF], sm.pan[j % NBUF],
+                      inv + f.inv + (long long)(k / MF_NB) * 2 * MF_NB * MF_NB + MF_NB * MF_NB, F, n, k0, k - k0, k, kb);
+    };
     for (int sc = 0; sc < S; sc += MF_SC) {
         const int ns = min(MF_SC, S - sc);
         for (int t = tid; t < rows * ns; t += blockDim.x)
             cp_async8(&sm.wb[t / ns][t % ns], &W[(long long)(k0 + t / ns) * S + sc + t % ns]);
-        for (int st = nsteps - 1; st >= 0; st--) {
-            const int k = k0 + st * MF_NB;
-            const int kb = min(MF_NB, f.e - k);
-            const int pr = k - k0;                // panel rows above the step
-            const float2* Ui = inv + f.inv + (long long)(k / MF_NB) * 2 * MF_NB * MF_NB + MF_NB * MF_NB;
-            for (int t = tid; t < MF_NB * MF_NB; t += blockDim.x) cp_async8(&sm.li[t], &Ui[t]);
-            for (int t = tid; t < pr * kb; t += blockDim.x) {
-                int c = t / pr, r = t - c * pr;
-                cp_async8(&sm.pan[r][c], &F[(k0 + r) + (long long)(k + c) * n]);
+        stage(0);
+        for (int j = 0; j < nsteps; j++) {
+            const int k = k0 + (nsteps - 1 - j) * MF_NB, kb = min(MF_NB, f.e - k), pr = k - k0;
+            if (NBUF == 2 && j + 1 < nsteps) {
+                stage(j + 1);
+                cp_async_wait_1();
+            } else {
+                cp_async_wait_all();
             }
-            cp_async_wait_all();
             __syncthreads();
+            const float2* ui = sm.li[j % NBUF];
             for (int t = tid; t < kb * ns; t += blockDim.x) {
                 int i = t / ns, sj = t % ns;
                 float2 acc = make_float2(0.f, 0.f);
-                for (int c = i; c < kb; c++) cfma(acc, sm.li[i + c * MF_NB], sm.wb[k - k0 + c][sj]);
+                for (int c = i; c < kb; c++) cfma(acc, ui[i + c * MF_NB], sm.wb[k - k0 + c][sj]);
                 sm.y[i][sj] = acc;
             }
             __syncthreads();
@@ -666,10 +697,11 @@ __global__ void __launch_bounds__(256) mf_bwd_block_kernel(const int* __restrict
             for (int t = tid; t < pr * ns; t += blockDim.x) {
                 int r = t / ns, sj = t % ns;
                 float2 acc = sm.wb[r][sj];
-                for (int c = 0; c < kb; c++) cfms(acc, sm.pan[r][c], sm.y[c][sj]);
+                for (int c = 0; c < kb; c++) cfms(acc, sm.pan[j % NBUF][r][c], sm.y[c][sj]);
                 sm.wb[r][sj] = acc;
             }
             __syncthreads();
+            if (NBUF == 1 && j + 1 < nsteps) stage(j + 1);
         }
         for (int t = tid; t < rows * ns; t += blockDim.x) W[(long long)(k0 + t / ns) * S + sc + t % ns] = sm.wb[t / ns][t % ns];
         __syncthreads();
@@ -807,8 +839,11 @@ int mf_apply(emfem_mf_s* m, int S, const double2* r, double2* x, cudaStream_t s)
             mf_fwd_ea_kernel<<<ge, 256, 0, s>>>(lst + y0, m->d_meta, S, 1, m->d_ea, m->suv, m->sw);
             const unsigned sz = (unsigned)((S + 7) / 8);
             for (int k0 = 0; k0 < m->lvl_max_e[L]; k0 += MF_SB) {
-                mf_fwd_block_kernel<<<ny, 256, MF_BLOCK_SMEM, s>>>(lst + y0, m->d_meta, S, k0, m->fact, m->inv, m->sw);
-                dim3 gu(nblk(maxn - k0, 32), ny, sz);      // rows [k1, n) of a front: at most n - k0
+                if (ny < 148)   // a few large fronts: the serial step chain, so overlap its copies
+                    mf_fwd_block_kernel<2><<<ny, 256, MF_BLOCK_SMEM2, s>>>(lst + y0, m->d_meta, S, k0, m->fact, m->inv, m->sw);
+                else
+                    mf_fwd_block_kernel<1><<<ny, 256, MF_BLOCK_SMEM, s>>>(lst + y0, m->d_meta, S, k0, m->fact, m->inv, m->sw);
+                dim3 gu(nblk(maxn - k0, 32), ny, sz);   // rows [k1, n) of a front: at most n - k0
                 mf_fwd_update_kernel<<<gu, 256, 0, s>>>(lst + y0, m->d_meta, S, k0, m->fact, m->sw);
             }
             mf_fwd_finish_kernel<<<g, 256, 0, s>>>(lst + y0, m->d_meta, S, m->sw, m->sy, m->suv);
@@ -830,7 +865,10 @@ int mf_apply(emfem_mf_s* m, int S, const double2* r, double2* x, cudaStream_t s)
             const int nblocks = (int)((maxe + MF_SB - 1) / MF_SB);
             for (int bi = nblocks - 1; bi >= 0; bi--) {
                 const int k0 = bi * MF_SB;
-                mf_bwd_block_kernel<<<ny, 256, MF_BLOCK_SMEM, s>>>(lst + y0, m->d_meta, S, k0, m->fact, m->inv, m->sw);
+                if (ny < 148)
+                    mf_bwd_block_kernel<2><<<ny, 256, MF_BLOCK_SMEM2, s>>>(lst + y0, m->d_meta, S, k0, m->fact, m->inv, m->sw);
+                else
+                    mf_bwd_block_kernel<1><<<ny, 256, MF_BLOCK_SMEM, s>>>(lst + y0, m->d_meta, S, k0, m->fact, m->inv, m->sw);
                 if (k0 > 0) {
                     dim3 gu(nblk(k0, 32), ny, sz);
                     mf_bwd_update_kernel<<<gu, 256, 0, s>>>(lst + y0, m->d_meta, S, k0, m->fact, m->sw);
@@ -1009,11 +1047,17 @@ int emfem_mf_create(emfem_handle h, int64_t n, int n_fronts, const int32_t* e, c
     mk((void**)&m->upd, sizeof(float2) * upd_top);
     mk((void**)&m->d_npert, sizeof(int));
     if (rc != EMFEM_OK) { mf_free(m); delete m; return rc; }
-    rc = check_cuda(cudaFuncSetAttribute(mf_fwd_block_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    rc = check_cuda(cudaFuncSetAttribute(mf_fwd_block_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)MF_BLOCK_SMEM), "cudaFuncSetAttribute");
     if (rc == EMFEM_OK)
-        rc = check_cuda(cudaFuncSetAttribute(mf_bwd_block_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        rc = check_cuda(cudaFuncSetAttribute(mf_bwd_block_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              (int)MF_BLOCK_SMEM), "cudaFuncSetAttribute");
+    if (rc == EMFEM_OK)
+        rc = check_cuda(cudaFuncSetAttribute(mf_fwd_block_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)MF_BLOCK_SMEM2), "cudaFuncSetAttribute");
+    if (rc == EMFEM_OK)
+        rc = check_cuda(cudaFuncSetAttribute(mf_bwd_block_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)MF_BLOCK_SMEM2), "cudaFuncSetAttribute");
     if (rc != EMFEM_OK) { mf_free(m); delete m; return rc; }
     *out = m;
     return EMFEM_OK;

@@ -74,16 +74,41 @@ struct FrontMeta {        // per front, device
 };
 
 // ---------------------------------------------------------------- factorization kernels
+// Symmetric diagonal equilibration: the factorization runs on D^-1/2 K D^-1/2 with D = |diag K|, so every
+// pivot candidate is measured against unit diagonals.  Without it the gradient-type DOFs of the
+// second-order basis (curl-curl column exactly zero, diagonal -k0^2 B_jj only) carry legitimate pivots
+// far below the curl-curl scale at low frequency, and the 32-row pivot floor would perturb them.
+// The scale of a DOF is set by the front that eliminates it, from its diagonal assembly entry.
+__global__ void mf_scale_kernel(const int* __restrict__ lst, const FrontMeta* __restrict__ fm,
+                                const double2* __restrict__ K, const int* __restrict__ slot, const int* __restrict__ off,
+                                const int* __restrict__ fdof, double* __restrict__ scale) {
+    const FrontMeta& f = fm[lst[blockIdx.y]];
+    long long k0 = f.asm0 + (long long)blockIdx.x * MF_CHUNK;
+    long long k1 = min(k0 + MF_CHUNK, f.asm1);
+    const int n = f.n;
+    for (long long k = k0 + threadIdx.x; k < k1; k += blockDim.x) {
+        const int o = off[k], li = o % n;
+        if (li != o / n || li >= f.e) continue;
+        double2 v = K[slot[k]];
+        double a = fabs(v.x) + fabs(v.y);          // |.|_1 of the diagonal: scale only, no accuracy rides on it
+        scale[fdof[f.fdof + li]] = a > 0.0 ? rsqrt(a) : 1.0;
+    }
+}
+
 __global__ void mf_asm_kernel(const int* __restrict__ lst, const FrontMeta* __restrict__ fm,
                               const double2* __restrict__ K, const int* __restrict__ slot, const int* __restrict__ off,
-                              float2* __restrict__ ws) {
+                              const int* __restrict__ fdof, const double* __restrict__ scale, float2* __restrict__ ws) {
     const FrontMeta& f = fm[lst[blockIdx.y]];
     long long k0 = f.asm0 + (long long)blockIdx.x * MF_CHUNK;
     long long k1 = min(k0 + MF_CHUNK, f.asm1);
     float2* W = ws + f.ws;
+    const int n = f.n;
+    const int* D = fdof + f.fdof;
     for (long long k = k0 + threadIdx.x; k < k1; k += blockDim.x) {
+        const int o = off[k];
         double2 v = K[slot[k]];
-        W[off[k]] = make_float2((float)v.x, (float)v.y);
+        double sc = scale[D[o % n]] * scale[D[o / n]];
+        W[o] = make_float2((float)(v.x * sc), (float)(v.y * sc));
     }
 }
 
@@ -419,7 +444,8 @@ __global__ void mf_list_fill_kernel(long long n, const int* __restrict__ indptr,
 // ---------------------------------------------------------------- solve kernels
 // w (rows of the level's fronts, S per row): own rows from the right-hand side, boundary rows zero
 __global__ void mf_fwd_gather_kernel(const int* __restrict__ lst, const FrontMeta* __restrict__ fm, int S,
-                                     const int* __restrict__ fdof, const double2* __restrict__ rhs, float2* __restrict__ w) {
+                                     const int* __restrict__ fdof, const double* __restrict__ scale,
+                                     const double2* __restrict__ rhs, float2* __restrict__ w) {
     const FrontMeta& f = fm[lst[blockIdx.y]];
     long long tot = (long long)f.n * S;
     long long i0 = (long long)blockIdx.x * MF_CHUNK;
@@ -433,7 +459,8 @@ __global__ void mf_fwd_gather_kernel(const int* __restrict__ lst, const FrontMet
         float2 v = make_float2(0.f, 0.f);
         if (i < f.e) {
             double2 r = rhs[(long long)d[i] * S + s];
-            v = make_float2((float)r.x, (float)r.y);
+            double sc = scale[d[i]];
+            v = make_float2((float)(r.x * sc), (float)(r.y * sc));
         }
         W[idx] = v;
     }
@@ -741,12 +768,19 @@ __global__ void mf_bwd_finish_kernel(const int* __restrict__ lst, const FrontMet
     }
 }
 
-__global__ void mf_out_kernel(long long n, int S, const uint8_t* __restrict__ freed, const float2* __restrict__ xs,
-                              double2* __restrict__ x) {
+__global__ void mf_fill_kernel(long long n, double v, double* __restrict__ x) {
+    long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (g < n) x[g] = v;
+}
+
+// x = D^-1/2 (scaled solution), zero outside every front
+__global__ void mf_out_kernel(long long n, int S, const uint8_t* __restrict__ freed, const double* __restrict__ scale,
+                              const float2* __restrict__ xs, double2* __restrict__ x) {
     long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (g >= n * S) return;
     float2 v = xs[g];
-    x[g] = freed[g / S] ? make_double2((double)v.x, (double)v.y) : make_double2(0.0, 0.0);
+    const double sc = scale[g / S];
+    x[g] = freed[g / S] ? make_double2((double)v.x * sc, (double)v.y * sc) : make_double2(0.0, 0.0);
 }
 
 }  // namespace emfem
@@ -769,6 +803,7 @@ struct emfem_mf_s {
     int* d_slot = nullptr;
     int* d_off = nullptr;
     uint8_t* d_free = nullptr;                    // 1 where a DOF belongs to some front
+    double* d_scale = nullptr;                    // equilibration D^-1/2 of the current factorization
     float2* fact = nullptr;
     float2* inv = nullptr;
     int* piv = nullptr;
@@ -788,7 +823,7 @@ struct emfem_mf_s {
 };
 
 static void mf_free(emfem_mf_s* m) {
-    void* ps[] = {m->d_meta, m->d_lst, m->d_fdof, m->d_ea, m->d_slot, m->d_off, m->d_free, m->fact, m->inv, m->piv,
+    void* ps[] = {m->d_meta, m->d_lst, m->d_fdof, m->d_ea, m->d_slot, m->d_off, m->d_free, m->d_scale, m->fact, m->inv, m->piv,
                   m->ws, m->upd, m->d_npert, m->sw, m->suv, m->sy, m->sx};
     for (void* p : ps)
         if (p) cudaFree(p);
@@ -833,7 +868,7 @@ int mf_apply(emfem_mf_s* m, int S, const double2* r, double2* x, cudaStream_t s)
         for (int y0 = 0; y0 < nfl; y0 += 65535) {
             const int ny = std::min(65535, nfl - y0);
             dim3 g(nblk(maxn * S, MF_CHUNK), ny);
-            mf_fwd_gather_kernel<<<g, 256, 0, s>>>(lst + y0, m->d_meta, S, m->d_fdof, r, m->sw);
+            mf_fwd_gather_kernel<<<g, 256, 0, s>>>(lst + y0, m->d_meta, S, m->d_fdof, m->d_scale, r, m->sw);
             dim3 ge(nblk(maxb * S, MF_CHUNK), ny);
             mf_fwd_ea_kernel<<<ge, 256, 0, s>>>(lst + y0, m->d_meta, S, 0, m->d_ea, m->suv, m->sw);
             mf_fwd_ea_kernel<<<ge, 256, 0, s>>>(lst + y0, m->d_meta, S, 1, m->d_ea, m->suv, m->sw);
@@ -879,7 +914,7 @@ int mf_apply(emfem_mf_s* m, int S, const double2* r, double2* x, cudaStream_t s)
         }
         EMFEM_LAUNCH("multifrontal backward");
     }
-    mf_out_kernel<<<grid_for(m->n * S, 256), 256, 0, s>>>(m->n, S, m->d_free, m->sx, x);
+    mf_out_kernel<<<grid_for(m->n * S, 256), 256, 0, s>>>(m->n, S, m->d_free, m->d_scale, m->sx, x);
     EMFEM_LAUNCH("mf_out_kernel");
     return EMFEM_OK;
 }
@@ -1046,6 +1081,7 @@ int emfem_mf_create(emfem_handle h, int64_t n, int n_fronts, const int32_t* e, c
     mk((void**)&m->ws, sizeof(float2) * ws_max);
     mk((void**)&m->upd, sizeof(float2) * upd_top);
     mk((void**)&m->d_npert, sizeof(int));
+    mk((void**)&m->d_scale, sizeof(double) * n);
     if (rc != EMFEM_OK) { mf_free(m); delete m; return rc; }
     rc = check_cuda(cudaFuncSetAttribute(mf_fwd_block_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)MF_BLOCK_SMEM), "cudaFuncSetAttribute");
@@ -1066,7 +1102,8 @@ int emfem_mf_create(emfem_handle h, int64_t n, int n_fronts, const int32_t* e, c
 int emfem_mf_info(emfem_mf m, size_t* device_bytes, double* flops, int* n_levels) {
     EMFEM_REQUIRE(m, "emfem_mf_info: bad handle");
     if (device_bytes)
-        *device_bytes = sizeof(float2) * (m->fact_n + m->inv_n + m->ws_n + m->upd_n) + sizeof(int) * m->piv_n;
+        *device_bytes = sizeof(float2) * (m->fact_n + m->inv_n + m->ws_n + m->upd_n) + sizeof(int) * m->piv_n +
+                        sizeof(double) * m->n;
     if (flops) *flops = m->flops;
     if (n_levels) *n_levels = (int)m->levels.size();
     return EMFEM_OK;
@@ -1083,6 +1120,18 @@ int emfem_mf_factor(emfem_mf m, const void* K_vals, int* n_perturbed) {
     m->factored = false;
     rc = check_cuda(cudaMemsetAsync(m->d_npert, 0, sizeof(int), s), "cudaMemsetAsync");
     const int nl = (int)m->levels.size();
+    // equilibration first: a front's boundary DOFs take their scale from the ancestors that eliminate them
+    if (rc == EMFEM_OK) {
+        mf_fill_kernel<<<grid_for(m->n, 256), 256, 0, s>>>(m->n, 1.0, m->d_scale);
+        for (int L = 0; L < nl; L++)
+            for (int y0 = 0; y0 < (int)m->levels[L].size(); y0 += 65535) {
+                const int ny = std::min(65535, (int)m->levels[L].size() - y0);
+                mf_scale_kernel<<<dim3(nblk(m->lvl_max_asm[L], MF_CHUNK), ny), 256, 0, s>>>(
+                    m->d_lst + m->lvl_off[L] + y0, m->d_meta, (const double2*)K_vals, m->d_slot, m->d_off, m->d_fdof,
+                    m->d_scale);
+            }
+        rc = check_cuda(cudaGetLastError(), "multifrontal equilibration");
+    }
     for (int L = 0; L < nl && rc == EMFEM_OK; L++) {
         const int nfl = (int)m->levels[L].size();
         long long wsz = 0;
@@ -1093,7 +1142,7 @@ int emfem_mf_factor(emfem_mf m, const void* K_vals, int* n_perturbed) {
             const int* lst = m->d_lst + m->lvl_off[L] + y0;
             long long maxn = m->lvl_max_n[L], maxb = m->lvl_max_b[L];
             mf_asm_kernel<<<dim3(nblk(m->lvl_max_asm[L], MF_CHUNK), ny), 256, 0, s>>>(
-                lst, m->d_meta, (const double2*)K_vals, m->d_slot, m->d_off, m->ws);
+                lst, m->d_meta, (const double2*)K_vals, m->d_slot, m->d_off, m->d_fdof, m->d_scale, m->ws);
             for (int c = 0; c < 2; c++)
                 mf_ea_kernel<<<dim3(nblk(maxb * maxb, MF_CHUNK), ny), 256, 0, s>>>(lst, m->d_meta, c, m->d_ea, m->upd, m->ws);
             for (int k = 0; k < m->lvl_max_e[L]; k += MF_NB) {
@@ -1106,10 +1155,6 @@ int emfem_mf_factor(emfem_mf m, const void* K_vals, int* n_perturbed) {
             }
             mf_compact_kernel<<<dim3(nblk(maxn * maxn, MF_CHUNK), ny), 256, 0, s>>>(lst, m->d_meta, m->ws, m->fact, m->upd);
             rc = check_cuda(cudaGetLastError(), "multifrontal factor level");
-        }
-        if (nfl > 65535 && rc == EMFEM_OK) {
-            // the level workspace holds every front of the level at once; levels wider than one grid are split
-            // only in their launches, never in their storage
         }
     }
     int np = 0;

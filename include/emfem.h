@@ -372,9 +372,11 @@ int emfem_adam_step(emfem_handle h, int64_t n, float *params, const float *grad,
  *   emfem_mf_build_lists builds them on the device from the CSR pattern (device indptr (n + 1) and
  *   indices (nnz), int32), which must come before the first factorization.
  * info: device bytes held, factorization flops, number of levels.
- * factor: K_vals (nnz c128, device) on the CSR pattern the structure was built for; *n_perturbed
- *   (host) gets the number of pivots raised to 1e-6 of their 32 x 32 block's largest entry (pivoting is
- *   partial inside each 32-row diagonal block).  Synchronises the stream.
+ * factor: K_vals (nnz c128, device) on the CSR pattern the structure was built for; the factorization
+ *   runs on the equilibrated D^-1/2 K D^-1/2 (D = |diag K|_1, 1 where the diagonal is zero), and solve
+ *   undoes the scaling; *n_perturbed (host) gets the number of pivots raised to 1e-6 of their 32 x 32
+ *   block's largest entry (pivoting is partial inside each 32-row diagonal block).  Synchronises the
+ *   stream.
  * reserve: solve buffers for up to nrhs right-hand sides (<= 256).
  * solve: x = (LU)^-1 b for nrhs right-hand sides, b and x (n, nrhs) c128 DOF-major, device; x is zero on
  *   DOFs that belong to no front (PEC).

@@ -460,7 +460,7 @@ def configs_sweep_section(n_meshes: int = 16, tol: float = 1e-8) -> dict:
     t_setup = time.perf_counter() - ts
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    rd = sw.solve_direct(sys4, window=9, tol=tol, adaptive=True)
+    rd = sw.solve_direct(sys4, window=9, tol=tol, adaptive=True, precision="auto")
     torch.cuda.synchronize()
     t_d = time.perf_counter() - t0
     rk = sw.solve(sys4[-8:], tol=tol, maxit=30000, precond="aux")
@@ -475,7 +475,11 @@ def configs_sweep_section(n_meshes: int = 16, tol: float = 1e-8) -> dict:
         "device_lu": {"converged": int(((rd.status == 0) & (rd.relres <= tol)).sum()), "systems": len(sys4),
                       "seconds": t_d, "solves_per_s": int(((rd.status == 0) & (rd.relres <= tol)).sum()) / t_d,
                       "setup_seconds": t_setup, "iters_max": int(rd.iters.max()),
-                      "relres_max": float(rd.relres.max()), "windows": len(rd.windows)},
+                      "relres_max": float(rd.relres.max()), "windows": len(rd.windows),
+                      "precision": "auto (complex64 first, complex128 for the systems it leaves)",
+                      "factorizations_c128": sum(1 for w in rd.windows if w["precision"] == "c128"),
+                      "c128_frequencies_max": max([w["factored"] for w in rd.windows if w["precision"] == "c128"],
+                                                  default=None)},
         "aux_krylov_top8_freqs": {"converged": int((rk.status == 0).sum()), "seconds": rk.seconds,
                                   "iters_max": int(rk.iters.max())},
         "lu_vs_aux_rel_diff_per_freq": diff}
@@ -636,6 +640,8 @@ def main():
         tuning = {"variant": args.variant, "ms": None}
     else:
         tuning = plan.tune(er, ur)
+    tuned_info = plan.variant_info(int(tuning["variant"]))
+    tuning = dict(tuning, **tuned_info)
     for _ in range(args.warmup):
         plan.assemble(er, ur, E, B)
     torch.cuda.synchronize()
@@ -722,7 +728,9 @@ def main():
                                          "ncu capture at 82 944 tets (profiles/assemble_chunk_kernel_cavity24.md) "
                                          "scaled by tets; the invariants kernel adds ~1.4 KB/tet",
                          "peak_kind": peak_kind,
-                         "alg_bytes_per_tet": alg_bytes_per_tet, "kernels": "tet_invariants_kernel+assemble_kernel"},
+                         "alg_bytes_per_tet": alg_bytes_per_tet,
+                         "kernels": ("tet_canon_kernel+assemble_recipe_kernel" if tuned_info["table_driven"]
+                                     else "tet_invariants_kernel+assemble_chunk_kernel")},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
                     "api": "emerge_b200.assembly.tet_mass_stiffness_matrices (host numpy in, SciPy CSR out)"},
             "gpu_launches": 2 * args.steps,

@@ -59,6 +59,7 @@ _SIGS = {
     "emfem_plan_find_slots": ([_vp, _i64, _vp, _vp, _vp], _i32),
     "emfem_plan_variants": ([_vp, _i32p, _i32p], _i32),
     "emfem_plan_set_variant": ([_vp, _i32], _i32),
+    "emfem_plan_variant_info": ([_vp, _i32, _i32p, _i32p, _i32p, _i32p], _i32),
     "emfem_ned2_tri_robin": ([_vp, _i64, _vp, _i64, _vp, _dbl, _dbl, _vp, _vp, _i32, _vp, _vp], _i32),
     "emfem_segmented_gather_sum": ([_vp, _i64, _vp, _vp, _vp, _vp], _i32),
     "emfem_sweep_combine": ([_vp, _i64, _vp, _vp, _dbl, _i64, _vp, _vp, _dbl, _dbl, _vp], _i32),
@@ -108,6 +109,7 @@ _SIGS = {
     "emfem_mf_build_lists": ([_vp, _i64, _vp, _vp], _i32),
     "emfem_mf_info": ([_vp, ctypes.POINTER(ctypes.c_size_t), ctypes.POINTER(ctypes.c_double), _i32p], _i32),
     "emfem_mf_factor": ([_vp, _vp, _i32p], _i32),
+    "emfem_mf_set_precision": ([_vp, _i32], _i32),
     "emfem_mf_reserve": ([_vp, _i32], _i32),
     "emfem_mf_solve": ([_vp, _i32, _vp, _vp], _i32),
     "emfem_mf_destroy": ([_vp], _i32),

@@ -145,6 +145,13 @@ class CsrPlan:
     def set_variant(self, v: int) -> None:
         check(lib().emfem_plan_set_variant(self._p, int(v)), "emfem_plan_set_variant")
 
+    def variant_info(self, v: int) -> dict:
+        """Chunk capacity, threads per CTA, table-driven flag and availability of kernel variant ``v``."""
+        ch, nt, td, av = (ctypes.c_int() for _ in range(4))
+        check(lib().emfem_plan_variant_info(self._p, int(v), ctypes.byref(ch), ctypes.byref(nt), ctypes.byref(td),
+                                            ctypes.byref(av)), "emfem_plan_variant_info")
+        return {"chunk": ch.value, "threads": nt.value, "table_driven": bool(td.value), "available": bool(av.value)}
+
     def tune(self, er: torch.Tensor, ur: torch.Tensor, reps: int = 3, cache: str | None = None) -> dict:
         """Autotune the assembly kernel variant (chunk capacity x CTA size) for this mesh on this GPU.
 
@@ -152,7 +159,9 @@ class CsrPlan:
         then ``reps`` launches) and keeps the fastest.  Results are cached as JSON keyed by GPU name
         and mesh size (``~/.cache/emerge_b200/autotune.json`` unless ``cache`` is given)."""
         path = cache or os.path.join(os.path.expanduser("~"), ".cache", "emerge_b200", "autotune.json")
-        key = f"{torch.cuda.get_device_name(self.device)}|assemble|{self.dmesh.n_tets}|{self.nnz}"
+        nv = ctypes.c_int()
+        check(lib().emfem_plan_variants(self._p, ctypes.byref(nv), None), "emfem_plan_variants")
+        key = f"{torch.cuda.get_device_name(self.device)}|assemble|{self.dmesh.n_tets}|{self.nnz}|{nv.value}"
         try:
             table = json.load(open(path))
         except (OSError, ValueError):

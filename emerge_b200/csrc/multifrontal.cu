@@ -64,6 +64,43 @@ __device__ __forceinline__ float2 cinv(float2 a) {
     return make_float2(a.x * d, -a.y * d);
 }
 
+// The same operations in double precision (factorizations computed in complex128)
+__device__ __forceinline__ double2 cmul(double2 a, double2 b) {
+    return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__device__ __forceinline__ void cfma(double2& c, double2 a, double2 b) {
+    c.x = fma(a.x, b.x, fma(-a.y, b.y, c.x));
+    c.y = fma(a.x, b.y, fma(a.y, b.x, c.y));
+}
+__device__ __forceinline__ void cfms(double2& c, double2 a, double2 b) {
+    c.x = fma(-a.x, b.x, fma(a.y, b.y, c.x));
+    c.y = fma(-a.x, b.y, fma(-a.y, b.x, c.y));
+}
+__device__ __forceinline__ double cabs2(double2 a) { return a.x * a.x + a.y * a.y; }
+__device__ __forceinline__ double2 cinv(double2 a) {
+    double d = 1.0 / cabs2(a);
+    return make_double2(a.x * d, -a.y * d);
+}
+
+// complex64 / complex128 element helpers for the templated factorization kernels
+template <typename T> struct CxT;
+template <> struct CxT<float2> {
+    typedef float R;
+    __device__ static float2 make(double x, double y) { return make_float2((float)x, (float)y); }
+};
+template <> struct CxT<double2> {
+    typedef double R;
+    __device__ static double2 make(double x, double y) { return make_double2(x, y); }
+};
+__device__ __forceinline__ float2 to_c64(float2 v) { return v; }
+__device__ __forceinline__ float2 to_c64(double2 v) { return make_float2((float)v.x, (float)v.y); }
+__device__ __forceinline__ void cp_async16(void* dst_smem, const void* src) {
+    unsigned d = (unsigned)__cvta_generic_to_shared(dst_smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_c(float2* dst_smem, const float2* src) { cp_async8(dst_smem, src); }
+__device__ __forceinline__ void cp_async_c(double2* dst_smem, const double2* src) { cp_async16(dst_smem, src); }
+
 struct FrontMeta {        // per front, device
     int e, b, n, parent;
     int child[2];
@@ -95,25 +132,31 @@ __global__ void mf_scale_kernel(const int* __restrict__ lst, const FrontMeta* __
     }
 }
 
+// Factorization kernels are templated on the workspace element T: float2 (complex64 fronts) or double2
+// (complex128 fronts).  The factor store that the solves read is complex64 in both cases; a complex128
+// factorization rounds its factors once, at compaction, so the rounding error does not compound through
+// the Schur-complement chain.
+template <typename T>
 __global__ void mf_asm_kernel(const int* __restrict__ lst, const FrontMeta* __restrict__ fm,
                               const double2* __restrict__ K, const int* __restrict__ slot, const int* __restrict__ off,
-                              const int* __restrict__ fdof, const double* __restrict__ scale, float2* __restrict__ ws) {
+                              const int* __restrict__ fdof, const double* __restrict__ scale, T* __restrict__ ws) {
     const FrontMeta& f = fm[lst[blockIdx.y]];
     long long k0 = f.asm0 + (long long)blockIdx.x * MF_CHUNK;
     long long k1 = min(k0 + MF_CHUNK, f.asm1);
-    float2* W = ws + f.ws;
+    T* W = ws + f.ws;
     const int n = f.n;
     const int* D = fdof + f.fdof;
     for (long long k = k0 + threadIdx.x; k < k1; k += blockDim.x) {
         const int o = off[k];
         double2 v = K[slot[k]];
         double sc = scale[D[o % n]] * scale[D[o / n]];
-        W[o] = make_float2((float)(v.x * sc), (float)(v.y * sc));
+        W[o] = CxT<T>::make(v.x * sc, v.y * sc);
     }
 }
 
+template <typename T>
 __global__ void mf_ea_kernel(const int* __restrict__ lst, const FrontMeta* __restrict__ fm, int cslot,
-                             const int* __restrict__ ea, const float2* __restrict__ upd, float2* __restrict__ ws) {
+                             const int* __restrict__ ea, const T* __restrict__ upd, T* __restrict__ ws) {
     const FrontMeta& f = fm[lst[blockIdx.y]];
     int c = f.child[cslot];
     if (c < 0) return;
@@ -124,71 +167,76 @@ __global__ void mf_ea_kernel(const int* __restrict__ lst, const FrontMeta* __res
     if (i0 >= tot) return;
     long long i1 = min(i0 + MF_CHUNK, tot);
     const int* map = ea + g.ea;
-    const float2* U = upd + g.upd;
-    float2* W = ws + f.ws;
+    const T* U = upd + g.upd;
+    T* W = ws + f.ws;
     long long ld = f.n;
     for (long long idx = i0 + threadIdx.x; idx < i1; idx += blockDim.x) {
         long long i = idx % nb, j = idx / nb;
-        float2 u = U[idx];
-        float2* dst = W + map[i] + (long long)map[j] * ld;
+        T u = U[idx];
+        T* dst = W + map[i] + (long long)map[j] * ld;
         dst->x += u.x;
         dst->y += u.y;
     }
 }
 
 // LU with partial pivoting of the 32 x 32 diagonal block at step k, plus the explicit inverses of its
-// unit-lower L and upper U.  One warp per front; lane = column (or row in the pivot search).
+// unit-lower L and upper U.  One warp per front; lane = column (or row in the pivot search).  The
+// inverses go to inv (complex64, read by the solves) and, for a complex128 factorization, also to invc
+// (complex128, read by the panel kernel); for complex64 invc is inv.
+template <typename T>
 __global__ void __launch_bounds__(32) mf_diag_kernel(const int* __restrict__ lst, const FrontMeta* __restrict__ fm, int k,
-                                                     float2* __restrict__ ws, float2* __restrict__ inv,
+                                                     T* __restrict__ ws, float2* __restrict__ inv, T* __restrict__ invc,
                                                      int* __restrict__ piv, int* __restrict__ nperturbed) {
-    __shared__ float2 D[MF_NB][MF_NB + 1];
-    __shared__ float2 X[MF_NB][MF_NB + 1];
+    typedef typename CxT<T>::R R;
+    __shared__ T D[MF_NB][MF_NB + 1];
+    __shared__ T X[MF_NB][MF_NB + 1];
     const FrontMeta& f = fm[lst[blockIdx.x]];
     if (k >= f.e) return;
     const int kb = min(MF_NB, f.e - k);
     const int lane = threadIdx.x;
     const long long ld = f.n;
-    float2* W = ws + f.ws + k + (long long)k * ld;
-    float bmax = 0.0f;
+    T* W = ws + f.ws + k + (long long)k * ld;
+    const T zero = CxT<T>::make(0.0, 0.0);
+    R bmax = 0;
     for (int c = 0; c < kb; c++) {
-        float2 v = lane < kb ? W[lane + (long long)c * ld] : make_float2(0.f, 0.f);
+        T v = lane < kb ? W[lane + (long long)c * ld] : zero;
         D[lane][c] = v;
-        bmax = fmaxf(bmax, cabs2(v));
+        bmax = max(bmax, cabs2(v));
     }
-    for (int o = 16; o > 0; o >>= 1) bmax = fmaxf(bmax, __shfl_xor_sync(0xffffffffu, bmax, o));
-    const float floor2 = fmaxf(bmax, 1e-30f) * 1e-12f;      // (1e-6 of the block's largest entry)^2
+    for (int o = 16; o > 0; o >>= 1) bmax = max(bmax, __shfl_xor_sync(0xffffffffu, bmax, o));
+    const R floor2 = max(bmax, (R)1e-30) * (R)1e-12;      // (1e-6 of the block's largest entry)^2
     __syncwarp();
     int* P = piv + f.piv + k;
     int pert = 0;
     for (int j = 0; j < kb; j++) {
         // pivot: largest |D[r][j]| for r >= j (ties: smallest r)
-        float best = (lane >= j && lane < kb) ? cabs2(D[lane][j]) : -1.0f;
+        R best = (lane >= j && lane < kb) ? cabs2(D[lane][j]) : (R)-1;
         int br = lane;
         for (int o = 16; o > 0; o >>= 1) {
-            float ob = __shfl_xor_sync(0xffffffffu, best, o);
+            R ob = __shfl_xor_sync(0xffffffffu, best, o);
             int orr = __shfl_xor_sync(0xffffffffu, br, o);
             if (ob > best || (ob == best && orr < br)) { best = ob; br = orr; }
         }
         if (lane == 0) P[j] = br;
         if (br != j && lane < kb) {
-            float2 t = D[j][lane];
+            T t = D[j][lane];
             D[j][lane] = D[br][lane];
             D[br][lane] = t;
         }
         __syncwarp();
         if (lane == 0 && cabs2(D[j][j]) < floor2) {
-            float2 d = D[j][j];
-            float a = sqrtf(cabs2(d));
-            float fl = sqrtf(floor2);
-            D[j][j] = a > 0.f ? make_float2(d.x / a * fl, d.y / a * fl) : make_float2(fl, 0.f);
+            T d = D[j][j];
+            R a = sqrt(cabs2(d));
+            R fl = sqrt(floor2);
+            D[j][j] = a > 0 ? CxT<T>::make(d.x / a * fl, d.y / a * fl) : CxT<T>::make(fl, 0.0);
             pert++;
         }
         __syncwarp();
-        float2 pinv = cinv(D[j][j]);
+        T pinv = cinv(D[j][j]);
         if (lane > j && lane < kb) D[lane][j] = cmul(D[lane][j], pinv);
         __syncwarp();
         if (lane > j && lane < kb) {
-            float2 u = D[j][lane];
+            T u = D[j][lane];
             for (int r = j + 1; r < kb; r++) cfms(D[r][lane], D[r][j], u);
         }
         __syncwarp();
@@ -197,35 +245,42 @@ __global__ void __launch_bounds__(32) mf_diag_kernel(const int* __restrict__ lst
     // write L\U back
     for (int c = 0; c < kb; c++)
         if (lane < kb) W[lane + (long long)c * ld] = D[lane][c];
-    float2* Li = inv + f.inv + (long long)(k / MF_NB) * 2 * MF_NB * MF_NB;   // Linv then Uinv, column-major 32x32
+    const long long ib = f.inv + (long long)(k / MF_NB) * 2 * MF_NB * MF_NB;   // Linv then Uinv, column-major 32x32
+    float2* Li = inv + ib;
     float2* Ui = Li + MF_NB * MF_NB;
+    T* Lc = invc + ib;
+    T* Uc = Lc + MF_NB * MF_NB;
+    constexpr bool wide = sizeof(T) != sizeof(float2);
     // Uinv: lane = column c of X = U^-1 (back substitution, own column only)
     {
         int c = lane;
-        for (int i = 0; i < MF_NB; i++) X[i][c] = make_float2(0.f, 0.f);
+        for (int i = 0; i < MF_NB; i++) X[i][c] = zero;
         if (c < kb) {
             X[c][c] = cinv(D[c][c]);
             for (int i = c - 1; i >= 0; i--) {
-                float2 s = make_float2(0.f, 0.f);
+                T s = zero;
                 for (int t = i + 1; t <= c; t++) cfma(s, D[i][t], X[t][c]);
-                float2 q = cmul(s, cinv(D[i][i]));
-                X[i][c] = make_float2(-q.x, -q.y);
+                T q = cmul(s, cinv(D[i][i]));
+                X[i][c] = CxT<T>::make(-q.x, -q.y);
             }
         }
     }
     __syncwarp();
-    for (int c = 0; c < MF_NB; c++) Ui[lane + c * MF_NB] = X[lane][c];
+    for (int c = 0; c < MF_NB; c++) {
+        Ui[lane + c * MF_NB] = to_c64(X[lane][c]);
+        if (wide) Uc[lane + c * MF_NB] = X[lane][c];
+    }
     __syncwarp();
     // Linv: lane = column c of Y = L^-1 (unit lower, forward substitution)
     {
         int c = lane;
-        for (int i = 0; i < MF_NB; i++) X[i][c] = make_float2(0.f, 0.f);
+        for (int i = 0; i < MF_NB; i++) X[i][c] = zero;
         if (c < kb) {
-            X[c][c] = make_float2(1.f, 0.f);
+            X[c][c] = CxT<T>::make(1.0, 0.0);
             for (int i = c + 1; i < kb; i++) {
-                float2 s = make_float2(0.f, 0.f);
+                T s = zero;
                 for (int t = c; t < i; t++) cfma(s, D[i][t], X[t][c]);
-                X[i][c] = make_float2(-s.x, -s.y);
+                X[i][c] = CxT<T>::make(-s.x, -s.y);
             }
         }
     }
@@ -244,38 +299,43 @@ __global__ void __launch_bounds__(32) mf_diag_kernel(const int* __restrict__ lst
         for (int i = 0; i < MF_NB; i++) { if (i == j) q[i] = b2; if (i == r) q[i] = a; }
     }
 #pragma unroll
-    for (int i = 0; i < MF_NB; i++) Li[lane + q[i] * MF_NB] = X[lane][i];
+    for (int i = 0; i < MF_NB; i++) {
+        Li[lane + q[i] * MF_NB] = to_c64(X[lane][i]);
+        if (wide) Lc[lane + q[i] * MF_NB] = X[lane][i];
+    }
 }
 
 // Block row (columns >= k + kb): row swaps, then L^-1; block column (rows >= k + kb): times U^-1.
 // Items 0 .. m-1 are columns, m .. 2m-1 rows (m = n - k - kb).
+template <typename T>
 __global__ void __launch_bounds__(256) mf_panel_kernel(const int* __restrict__ lst, const FrontMeta* __restrict__ fm, int k,
-                                                       float2* __restrict__ ws, const float2* __restrict__ inv,
+                                                       T* __restrict__ ws, const T* __restrict__ invc,
                                                        const int* __restrict__ piv) {
-    __shared__ float2 Li[MF_NB * MF_NB];
-    __shared__ float2 Ui[MF_NB * MF_NB];
+    __shared__ T Li[MF_NB * MF_NB];
+    __shared__ T Ui[MF_NB * MF_NB];
     const FrontMeta& f = fm[lst[blockIdx.y]];
     if (k >= f.e) return;
     const int kb = min(MF_NB, f.e - k);
     const long long m = f.n - k - kb;
     long long item = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if ((long long)blockIdx.x * blockDim.x >= 2 * m) return;
-    const float2* L = inv + f.inv + (long long)(k / MF_NB) * 2 * MF_NB * MF_NB;
+    const T* L = invc + f.inv + (long long)(k / MF_NB) * 2 * MF_NB * MF_NB;
     for (int t = threadIdx.x; t < MF_NB * MF_NB; t += blockDim.x) { Li[t] = L[t]; Ui[t] = L[MF_NB * MF_NB + t]; }
     __syncthreads();
     if (item >= 2 * m) return;
     const long long ld = f.n;
-    float2* W = ws + f.ws;
-    float2 v[MF_NB];
+    T* W = ws + f.ws;
+    const T zero = CxT<T>::make(0.0, 0.0);
+    T v[MF_NB];
     if (item < m) {
         long long c = k + kb + item;
-        float2* col = W + k + c * ld;
+        T* col = W + k + c * ld;
 #pragma unroll
-        for (int i = 0; i < MF_NB; i++) v[i] = i < kb ? col[i] : make_float2(0.f, 0.f);
+        for (int i = 0; i < MF_NB; i++) v[i] = i < kb ? col[i] : zero;
 #pragma unroll
         for (int i = 0; i < MF_NB; i++) {
             if (i < kb) {
-                float2 s = make_float2(0.f, 0.f);
+                T s = zero;
 #pragma unroll
                 for (int t = 0; t < MF_NB; t++) cfma(s, Li[i + t * MF_NB], v[t]);   // (Linv P) times the column
                 col[i] = s;
@@ -283,13 +343,13 @@ __global__ void __launch_bounds__(256) mf_panel_kernel(const int* __restrict__ l
         }
     } else {
         long long r = k + kb + (item - m);
-        float2* row = W + r + (long long)k * ld;
+        T* row = W + r + (long long)k * ld;
 #pragma unroll
-        for (int i = 0; i < MF_NB; i++) v[i] = i < kb ? row[(long long)i * ld] : make_float2(0.f, 0.f);
+        for (int i = 0; i < MF_NB; i++) v[i] = i < kb ? row[(long long)i * ld] : zero;
 #pragma unroll
         for (int c = 0; c < MF_NB; c++) {
             if (c < kb) {
-                float2 s = make_float2(0.f, 0.f);
+                T s = zero;
 #pragma unroll
                 for (int t = 0; t < MF_NB; t++) cfma(s, v[t], Ui[t + c * MF_NB]);
                 row[(long long)c * ld] = s;
@@ -298,11 +358,15 @@ __global__ void __launch_bounds__(256) mf_panel_kernel(const int* __restrict__ l
     }
 }
 
-// Trailing update C -= A B on 64 x 64 tiles: A = W[k+kb.., k..k+kb), B = W[k..k+kb, k+kb..).
+// Trailing update C -= A B on 64 x 64 tiles: A = W[k+kb.., k..k+kb), B = W[k..k+kb, k+kb..).  The k
+// extent runs in stages of KH columns (32 for complex64: one stage; 16 for complex128, whose tiles
+// would otherwise exceed the static shared-memory limit).
+template <typename T>
 __global__ void __launch_bounds__(256) mf_trail_kernel(const int* __restrict__ lst, const FrontMeta* __restrict__ fm, int k,
-                                                       float2* __restrict__ ws) {
-    __shared__ float2 As[MF_NB][MF_TILE + 1];
-    __shared__ float2 Bs[MF_NB][MF_TILE + 1];
+                                                       T* __restrict__ ws) {
+    constexpr int KH = sizeof(T) == sizeof(float2) ? MF_NB : MF_NB / 2;
+    __shared__ T As[KH][MF_TILE + 1];
+    __shared__ T Bs[KH][MF_TILE + 1];
     const FrontMeta& f = fm[lst[blockIdx.y]];
     if (k >= f.e) return;
     const int kb = min(MF_NB, f.e - k);
@@ -312,43 +376,50 @@ __global__ void __launch_bounds__(256) mf_trail_kernel(const int* __restrict__ l
     const long long ti = blockIdx.x % nt, tj = blockIdx.x / nt;
     const long long r0 = k + kb + ti * MF_TILE, c0 = k + kb + tj * MF_TILE;
     const long long ld = f.n;
-    float2* W = ws + f.ws;
+    T* W = ws + f.ws;
     const int tid = threadIdx.x;
-    // A tile (64 rows x kb) and B tile (kb x 64 cols) by asynchronous copies; out-of-range parts zeroed
-    for (int t = tid; t < MF_NB * MF_TILE; t += 256) {
-        int rr = t % MF_TILE, kk = t / MF_TILE;
-        long long r = r0 + rr;
-        if (kk < kb && r < f.n) cp_async8(&As[kk][rr], &W[r + (long long)(k + kk) * ld]);
-        else As[kk][rr] = make_float2(0.f, 0.f);
-        int kk2 = t % MF_NB, cc = t / MF_NB;
-        long long c = c0 + cc;
-        if (kk2 < kb && c < f.n) cp_async8(&Bs[kk2][cc], &W[(k + kk2) + c * ld]);
-        else Bs[kk2][cc] = make_float2(0.f, 0.f);
-    }
     const int tx = tid % 16, ty = tid / 16;
-    // the thread's 16 C entries go straight into its accumulators while the tiles are in flight
-    float2 acc[4][4];
-#pragma unroll
-    for (int j = 0; j < 4; j++) {
-        long long c = c0 + ty + 16 * j;
-#pragma unroll
-        for (int i = 0; i < 4; i++) {
-            long long r = r0 + tx + 16 * i;
-            acc[i][j] = (r < f.n && c < f.n) ? W[r + c * ld] : make_float2(0.f, 0.f);
+    const T zero = CxT<T>::make(0.0, 0.0);
+    T acc[4][4];
+    for (int k2 = 0; k2 < kb; k2 += KH) {
+        if (k2) __syncthreads();                  // the previous stage's tiles are consumed
+        // A tile (64 rows x KH) and B tile (KH x 64 cols) by asynchronous copies; out-of-range parts zeroed
+        for (int t = tid; t < KH * MF_TILE; t += 256) {
+            int rr = t % MF_TILE, kk = t / MF_TILE;
+            long long r = r0 + rr;
+            if (k2 + kk < kb && r < f.n) cp_async_c(&As[kk][rr], &W[r + (long long)(k + k2 + kk) * ld]);
+            else As[kk][rr] = zero;
+            int kk2 = t % KH, cc = t / KH;
+            long long c = c0 + cc;
+            if (k2 + kk2 < kb && c < f.n) cp_async_c(&Bs[kk2][cc], &W[(k + k2 + kk2) + c * ld]);
+            else Bs[kk2][cc] = zero;
         }
-    }
-    cp_async_wait_all();
-    __syncthreads();
-    for (int kk = 0; kk < kb; kk++) {
-        float2 a[4], b[4];
+        if (k2 == 0) {
+            // the thread's 16 C entries go straight into its accumulators while the tiles are in flight
 #pragma unroll
-        for (int i = 0; i < 4; i++) a[i] = As[kk][tx + 16 * i];
+            for (int j = 0; j < 4; j++) {
+                long long c = c0 + ty + 16 * j;
 #pragma unroll
-        for (int j = 0; j < 4; j++) b[j] = Bs[kk][ty + 16 * j];
+                for (int i = 0; i < 4; i++) {
+                    long long r = r0 + tx + 16 * i;
+                    acc[i][j] = (r < f.n && c < f.n) ? W[r + c * ld] : zero;
+                }
+            }
+        }
+        cp_async_wait_all();
+        __syncthreads();
+        const int kn = min(KH, kb - k2);
+        for (int kk = 0; kk < kn; kk++) {
+            T a[4], b[4];
 #pragma unroll
-        for (int i = 0; i < 4; i++)
+            for (int i = 0; i < 4; i++) a[i] = As[kk][tx + 16 * i];
 #pragma unroll
-            for (int j = 0; j < 4; j++) cfms(acc[i][j], a[i], b[j]);
+            for (int j = 0; j < 4; j++) b[j] = Bs[kk][ty + 16 * j];
+#pragma unroll
+            for (int i = 0; i < 4; i++)
+#pragma unroll
+                for (int j = 0; j < 4; j++) cfms(acc[i][j], a[i], b[j]);
+        }
     }
 #pragma unroll
     for (int j = 0; j < 4; j++) {
@@ -362,22 +433,24 @@ __global__ void __launch_bounds__(256) mf_trail_kernel(const int* __restrict__ l
     }
 }
 
-// Factor columns (n x e), U block row (e x b) and Schur complement (b x b) out of the workspace.
+// Factor columns (n x e) and U block row (e x b), rounded to complex64, and the Schur complement (b x b,
+// workspace precision) out of the workspace.
+template <typename T>
 __global__ void mf_compact_kernel(const int* __restrict__ lst, const FrontMeta* __restrict__ fm,
-                                  const float2* __restrict__ ws, float2* __restrict__ fact, float2* __restrict__ upd) {
+                                  const T* __restrict__ ws, float2* __restrict__ fact, T* __restrict__ upd) {
     const FrontMeta& f = fm[lst[blockIdx.y]];
     const long long n = f.n, e = f.e, b = f.b;
     long long i0 = (long long)blockIdx.x * MF_CHUNK;
     if (i0 >= n * n) return;
     long long i1 = min(i0 + MF_CHUNK, n * n);
-    const float2* W = ws + f.ws;
+    const T* W = ws + f.ws;
     float2* F = fact + f.fact;
-    float2* U = upd + f.upd;
+    T* U = upd + f.upd;
     for (long long idx = i0 + threadIdx.x; idx < i1; idx += blockDim.x) {
         long long i = idx % n, j = idx / n;
-        float2 v = W[idx];
-        if (j < e) F[idx] = v;
-        else if (i < e) F[n * e + i + (j - e) * e] = v;
+        T v = W[idx];
+        if (j < e) F[idx] = to_c64(v);
+        else if (i < e) F[n * e + i + (j - e) * e] = to_c64(v);
         else U[(i - e) + (j - e) * b] = v;
     }
 }
@@ -807,8 +880,10 @@ struct emfem_mf_s {
     float2* fact = nullptr;
     float2* inv = nullptr;
     int* piv = nullptr;
-    float2* ws = nullptr;
-    float2* upd = nullptr;
+    void* ws = nullptr;                           // level workspace, complex64 or (wide) complex128
+    void* upd = nullptr;                          // update store, same precision as ws
+    void* invc = nullptr;                         // complex128 copies of the inverse blocks (wide only)
+    bool wide = false;                            // fronts factored in complex128
     int* d_npert = nullptr;
     long long fact_n = 0, inv_n = 0, piv_n = 0, ws_n = 0, upd_n = 0;
     long long wv_n = 0, uv_n = 0, y_n = 0;        // solve buffer rows
@@ -824,7 +899,7 @@ struct emfem_mf_s {
 
 static void mf_free(emfem_mf_s* m) {
     void* ps[] = {m->d_meta, m->d_lst, m->d_fdof, m->d_ea, m->d_slot, m->d_off, m->d_free, m->d_scale, m->fact, m->inv, m->piv,
-                  m->ws, m->upd, m->d_npert, m->sw, m->suv, m->sy, m->sx};
+                  m->ws, m->upd, m->invc, m->d_npert, m->sw, m->suv, m->sy, m->sx};
     for (void* p : ps)
         if (p) cudaFree(p);
 }
@@ -919,6 +994,43 @@ int mf_apply(emfem_mf_s* m, int S, const double2* r, double2* x, cudaStream_t s)
     return EMFEM_OK;
 }
 }  // namespace emfem
+
+// The level loop of one factorization, fronts in workspace precision T.
+template <typename T>
+static int mf_factor_levels(emfem_mf_s* m, const double2* K_vals, cudaStream_t s) {
+    T* ws = (T*)m->ws;
+    T* upd = (T*)m->upd;
+    T* invc = m->wide ? (T*)m->invc : (T*)m->inv;
+    int rc = EMFEM_OK;
+    const int nl = (int)m->levels.size();
+    for (int L = 0; L < nl && rc == EMFEM_OK; L++) {
+        const int nfl = (int)m->levels[L].size();
+        long long wsz = 0;
+        for (int v : m->levels[L]) wsz += (long long)m->meta[v].n * m->meta[v].n;
+        rc = check_cuda(cudaMemsetAsync(ws, 0, sizeof(T) * wsz, s), "cudaMemsetAsync");
+        for (int y0 = 0; y0 < nfl && rc == EMFEM_OK; y0 += 65535) {
+            const int ny = std::min(65535, nfl - y0);
+            const int* lst = m->d_lst + m->lvl_off[L] + y0;
+            long long maxn = m->lvl_max_n[L], maxb = m->lvl_max_b[L];
+            mf_asm_kernel<T><<<dim3(nblk(m->lvl_max_asm[L], MF_CHUNK), ny), 256, 0, s>>>(
+                lst, m->d_meta, K_vals, m->d_slot, m->d_off, m->d_fdof, m->d_scale, ws);
+            for (int c = 0; c < 2; c++)
+                mf_ea_kernel<T><<<dim3(nblk(maxb * maxb, MF_CHUNK), ny), 256, 0, s>>>(lst, m->d_meta, c, m->d_ea, upd, ws);
+            for (int k = 0; k < m->lvl_max_e[L]; k += MF_NB) {
+                mf_diag_kernel<T><<<ny, 32, 0, s>>>(lst, m->d_meta, k, ws, m->inv, invc, m->piv, m->d_npert);
+                long long mm = maxn - k - 1;
+                if (mm < 1) mm = 1;
+                mf_panel_kernel<T><<<dim3(nblk(2 * mm, 256), ny), 256, 0, s>>>(lst, m->d_meta, k, ws, invc, m->piv);
+                long long nt = (mm + MF_TILE - 1) / MF_TILE;
+                mf_trail_kernel<T><<<dim3((unsigned)std::max(1LL, nt * nt), ny), 256, 0, s>>>(lst, m->d_meta, k, ws);
+            }
+            mf_compact_kernel<T><<<dim3(nblk(maxn * maxn, MF_CHUNK), ny), 256, 0, s>>>(lst, m->d_meta, ws, m->fact, upd);
+            rc = check_cuda(cudaGetLastError(), "multifrontal factor level");
+        }
+    }
+    return rc;
+}
+
 
 extern "C" {
 
@@ -1102,11 +1214,46 @@ int emfem_mf_create(emfem_handle h, int64_t n, int n_fronts, const int32_t* e, c
 int emfem_mf_info(emfem_mf m, size_t* device_bytes, double* flops, int* n_levels) {
     EMFEM_REQUIRE(m, "emfem_mf_info: bad handle");
     if (device_bytes)
-        *device_bytes = sizeof(float2) * (m->fact_n + m->inv_n + m->ws_n + m->upd_n) + sizeof(int) * m->piv_n +
+        *device_bytes = sizeof(float2) * (m->fact_n + m->inv_n) + (m->wide ? sizeof(double2) : sizeof(float2)) *
+                        (m->ws_n + m->upd_n) + (m->wide ? sizeof(double2) * m->inv_n : 0) + sizeof(int) * m->piv_n +
                         sizeof(double) * m->n;
     if (flops) *flops = m->flops;
     if (n_levels) *n_levels = (int)m->levels.size();
     return EMFEM_OK;
+}
+
+int emfem_mf_set_precision(emfem_mf m, int bits) {
+    EMFEM_REQUIRE(m && (bits == 64 || bits == 128), "emfem_mf_set_precision: bits must be 64 or 128");
+    const bool wide = bits == 128;
+    if (wide == m->wide) return EMFEM_OK;
+    int prev = 0;
+    EMFEM_CUDA(cudaGetDevice(&prev));
+    if (prev != m->h->device) EMFEM_CUDA(cudaSetDevice(m->h->device));
+    EMFEM_CUDA(cudaStreamSynchronize(m->h->stream));
+    void* ps[] = {m->ws, m->upd, m->invc};
+    for (void* p : ps)
+        if (p) cudaFree(p);
+    m->ws = m->upd = m->invc = nullptr;
+    m->factored = false;
+    const size_t el = wide ? sizeof(double2) : sizeof(float2);
+    int rc = check_cuda(cudaMalloc(&m->ws, el * std::max(1LL, m->ws_n)), "cudaMalloc");
+    if (rc == EMFEM_OK) rc = check_cuda(cudaMalloc(&m->upd, el * std::max(1LL, m->upd_n)), "cudaMalloc");
+    if (rc == EMFEM_OK && wide) rc = check_cuda(cudaMalloc(&m->invc, sizeof(double2) * std::max(1LL, m->inv_n)), "cudaMalloc");
+    if (rc == EMFEM_OK) {
+        m->wide = wide;
+    } else {
+        // leave a usable complex64 handle behind when the complex128 workspace does not fit
+        void* qs[] = {m->ws, m->upd, m->invc};
+        for (void* p : qs)
+            if (p) cudaFree(p);
+        m->ws = m->upd = m->invc = nullptr;
+        m->wide = false;
+        if (cudaMalloc(&m->ws, sizeof(float2) * std::max(1LL, m->ws_n)) != cudaSuccess ||
+            cudaMalloc(&m->upd, sizeof(float2) * std::max(1LL, m->upd_n)) != cudaSuccess)
+            set_error("emfem_mf_set_precision: the complex64 workspace could not be restored either");
+    }
+    if (prev != m->h->device) cudaSetDevice(prev);
+    return rc;
 }
 
 int emfem_mf_factor(emfem_mf m, const void* K_vals, int* n_perturbed) {
@@ -1132,31 +1279,9 @@ int emfem_mf_factor(emfem_mf m, const void* K_vals, int* n_perturbed) {
             }
         rc = check_cuda(cudaGetLastError(), "multifrontal equilibration");
     }
-    for (int L = 0; L < nl && rc == EMFEM_OK; L++) {
-        const int nfl = (int)m->levels[L].size();
-        long long wsz = 0;
-        for (int v : m->levels[L]) wsz += (long long)m->meta[v].n * m->meta[v].n;
-        rc = check_cuda(cudaMemsetAsync(m->ws, 0, sizeof(float2) * wsz, s), "cudaMemsetAsync");
-        for (int y0 = 0; y0 < nfl && rc == EMFEM_OK; y0 += 65535) {
-            const int ny = std::min(65535, nfl - y0);
-            const int* lst = m->d_lst + m->lvl_off[L] + y0;
-            long long maxn = m->lvl_max_n[L], maxb = m->lvl_max_b[L];
-            mf_asm_kernel<<<dim3(nblk(m->lvl_max_asm[L], MF_CHUNK), ny), 256, 0, s>>>(
-                lst, m->d_meta, (const double2*)K_vals, m->d_slot, m->d_off, m->d_fdof, m->d_scale, m->ws);
-            for (int c = 0; c < 2; c++)
-                mf_ea_kernel<<<dim3(nblk(maxb * maxb, MF_CHUNK), ny), 256, 0, s>>>(lst, m->d_meta, c, m->d_ea, m->upd, m->ws);
-            for (int k = 0; k < m->lvl_max_e[L]; k += MF_NB) {
-                mf_diag_kernel<<<ny, 32, 0, s>>>(lst, m->d_meta, k, m->ws, m->inv, m->piv, m->d_npert);
-                long long mm = maxn - k - 1;
-                if (mm < 1) mm = 1;
-                mf_panel_kernel<<<dim3(nblk(2 * mm, 256), ny), 256, 0, s>>>(lst, m->d_meta, k, m->ws, m->inv, m->piv);
-                long long nt = (mm + MF_TILE - 1) / MF_TILE;
-                mf_trail_kernel<<<dim3((unsigned)std::max(1LL, nt * nt), ny), 256, 0, s>>>(lst, m->d_meta, k, m->ws);
-            }
-            mf_compact_kernel<<<dim3(nblk(maxn * maxn, MF_CHUNK), ny), 256, 0, s>>>(lst, m->d_meta, m->ws, m->fact, m->upd);
-            rc = check_cuda(cudaGetLastError(), "multifrontal factor level");
-        }
-    }
+    if (rc == EMFEM_OK)
+        rc = m->wide ? mf_factor_levels<double2>(m, (const double2*)K_vals, s)
+                     : mf_factor_levels<float2>(m, (const double2*)K_vals, s);
     int np = 0;
     if (rc == EMFEM_OK) rc = check_cuda(cudaMemcpyAsync(&np, m->d_npert, sizeof(int), cudaMemcpyDeviceToHost, s), "copy");
     if (rc == EMFEM_OK) rc = check_cuda(cudaStreamSynchronize(s), "sync");

@@ -286,10 +286,13 @@ class DeviceLU:
 
     The structure (ordering, fronts, assembly lists) is built once per mesh and PEC set; ``factor(f)``
     forms K_f = E − k0²B + Σ_p γ_p(k0) R_p on the device (``emfem_sweep_combine``; the Robin/port entries
-    summed per CSR slot) and factors it in complex64.  ``solve`` applies (LU)⁻¹; the sweep uses it as the
-    preconditioner of FP64 BiCGStab (:meth:`FrequencySweep.solve_lu`), also at neighbouring frequencies."""
+    summed per CSR slot) and factors its equilibrated form.  ``precision`` is the arithmetic of the
+    factorization: "c64" (complex64 fronts) or "c128" (complex128 fronts and update store, twice their
+    memory, about half the speed); the factors the solves read are complex64 either way.  ``solve``
+    applies (LU)⁻¹; the sweep uses it as the preconditioner of FP64 BiCGStab
+    (:meth:`FrequencySweep.solve_lu`), also at neighbouring frequencies."""
 
-    def __init__(self, sweep, leaf_tets: int = 64):
+    def __init__(self, sweep, leaf_tets: int = 64, precision: str = "c64"):
         import ctypes
         import time
         import torch
@@ -335,8 +338,27 @@ class DeviceLU:
                            torch.from_numpy(seg).to(self.device), torch.from_numpy(idx).to(self.device))
         self.frequency = None
         self.n_perturbed = 0
+        self.precision = "c64"
+        self.set_precision(precision)
         self.seconds_create = time.perf_counter() - t0
         self._reserved = 0
+
+    def set_precision(self, precision: str) -> "DeviceLU":
+        """Switch the factorization arithmetic ("c64" or "c128"); reallocates the workspace and drops the
+        current factorization.  If the complex128 workspace does not fit, the LU stays complex64 and
+        this raises."""
+        from ._lib import check, lib
+        if precision not in ("c64", "c128"):
+            raise ValueError(f"DeviceLU: precision must be 'c64' or 'c128', not {precision!r}")
+        if precision != self.precision:
+            self.frequency = None
+            check(lib().emfem_mf_set_precision(self._p, 128 if precision == "c128" else 64), "emfem_mf_set_precision")
+            self.precision = precision
+            import ctypes
+            nb, fl, nl = ctypes.c_size_t(), ctypes.c_double(), ctypes.c_int()
+            check(lib().emfem_mf_info(self._p, ctypes.byref(nb), ctypes.byref(fl), ctypes.byref(nl)), "emfem_mf_info")
+            self.device_bytes = nb.value
+        return self
 
     def __del__(self):
         p = getattr(self, "_p", None)

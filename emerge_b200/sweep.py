@@ -491,18 +491,29 @@ class FrequencySweep:
         return self._lu
 
     def solve_direct(self, systems, window: int = 5, tol: float = 1e-8, maxit: int = 400, adaptive: bool = False,
-                     iter_band: tuple = (20, 40), max_window: int = 15) -> SolveResult:
+                     iter_band: tuple = (20, 40), max_window: int = 15, precision: str = "c64",
+                     probe_maxit: int = 60) -> SolveResult:
         """Every listed (frequency, port) system through the device LU, the GPU counterpart of the
         reference's direct solve per frequency (``SolverSuperLU``, LU reused across the ports of a
         frequency, ``MW/simjob.py:82-107``).  The distinct frequencies, ascending, are cut into windows of
-        ``window`` consecutive ones; each window's middle frequency is factored (complex64) and all systems
-        of the window are solved together by FP64 BiCGStab preconditioned with that factorization (at
-        the factored frequency a couple of refinement steps, at its neighbours a Krylov solve of the
-        shifted operator).  With ``adaptive``, each window's width follows the previous one's largest
-        iteration count: wider by 2 below ``iter_band[0]``, narrower by 2 above ``iter_band[1]`` (between 3
-        and ``max_window``), since the shifted systems at a window's edges need more iterations where the
-        cavity's modes are denser.  Results come back in the order of ``systems``; ``windows`` on the
-        result lists (factored frequency, systems, factor seconds, solve seconds, iterations) per window."""
+        ``window`` consecutive ones; each window's middle frequency is factored and all systems of the
+        window are solved together by FP64 BiCGStab preconditioned with that factorization (at the
+        factored frequency a couple of refinement steps, at its neighbours a Krylov solve of the shifted
+        operator).  With ``adaptive``, each window's width follows the previous one's largest iteration
+        count: wider by 2 below ``iter_band[0]``, narrower by 2 above ``iter_band[1]`` (between 3 and
+        ``max_window``), since the shifted systems at a window's edges need more iterations where the
+        cavity's modes are denser.
+
+        ``precision`` is the factorization's arithmetic: "c64", "c128", or "auto": each window is first
+        tried with a complex64 factorization and at most ``probe_maxit`` iterations; the systems it leaves
+        unconverged are solved again from a complex128 factorization at the same frequency (at low
+        frequency the near-null gradient space makes K ill-conditioned enough that complex64 fronts give
+        no usable preconditioner).  After a complex128 window that needed fewer than ``iter_band[0]``
+        iterations, the next window tries complex64 again.  Results come back in the order of
+        ``systems``; ``windows`` on the result lists (factored frequency, precision, systems, factor
+        seconds, solve seconds, iterations) per attempt."""
+        if precision not in ("c64", "c128", "auto"):
+            raise ValueError(f"solve_direct: precision must be 'c64', 'c128' or 'auto', not {precision!r}")
         lu = self.direct_solver()
         freqs = sorted({f for f, _ in systems})
         n = len(systems)
@@ -513,25 +524,47 @@ class FrequencySweep:
         t0 = time.perf_counter()
         log = []
         w0, W = 0, window
+        first = "c128" if precision == "c128" else "c64"
         while w0 < len(freqs):
             wf = freqs[w0:w0 + W]
             w0 += len(wf)
-            idx = [j for j, (f, _) in enumerate(systems) if f in set(wf)]
+            fw = set(wf)
+            todo = [j for j, (f, _) in enumerate(systems) if f in fw]
+            fc = wf[len(wf) // 2]
             imax = 0
-            tf = time.perf_counter()
-            lu.factor(wf[len(wf) // 2])
-            tf = time.perf_counter() - tf
-            for c0 in range(0, len(idx), 64):
-                sub = idx[c0:c0 + 64]
-                r = self.solve_lu([systems[j] for j in sub], lu, tol=tol, maxit=maxit)
-                x[:, sub] = r.x
-                status[sub] = r.status
-                iters[sub] = r.iters
-                relres[sub] = r.relres
-                log.append(dict(factored=wf[len(wf) // 2], systems=len(sub), factor_seconds=tf,
-                                solve_seconds=r.seconds, iters=r.iters.tolist(), perturbed=lu.n_perturbed))
-                tf = 0.0
-                imax = max(imax, int(r.iters.max()))
+            attempts = [first] if precision != "auto" or first == "c128" else ["c64", "c128"]
+            for prec in attempts:
+                if not todo:
+                    break
+                last = prec == attempts[-1]
+                imax = 0                          # the window width follows the attempt that finished it
+                lu.set_precision(prec)
+                tf = time.perf_counter()
+                lu.factor(fc)
+                tf = time.perf_counter() - tf
+                it_cap = maxit if last else min(maxit, probe_maxit)
+                left = []
+                for c0 in range(0, len(todo), 64):
+                    sub = todo[c0:c0 + 64]
+                    r = self.solve_lu([systems[j] for j in sub], lu, tol=tol, maxit=it_cap)
+                    ok = (r.status == 0) & (r.relres <= tol)
+                    keep = [i for i in range(len(sub)) if ok[i] or last]
+                    ks = [sub[i] for i in keep]
+                    x[:, ks] = r.x[:, keep]
+                    status[ks] = r.status[keep]
+                    iters[ks] = r.iters[keep]
+                    relres[ks] = r.relres[keep]
+                    left += [sub[i] for i in range(len(sub)) if not (ok[i] or last)]
+                    log.append(dict(factored=fc, precision=prec, systems=len(sub), factor_seconds=tf,
+                                    solve_seconds=r.seconds, iters=r.iters.tolist(), perturbed=lu.n_perturbed))
+                    tf = 0.0
+                    imax = max(imax, int(r.iters[keep].max()) if keep else it_cap)
+                todo = left
+                if precision == "auto":
+                    if prec == "c128":
+                        first = "c64" if imax < iter_band[0] else "c128"
+                    elif left:
+                        first = "c128"
             if adaptive:
                 if imax > iter_band[1] and W > 3:
                     W = max(3, W - 2)

@@ -107,6 +107,11 @@ int emfem_plan_assemble(emfem_plan plan, int64_t n_nodes, int64_t n_edges, const
  * whose chunk cannot hold the mesh's largest edge/face incidence are unavailable. */
 int emfem_plan_variants(emfem_plan plan, int *n_variants, int *current);
 int emfem_plan_set_variant(emfem_plan plan, int variant);
+/* Variant v: chunk capacity (incidences), threads per CTA, whether it is table-driven (1: pair blocks as
+ * the canonical recipes' sparse linear forms, values within rounding of the others; 0: the reference's
+ * formulas entry by entry, bit-identical across such variants) and whether this mesh can use it. */
+int emfem_plan_variant_info(emfem_plan plan, int variant, int *chunk, int *threads, int *table_driven,
+                            int *available);
 /* CSR slot of each (row, col) pair (device int64 arrays of length n), -1 where absent. */
 int emfem_plan_find_slots(emfem_plan plan, int64_t n, const int64_t *rows, const int64_t *cols,
                           int32_t *slots);
@@ -377,6 +382,10 @@ int emfem_adam_step(emfem_handle h, int64_t n, float *params, const float *grad,
  *   undoes the scaling; *n_perturbed (host) gets the number of pivots raised to 1e-6 of their 32 x 32
  *   block's largest entry (pivoting is partial inside each 32-row diagonal block).  Synchronises the
  *   stream.
+ * set_precision: bits = 64 (default) factors in complex64, 128 in complex128 (the level workspace and
+ *   the update store double in size; the factor store stays complex64, rounded once at compaction).
+ *   Reallocates the workspace and drops the factorization; on an allocation failure the handle stays
+ *   complex64 and the call returns the error.
  * reserve: solve buffers for up to nrhs right-hand sides (<= 256).
  * solve: x = (LU)^-1 b for nrhs right-hand sides, b and x (n, nrhs) c128 DOF-major, device; x is zero on
  *   DOFs that belong to no front (PEC).
@@ -391,6 +400,7 @@ int emfem_mf_create(emfem_handle h, int64_t n, int n_fronts, const int32_t *e, c
 int emfem_mf_build_lists(emfem_mf lu, int64_t nnz, const int32_t *indptr, const int32_t *indices);
 int emfem_mf_info(emfem_mf lu, size_t *device_bytes, double *flops, int *n_levels);
 int emfem_mf_factor(emfem_mf lu, const void *K_vals, int *n_perturbed);
+int emfem_mf_set_precision(emfem_mf lu, int bits);
 int emfem_mf_reserve(emfem_mf lu, int nrhs);
 int emfem_mf_solve(emfem_mf lu, int nrhs, const void *b, void *x);
 int emfem_mf_destroy(emfem_mf lu);

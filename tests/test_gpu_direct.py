@@ -133,3 +133,58 @@ def test_partitioned_entry_points_on_one_rank(cuda):
     sl = [[(10e9, 0), (10e9, 1)] for _ in Ps]
     out = solve_meshes_partitioned(Ps, sl, tol=1e-8, maxit=20000, precond="aux")
     assert len(out) == 3 and all(d["status"] == 0 for per in out for d in per)
+
+
+def _substrate_direct(P, f):
+    """SuperLU on the oracle's K_f of a substrate box (lumped ports, order-2 ABC) for port 1."""
+    from oracle import abc2 as oabc2
+    k0 = k0_of(f)
+    E, B = oracle.tet_mass_stiffness_matrices(P.field, P.er, P.ur)
+    Bm = P.field.empty_tri_matrix()
+    pvs = []
+    for p in P.ports:
+        Bm, bp = oracle.assemble_robin_bc_excited(P.field, Bm, p.tri_ids, lambda x, y, z, p=p: p.get_Uinc(x, y, z, k0),
+                                                  p.get_gamma(k0), oracle.dunavant4())
+        pvs.append(bp)
+    for bc in P.robin:
+        Bm = oracle.assemble_robin_bc(P.field, Bm, bc.tri_ids, bc.get_gamma(k0))
+        Bm = Bm + oabc2.abc_order_2_matrix(P.field, bc.tri_ids, bc.get_gamma2(k0))
+    K = (E - B * k0 ** 2 + P.field.generate_csr(Bm)).tocsr()
+    return oracle.solve_routine(K, pvs[:1], P.solve_ids)[0]
+
+
+def test_complex128_factorization_at_low_frequency_matches_superlu(cuda):
+    """The complex128 factorization (emfem_mf_set_precision 128, complex64 factor store) of an
+    equilibrated substrate box at 1 GHz, where the gradient near-null space is strongest, under FP64
+    BiCGStab: the oracle's SuperLU solution to 1e-10, within a few iterations."""
+    P = problems.substrate_box(10, 8, 10)
+    sw = FrequencySweep(P)
+    lu = sw.direct_solver()
+    bytes64 = lu.device_bytes
+    lu.set_precision("c128")
+    assert lu.device_bytes > bytes64
+    f = 1e9
+    lu.factor(f)
+    r = sw.solve_lu([(f, 0)], lu, tol=1e-12, maxit=40)
+    assert r.status[0] == 0 and r.iters[0] <= 10, (r.status, r.iters, r.relres)
+    xs = _substrate_direct(P, f)
+    x = r.x[:, 0].cpu().numpy()
+    assert np.linalg.norm(x - xs) <= 1e-10 * np.linalg.norm(xs)
+    lu.set_precision("c64")
+    assert lu.device_bytes == bytes64 and lu.frequency is None
+
+
+def test_auto_precision_sweep_converges_every_frequency(cuda):
+    """solve_direct(precision="auto") over 1-8 GHz of a substrate box: every system converges to the
+    FP64 tolerance, and the solutions at the lowest and highest frequency match the oracle's SuperLU."""
+    P = problems.substrate_box(10, 8, 10)
+    sw = FrequencySweep(P)
+    freqs = [1e9, 1.5e9, 2e9, 4e9, 6e9, 8e9]
+    systems = [(f, 0) for f in freqs]
+    r = sw.solve_direct(systems, window=3, tol=1e-10, precision="auto")
+    assert (r.status == 0).all() and (r.relres <= 1e-10).all(), (r.status, r.iters, r.relres, r.windows)
+    assert {w["precision"] for w in r.windows} <= {"c64", "c128"}
+    for j in (0, len(freqs) - 1):
+        xs = _substrate_direct(P, freqs[j])
+        x = r.x[:, j].cpu().numpy()
+        assert np.linalg.norm(x - xs) <= 1e-8 * np.linalg.norm(xs), freqs[j]

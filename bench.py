@@ -729,8 +729,7 @@ def main():
                                          "scaled by tets; the invariants kernel adds ~1.4 KB/tet",
                          "peak_kind": peak_kind,
                          "alg_bytes_per_tet": alg_bytes_per_tet,
-                         "kernels": ("tet_canon_kernel+assemble_recipe_kernel" if tuned_info["table_driven"]
-                                     else "tet_invariants_kernel+assemble_chunk_kernel")},
+                         "kernels": "tet_invariants_kernel+assemble_chunk_kernel"},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
                     "api": "emerge_b200.assembly.tet_mass_stiffness_matrices (host numpy in, SciPy CSR out)"},
             "gpu_launches": 2 * args.steps,

@@ -59,7 +59,7 @@ _SIGS = {
     "emfem_plan_find_slots": ([_vp, _i64, _vp, _vp, _vp], _i32),
     "emfem_plan_variants": ([_vp, _i32p, _i32p], _i32),
     "emfem_plan_set_variant": ([_vp, _i32], _i32),
-    "emfem_plan_variant_info": ([_vp, _i32, _i32p, _i32p, _i32p, _i32p], _i32),
+    "emfem_plan_variant_info": ([_vp, _i32, _i32p, _i32p, _i32p], _i32),
     "emfem_ned2_tri_robin": ([_vp, _i64, _vp, _i64, _vp, _dbl, _dbl, _vp, _vp, _i32, _vp, _vp], _i32),
     "emfem_segmented_gather_sum": ([_vp, _i64, _vp, _vp, _vp, _vp], _i32),
     "emfem_sweep_combine": ([_vp, _i64, _vp, _vp, _dbl, _i64, _vp, _vp, _dbl, _dbl, _vp], _i32),

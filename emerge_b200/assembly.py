@@ -146,11 +146,11 @@ class CsrPlan:
         check(lib().emfem_plan_set_variant(self._p, int(v)), "emfem_plan_set_variant")
 
     def variant_info(self, v: int) -> dict:
-        """Chunk capacity, threads per CTA, table-driven flag and availability of kernel variant ``v``."""
-        ch, nt, td, av = (ctypes.c_int() for _ in range(4))
-        check(lib().emfem_plan_variant_info(self._p, int(v), ctypes.byref(ch), ctypes.byref(nt), ctypes.byref(td),
-                                            ctypes.byref(av)), "emfem_plan_variant_info")
-        return {"chunk": ch.value, "threads": nt.value, "table_driven": bool(td.value), "available": bool(av.value)}
+        """Chunk capacity, threads per CTA and availability (for this mesh) of kernel variant ``v``."""
+        ch, nt, av = (ctypes.c_int() for _ in range(3))
+        check(lib().emfem_plan_variant_info(self._p, int(v), ctypes.byref(ch), ctypes.byref(nt), ctypes.byref(av)),
+              "emfem_plan_variant_info")
+        return {"chunk": ch.value, "threads": nt.value, "available": bool(av.value)}
 
     def tune(self, er: torch.Tensor, ur: torch.Tensor, reps: int = 3, cache: str | None = None) -> dict:
         """Autotune the assembly kernel variant (chunk capacity x CTA size) for this mesh on this GPU.

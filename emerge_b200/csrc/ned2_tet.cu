@@ -12,7 +12,6 @@
 //     buffer; the pattern equals SciPy's tocsr() of the reference COO (sorted rows, zeros kept).
 #include "emfem_internal.cuh"
 #include "ned2_math.cuh"
-#include "ned2_canon.cuh"
 
 #include <vector>
 
@@ -63,45 +62,6 @@ __global__ void __launch_bounds__(128) tet_invariants_kernel(
     tet_invariants(xs, ys, zs, ids, el, U, E, out);
     if (!(out[INV_SF] < 1e300)) flag(status, DEV_DEGENERATE);
     if (!finite) flag(status, DEV_NONFINITE);
-}
-
-// The same invariants, permuted into the canonical record (ned2_canon.cuh) the table-driven assembly reads.
-__global__ void __launch_bounds__(128) tet_canon_kernel(
-    long long nt, long long nn, long long ne, const double* __restrict__ nodes,
-    const int64_t* __restrict__ tets, const int64_t* __restrict__ t2e, const double* __restrict__ elen,
-    const double2* __restrict__ ur, const double2* __restrict__ er, double* __restrict__ can, int* status) {
-    long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= nt) return;
-    int64_t ids[4];
-    double xs[4], ys[4], zs[4], el[6];
-    bool bad = false, finite = true;
-#pragma unroll
-    for (int i = 0; i < 4; i++) {
-        int64_t v = tets[i * nt + t];
-        if (v < 0 || v >= nn) { bad = true; v = 0; }
-        ids[i] = v;
-        xs[i] = nodes[v]; ys[i] = nodes[nn + v]; zs[i] = nodes[2 * nn + v];
-        finite &= isfinite(xs[i]) && isfinite(ys[i]) && isfinite(zs[i]);
-    }
-#pragma unroll
-    for (int e = 0; e < 6; e++) {
-        int64_t id = t2e[e * nt + t];
-        if (id < 0 || id >= ne) { bad = true; id = 0; }
-        el[e] = elen[id];
-        finite &= isfinite(el[e]);
-    }
-    if (bad) flag(status, DEV_BAD_INDEX);
-    cd U[9], E[9];
-#pragma unroll
-    for (int k = 0; k < 9; k++) {
-        U[k] = load_c(ur, k * nt + t); E[k] = load_c(er, k * nt + t);
-        finite &= isfinite(U[k].x) && isfinite(U[k].y) && isfinite(E[k].x) && isfinite(E[k].y);
-    }
-    double loc[INV_STRIDE];
-    tet_invariants(xs, ys, zs, ids, el, U, E, loc);
-    if (!(loc[INV_SF] < 1e300)) flag(status, DEV_DEGENERATE);
-    if (!finite) flag(status, DEV_NONFINITE);
-    canon_record(loc, can + t * CAN_STRIDE);
 }
 
 __device__ __forceinline__ void load_vtab(double* sh) {
@@ -491,135 +451,9 @@ __global__ void __launch_bounds__(NT, MINB) assemble_chunk_kernel(
     }
 }
 
-// ---------------------------------------------------------------- table-driven (canonical) assembly
-// Same chunks, phases and staging as assemble_chunk_kernel, but phase 1 evaluates every pair block as
-// the fixed sparse linear form of its canonical entity pair (ned2_canon.cuh): the tet's local slots are
-// mapped to canonical ones by its rank code, and the block's D and F entries are sums of recipe
-// coefficients times the canonical invariants, scaled by the entities' length factors.  No orientation
-// decoding, no volume-table indexing: about 2 900 complex multiply-adds per tet.
-template <int ND>
-__device__ __forceinline__ void recipe_block(const double2* __restrict__ cr, const PackedRecipes* __restrict__ R,
-                                             int b, double rx0, double rx1, double ry0, double ry1, double sD,
-                                             double sF, double2 d[4], double2 f[4]) {
-    const int oD = R->offD[b], oF = 16 * b;
-#pragma unroll
-    for (int q = 0; q < 4; q++) {
-        double ax = 0.0, ay = 0.0, bx = 0.0, by = 0.0;
-#pragma unroll
-        for (int k = 0; k < ND; k++) {
-            const double c = R->coefD[oD + q * ND + k];
-            const double2 v = __ldg(&cr[CAN_Q / 2 + R->idxD[oD + q * ND + k]]);
-            ax = fma(c, v.x, ax);
-            ay = fma(c, v.y, ay);
-        }
-#pragma unroll
-        for (int k = 0; k < RCP_NF; k++) {
-            const double c = R->coefF[oF + 4 * q + k];
-            const double2 v = __ldg(&cr[CAN_P / 2 + R->idxF[oF + 4 * q + k]]);
-            bx = fma(c, v.x, bx);
-            by = fma(c, v.y, by);
-        }
-        const double rxy = (q < 2 ? rx0 : rx1) * ((q & 1) ? ry1 : ry0);
-        const double tD = rxy * sD, tF = rxy * sF;
-        d[q] = make_double2(ax * tD, ay * tD);
-        f[q] = make_double2(bx * tF, by * tF);
-    }
-}
-
-template <int CH>
-struct RecipeSmem {
-    static constexpr size_t stage = (size_t)(CH + 1) * 10 * 8 * 16;
-    static constexpr size_t rec = (size_t)CH * 16;
-    static constexpr size_t code = (size_t)CH * 4;
-    static constexpr size_t off_rec = stage;
-    static constexpr size_t off_code = off_rec + rec;
-    static constexpr size_t off_ent = off_code + code;
-    static constexpr size_t total = off_ent + (size_t)(2 * CH + 2) * 4;
-};
-
-template <int CH, int NT, int MINB>
-__global__ void __launch_bounds__(NT, MINB) assemble_recipe_kernel(
-    const int* __restrict__ chunk_ptr, long long H, const int* __restrict__ mptr,
-    const int* __restrict__ inc_ptr, const uint32_t* __restrict__ inc_code, const uint4* __restrict__ rec,
-    const double* __restrict__ can, const PackedRecipes* __restrict__ R, double2* __restrict__ Ev,
-    double2* __restrict__ Bv) {
-    typedef RecipeSmem<CH> L;
-    extern __shared__ __align__(16) unsigned char smem[];
-    double2* stage = reinterpret_cast<double2*>(smem);                 // [q][sy][CH + 1] (padded rows)
-    uint4* srec = reinterpret_cast<uint4*>(smem + L::off_rec);         // CH
-    uint32_t* scode = reinterpret_cast<uint32_t*>(smem + L::off_code); // CH
-    int* smptr = reinterpret_cast<int*>(smem + L::off_ent);             // chunk entities' mptr, X0..X1
-    int* sinc = smptr + CH + 1;                                          // chunk entities' inc_ptr - i0
-    const int X0 = chunk_ptr[blockIdx.x], X1 = chunk_ptr[blockIdx.x + 1];
-    const int i0 = inc_ptr[X0], ninc = inc_ptr[X1] - i0;
-    const int nent = X1 - X0;
-    for (int li = threadIdx.x; li < ninc; li += NT) {
-        srec[li] = rec[i0 + li];
-        scode[li] = inc_code[i0 + li];
-    }
-    for (int e = threadIdx.x; e <= nent; e += NT) {
-        smptr[e] = mptr[X0 + e];
-        sinc[e] = inc_ptr[X0 + e] - i0;
-    }
-    __syncthreads();
-    // phase 1: edge columns of every incidence, then face columns (warp-uniform block kinds)
-    for (int w = threadIdx.x; w < 10 * ninc; w += NT) {
-        int sy, li;
-        if (w < 6 * ninc) { li = w / 6; sy = w - 6 * li; }
-        else { int u = w - 6 * ninc; li = u >> 2; sy = 6 + (u & 3); }
-        const int sx = (int)((srec[li].z >> 16) & 0xff);  // byte 10 of the record
-        const double* c = can + (long long)(scode[li] >> 4) * CAN_STRIDE;
-        const double2* cr = reinterpret_cast<const double2*>(c);
-        const int code = (int)__ldg(&c[CAN_RANK]);
-        const int csx = canon_slot(sx, code), csy = canon_slot(sy, code);
-        const double2 rx = __ldg(&cr[CAN_R / 2 + csx]), ry = __ldg(&cr[CAN_R / 2 + csy]);
-        const double2 sc = __ldg(&cr[CAN_SD / 2]);
-        const int b = 10 * csx + csy;
-        double2 d[4], f[4];
-        const bool xe = sx < 6, ye = sy < 6;
-        if (xe && ye) recipe_block<RCP_ND_EE>(cr, R, b, rx.x, rx.y, ry.x, ry.y, sc.x, sc.y, d, f);
-        else if (xe != ye) recipe_block<RCP_ND_EF>(cr, R, b, rx.x, rx.y, ry.x, ry.y, sc.x, sc.y, d, f);
-        else recipe_block<RCP_ND_FF>(cr, R, b, rx.x, rx.y, ry.x, ry.y, sc.x, sc.y, d, f);
-#pragma unroll
-        for (int q = 0; q < 4; q++) {
-            stage[(q * 10 + sy) * (CH + 1) + li] = d[q];
-            stage[((4 + q) * 10 + sy) * (CH + 1) + li] = f[q];
-        }
-    }
-    __syncthreads();
-    // phase 2 (as assemble_chunk_kernel): one thread per output (X, k), tets in ascending order
-    const int m0 = smptr[0], total = smptr[nent] - m0;
-    const long long two_mH = 2LL * mptr[H];
-    for (int o = threadIdx.x; o < total; o += NT) {
-        int j = m0 + o;
-        int lo = 0, hi = nent;
-        while (hi - lo > 1) { int mid = (lo + hi) >> 1; if (smptr[mid] <= j) lo = mid; else hi = mid; }
-        const int mb = smptr[lo], k = j - mb, m = smptr[lo + 1] - mb;
-        double2 acc[8];
-#pragma unroll
-        for (int q = 0; q < 8; q++) acc[q] = make_double2(0.0, 0.0);
-        for (int li = sinc[lo]; li < sinc[lo + 1]; li++) {
-            uint4 r4 = srec[li];
-            uint32_t wds[4] = {r4.x, r4.y, r4.z, r4.w};
-            int sy = -1;
-#pragma unroll
-            for (int q = 0; q < 10; q++) if ((int)((wds[q >> 2] >> (8 * (q & 3))) & 0xff) == k) sy = q;
-            if (sy < 0) continue;
-#pragma unroll
-            for (int q = 0; q < 8; q++) {
-                double2 v = stage[(q * 10 + sy) * (CH + 1) + li];
-                acc[q].x += v.x; acc[q].y += v.y;
-            }
-        }
-        long long b1 = 2LL * mb + k, b2 = two_mH + 2LL * mb + k;
-        Ev[b1] = acc[0]; Ev[b1 + m] = acc[1]; Ev[b2] = acc[2]; Ev[b2 + m] = acc[3];
-        Bv[b1] = acc[4]; Bv[b1 + m] = acc[5]; Bv[b2] = acc[6]; Bv[b2 + m] = acc[7];
-    }
-}
-
 // Kernel variants: chunk capacity CH incidences, NT threads, min resident CTAs, invariants staged in
 // shared memory or read through L1.  The plan times them and keeps the fastest.
-struct AsmVariant { int ch; int nt; size_t smem; bool recipe; };
+struct AsmVariant { int ch; int nt; size_t smem; };
 #define EMFEM_ASM_VARIANTS(X)              \
     X(0, 32, 160, 2, true, false)          \
     X(1, 32, 160, 4, false, false)         \
@@ -634,29 +468,18 @@ struct AsmVariant { int ch; int nt; size_t smem; bool recipe; };
     X(10, 64, 256, 2, false, true)         \
     X(11, 32, 128, 4, false, true)         \
     X(12, 64, 192, 3, false, true)
-// table-driven (canonical recipe) variants: chunk capacity, threads, min resident CTAs
-#define EMFEM_RCP_VARIANTS(X)              \
-    X(13, 64, 320, 2)                      \
-    X(14, 64, 256, 2)                      \
-    X(15, 32, 160, 4)                      \
-    X(16, 32, 128, 5)                      \
-    X(17, 32, 192, 4)
-constexpr int N_ASM_VARIANTS = 18;
+constexpr int N_ASM_VARIANTS = 13;
 constexpr int DEFAULT_ASM_VARIANT = 6;
-#define EMFEM_V_ENTRY(i, ch, nt, mb, si, lm) {ch, nt, ChunkSmem<ch, si>::total, false},
-#define EMFEM_R_ENTRY(i, ch, nt, mb) {ch, nt, RecipeSmem<ch>::total, true},
-static const AsmVariant ASM_VARIANTS[N_ASM_VARIANTS] = {EMFEM_ASM_VARIANTS(EMFEM_V_ENTRY) EMFEM_RCP_VARIANTS(EMFEM_R_ENTRY)};
+#define EMFEM_V_ENTRY(i, ch, nt, mb, si, lm) {ch, nt, ChunkSmem<ch, si>::total},
+static const AsmVariant ASM_VARIANTS[N_ASM_VARIANTS] = {EMFEM_ASM_VARIANTS(EMFEM_V_ENTRY)};
 
 static void launch_asm_variant(int v, unsigned grid, cudaStream_t s, const int* chunk_ptr, long long H, const int* mptr,
                                const int* inc_ptr, const uint32_t* inc_code, const uint4* rec, const double* inv,
-                               const PackedRecipes* rcp, double2* E, double2* B) {
+                               double2* E, double2* B) {
     switch (v) {
 #define EMFEM_V_LAUNCH(i, ch, nt, mb, si, lm) \
     case i: assemble_chunk_kernel<ch, nt, mb, si, lm><<<grid, nt, ASM_VARIANTS[i].smem, s>>>(chunk_ptr, H, mptr, inc_ptr, inc_code, rec, inv, E, B); break;
         EMFEM_ASM_VARIANTS(EMFEM_V_LAUNCH)
-#define EMFEM_R_LAUNCH(i, ch, nt, mb) \
-    case i: assemble_recipe_kernel<ch, nt, mb><<<grid, nt, ASM_VARIANTS[i].smem, s>>>(chunk_ptr, H, mptr, inc_ptr, inc_code, rec, inv, rcp, E, B); break;
-        EMFEM_RCP_VARIANTS(EMFEM_R_LAUNCH)
     default: break;
     }
 }
@@ -666,9 +489,6 @@ static cudaError_t set_asm_smem_attributes() {
 #define EMFEM_V_ATTR(i, ch, nt, mb, si, lm) \
     if (e == cudaSuccess) e = cudaFuncSetAttribute(assemble_chunk_kernel<ch, nt, mb, si, lm>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ASM_VARIANTS[i].smem);
     EMFEM_ASM_VARIANTS(EMFEM_V_ATTR)
-#define EMFEM_R_ATTR(i, ch, nt, mb) \
-    if (e == cudaSuccess) e = cudaFuncSetAttribute(assemble_recipe_kernel<ch, nt, mb>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ASM_VARIANTS[i].smem);
-    EMFEM_RCP_VARIANTS(EMFEM_R_ATTR)
     return e;
 }
 
@@ -704,24 +524,16 @@ struct emfem_plan_s {
     uint8_t* rec = nullptr;        // 16 * 10 nt
     int* mptr = nullptr;           // H + 1
     int* S = nullptr;              // sum_m
-    double* inv = nullptr;         // per-tet invariants (INV_STRIDE) or canonical records (CAN_STRIDE), per variant
-    PackedRecipes* rcp = nullptr;  // recipe tables of the table-driven variants
+    double* inv = nullptr;         // INV_STRIDE * nt (array of structs)
     int* chunk_ptr[N_ASM_VARIANTS] = {nullptr};   // per variant: n_chunks + 1 entity boundaries
     int n_chunks[N_ASM_VARIANTS] = {0};
     int variant = 0;                                 // kernel variant used by emfem_plan_assemble
 };
 
-// The recipe tables, read off pair_block once per process (thread-safe static initialisation).
-static const PackedRecipes* host_recipes() {
-    static PackedRecipes r;
-    static const bool ok = pack_recipes(r);
-    return ok ? &r : nullptr;
-}
-
 static void plan_free(emfem_plan p) {
     if (!p) return;
     cudaFree(p->inc_ptr); cudaFree(p->inc_code); cudaFree(p->rec);
-    cudaFree(p->mptr); cudaFree(p->S); cudaFree(p->inv); cudaFree(p->rcp);
+    cudaFree(p->mptr); cudaFree(p->S); cudaFree(p->inv);
     for (int v = 0; v < N_ASM_VARIANTS; v++) cudaFree(p->chunk_ptr[v]);
     delete p;
 }
@@ -781,11 +593,7 @@ int emfem_plan_create(emfem_handle h, int64_t n_tets, int64_t n_edges, int64_t n
     PTRY(check_cuda(cudaMalloc(&p->inc_code, 10 * n_tets * sizeof(uint32_t)), "cudaMalloc(inc_code)"));
     PTRY(check_cuda(cudaMalloc(&p->rec, 10 * n_tets * (size_t)INC_REC), "cudaMalloc(rec)"));
     PTRY(check_cuda(cudaMalloc(&p->mptr, (H + 1) * sizeof(int)), "cudaMalloc(mptr)"));
-    PTRY(check_cuda(cudaMalloc(&p->inv, (size_t)std::max(INV_STRIDE, CAN_STRIDE) * n_tets * sizeof(double)),
-                    "cudaMalloc(inv)"));
-    if (!host_recipes()) { set_error("emfem_plan_create: recipe tables exceed their capacity"); st = EMFEM_ERR_INVALID_ARG; goto fail; }
-    PTRY(check_cuda(cudaMalloc(&p->rcp, sizeof(PackedRecipes)), "cudaMalloc(rcp)"));
-    PTRY(check_cuda(cudaMemcpy(p->rcp, host_recipes(), sizeof(PackedRecipes), cudaMemcpyHostToDevice), "copy(rcp)"));
+    PTRY(check_cuda(cudaMalloc(&p->inv, (size_t)INV_STRIDE * n_tets * sizeof(double)), "cudaMalloc(inv)"));
     PTRY(check_cuda(cudaMalloc(&cnt, H * sizeof(int)), "cudaMalloc(cnt)"));
     PTRY(check_cuda(cudaMalloc(&cursor, H * sizeof(int)), "cudaMalloc(cursor)"));
     PTRY(check_cuda(cudaMalloc(&scratch, nscr * sizeof(int)), "cudaMalloc(scan)"));
@@ -912,20 +720,13 @@ int emfem_plan_assemble(emfem_plan p, int64_t n_nodes, int64_t n_edges, const do
                   "emfem_plan_assemble: null argument");
     EMFEM_REQUIRE(n_edges == p->ne, "emfem_plan_assemble: n_edges differs from the plan's");
     cudaStream_t s = p->h->stream;
+    tet_invariants_kernel<<<grid_for(p->nt, 128), 128, 0, s>>>(p->nt, n_nodes, n_edges, nodes, tets, tet_to_edge,
+                                                                edge_lengths, (const double2*)ur, (const double2*)er,
+                                                                p->inv, p->h->dev_status);
+    EMFEM_LAUNCH("tet_invariants_kernel");
     const int v = p->variant;
-    if (ASM_VARIANTS[v].recipe) {
-        tet_canon_kernel<<<grid_for(p->nt, 128), 128, 0, s>>>(p->nt, n_nodes, n_edges, nodes, tets, tet_to_edge,
-                                                               edge_lengths, (const double2*)ur, (const double2*)er,
-                                                               p->inv, p->h->dev_status);
-        EMFEM_LAUNCH("tet_canon_kernel");
-    } else {
-        tet_invariants_kernel<<<grid_for(p->nt, 128), 128, 0, s>>>(p->nt, n_nodes, n_edges, nodes, tets, tet_to_edge,
-                                                                    edge_lengths, (const double2*)ur, (const double2*)er,
-                                                                    p->inv, p->h->dev_status);
-        EMFEM_LAUNCH("tet_invariants_kernel");
-    }
     launch_asm_variant(v, (unsigned)p->n_chunks[v], s, p->chunk_ptr[v], p->H, p->mptr, p->inc_ptr, p->inc_code,
-                       (const uint4*)p->rec, p->inv, p->rcp, (double2*)E_vals, (double2*)B_vals);
+                       (const uint4*)p->rec, p->inv, (double2*)E_vals, (double2*)B_vals);
     EMFEM_LAUNCH("assemble_chunk_kernel");
     return EMFEM_OK;
 }
@@ -937,11 +738,10 @@ int emfem_plan_variants(emfem_plan p, int* n_variants, int* current) {
     return EMFEM_OK;
 }
 
-int emfem_plan_variant_info(emfem_plan p, int variant, int* chunk, int* threads, int* table_driven, int* available) {
+int emfem_plan_variant_info(emfem_plan p, int variant, int* chunk, int* threads, int* available) {
     EMFEM_REQUIRE(p && variant >= 0 && variant < N_ASM_VARIANTS, "emfem_plan_variant_info: bad variant");
     if (chunk) *chunk = ASM_VARIANTS[variant].ch;
     if (threads) *threads = ASM_VARIANTS[variant].nt;
-    if (table_driven) *table_driven = ASM_VARIANTS[variant].recipe ? 1 : 0;
     if (available) *available = p->chunk_ptr[variant] != nullptr ? 1 : 0;
     return EMFEM_OK;
 }

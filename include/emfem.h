@@ -107,11 +107,8 @@ int emfem_plan_assemble(emfem_plan plan, int64_t n_nodes, int64_t n_edges, const
  * whose chunk cannot hold the mesh's largest edge/face incidence are unavailable. */
 int emfem_plan_variants(emfem_plan plan, int *n_variants, int *current);
 int emfem_plan_set_variant(emfem_plan plan, int variant);
-/* Variant v: chunk capacity (incidences), threads per CTA, whether it is table-driven (1: pair blocks as
- * the canonical recipes' sparse linear forms, values within rounding of the others; 0: the reference's
- * formulas entry by entry, bit-identical across such variants) and whether this mesh can use it. */
-int emfem_plan_variant_info(emfem_plan plan, int variant, int *chunk, int *threads, int *table_driven,
-                            int *available);
+/* Variant v: chunk capacity (incidences), threads per CTA, and whether this mesh can use it. */
+int emfem_plan_variant_info(emfem_plan plan, int variant, int *chunk, int *threads, int *available);
 /* CSR slot of each (row, col) pair (device int64 arrays of length n), -1 where absent. */
 int emfem_plan_find_slots(emfem_plan plan, int64_t n, const int64_t *rows, const int64_t *cols,
                           int32_t *slots);

@@ -84,10 +84,8 @@ def test_fused_assembly_is_deterministic(cuda):
 
 
 def test_every_kernel_variant_gives_identical_values(cuda):
-    """All assembly variants of one family (chunk sizes, invariants staged in shared memory or read
-    through L1) sum the same contributions in the same order: bit-identical E and B.  The table-driven
-    family evaluates each pair block as its canonical recipe's linear form, a different rounding order:
-    bit-identical within the family and within 1e-14 of the largest entry of each matrix across."""
+    """All assembly variants (chunk sizes, invariants staged in shared memory or read through L1)
+    sum the same contributions in the same order: bit-identical E and B."""
     nodes, tets = box_tet_mesh(7, 6, 5, 0.02, 0.017, 0.03, jitter=0.12, seed=12, shuffle_local=True)
     m = TetMesh(nodes, tets)
     f = Nedelec2(m)
@@ -103,23 +101,18 @@ def test_every_kernel_variant_gives_identical_values(cuda):
     n = ctypes.c_int()
     from emerge_b200._lib import lib as _l
     _l().emfem_plan_variants(plan._p, ctypes.byref(n), None)
-    assert n.value >= 18
-    ref = {}
+    assert n.value >= 13
+    ref = None
     for v in range(n.value):
-        info = plan.variant_info(v)
-        if not info["available"]:
+        if not plan.variant_info(v)["available"]:
             continue
         plan.set_variant(v)
         E, B = plan.assemble(er, ur)
         cur = (E.cpu().numpy(), B.cpu().numpy())
-        fam = info["table_driven"]
-        if fam not in ref:
-            ref[fam] = cur
+        if ref is None:
+            ref = cur
         else:
-            assert np.array_equal(cur[0], ref[fam][0]) and np.array_equal(cur[1], ref[fam][1]), v
-    assert set(ref) == {False, True}
-    for X, Y in zip(ref[False], ref[True]):
-        assert np.abs(X - Y).max() <= 1e-14 * np.abs(X).max()
+            assert np.array_equal(cur[0], ref[0]) and np.array_equal(cur[1], ref[1]), v
 
 
 def test_drop_in_results_never_alias(cuda, small):

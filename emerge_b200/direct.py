@@ -426,9 +426,11 @@ class DeviceLU:
 
 
 def _main(argv=None) -> None:
-    """``python -m emerge_b200.direct --cavity N``: build the N³ dielectric-loaded cavity's sweep, factor
-    its system at one frequency, apply the LU to that frequency's right-hand side once and print the
-    timings (one GPU)."""
+    """``python -m emerge_b200.direct --cavity N`` (or ``--substrate NX NY NZ``): build the N³
+    dielectric-loaded cavity's (or the substrate box's) sweep, factor its system at one frequency in the
+    given precision, apply the LU to that frequency's right-hand side once, optionally (``--refine``)
+    solve that system to 1e-8 with the LU-preconditioned FP64 BiCGStab, and print the timings (one
+    GPU)."""
     import argparse
     import json
     import time
@@ -437,20 +439,29 @@ def _main(argv=None) -> None:
     from .sweep import FrequencySweep
     ap = argparse.ArgumentParser()
     ap.add_argument("--cavity", type=int, default=16, help="hex grid size of the cavity (40: 384 000 tets)")
-    ap.add_argument("--freq-index", type=int, default=50)
+    ap.add_argument("--substrate", type=int, nargs=3, default=None, metavar=("NX", "NY", "NZ"),
+                    help="the substrate box's hex grid instead of the cavity (40 30 26: 187 200 tets)")
+    ap.add_argument("--freq-index", type=int, default=50, help="index into the problem's frequency list")
+    ap.add_argument("--precision", default="c64", choices=["c64", "c128"], help="factorization arithmetic")
+    ap.add_argument("--refine", action="store_true", help="also solve the system to 1e-8 (LU-preconditioned)")
     a = ap.parse_args(argv)
-    P = problems.cavity(n=a.cavity)
+    P = problems.substrate_box(*a.substrate) if a.substrate else problems.cavity(n=a.cavity)
     sw = FrequencySweep(P)
-    f = float(P.freqs[a.freq_index])
-    lu = DeviceLU(sw).factor(f)
+    f = float(P.freqs[min(a.freq_index, len(P.freqs) - 1)])
+    lu = DeviceLU(sw, precision=a.precision).factor(f)
     b = sw.rhs([(f, 0)])
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     lu.solve(b)
     torch.cuda.synchronize()
-    print(json.dumps({"tets": int(P.mesh.n_tets), "dof": int(sw.n), "fronts": lu.n_fronts, "levels": lu.n_levels,
-                      "factor_seconds": lu.seconds_factor, "flops": lu.flops, "device_gb": lu.device_bytes / 1e9,
-                      "solve_seconds": time.perf_counter() - t0, "perturbed_pivots": lu.n_perturbed}))
+    t_solve = time.perf_counter() - t0
+    out = {"tets": int(P.mesh.n_tets), "dof": int(sw.n), "freq": f, "precision": a.precision,
+           "fronts": lu.n_fronts, "levels": lu.n_levels, "factor_seconds": lu.seconds_factor, "flops": lu.flops,
+           "device_gb": lu.device_bytes / 1e9, "solve_seconds": t_solve, "perturbed_pivots": lu.n_perturbed}
+    if a.refine:
+        r = sw.solve_lu([(f, 0)], lu, tol=1e-8, maxit=200)
+        out.update(refined_status=int(r.status[0]), refined_iters=int(r.iters[0]), refined_relres=float(r.relres[0]))
+    print(json.dumps(out))
 
 
 if __name__ == "__main__":

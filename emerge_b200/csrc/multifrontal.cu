@@ -733,6 +733,76 @@ __global__ void mf_bwd_gather_kernel(const int* __restrict__ lst, const FrontMet
 }
 
 // own rows: w[r] -= U12[r, :] x_bnd   (U12 is e x b, column-major with ld e; x_bnd = rows e.. of w)
+// The same U12 product split over the boundary columns for fronts with long boundaries: CTA (row group,
+// column chunk of MF_CW) writes its partial sums to part[chunk][level row][S]; mf_bwd_bnd_sum_kernel
+// then subtracts the chunks in ascending order (deterministic).  A front's own rows [0, e) of its
+// level rows f.wv .. f.wv + n index the partials; chunks past the front's boundary write zeros.
+constexpr int MF_CW = 512;
+__global__ void __launch_bounds__(256) mf_bwd_bnd_split_kernel(const int* __restrict__ lst, const FrontMeta* __restrict__ fm,
+                                                               int S, int nrg, long long wvl,
+                                                               const float2* __restrict__ fact,
+                                                               const float2* __restrict__ w, float2* __restrict__ part) {
+    __shared__ float2 red[8][32][8];
+    const FrontMeta& f = fm[lst[blockIdx.y]];
+    if (f.b == 0) return;
+    const int rg = blockIdx.x % nrg, sp = blockIdx.x / nrg;
+    const long long r0 = (long long)rg * 32;
+    if (r0 >= f.e) return;
+    const int s0 = blockIdx.z * 8, ns = min(8, S - s0);
+    const int rl = threadIdx.x % 32, g = threadIdx.x / 32;
+    const long long r = r0 + rl;
+    const bool live = r < f.e;
+    const float2* W = w + f.wv * S;
+    const float2* M = fact + f.fact + (long long)f.n * f.e;
+    const long long c0 = min((long long)sp * MF_CW, (long long)f.b), c1 = min(c0 + MF_CW, (long long)f.b);
+    float2 acc[8];
+#pragma unroll
+    for (int q = 0; q < 8; q++) acc[q] = make_float2(0.f, 0.f);
+    if (live) {
+#pragma unroll 8
+        for (long long c = c0 + g; c < c1; c += 8) {
+            float2 mv = M[r + c * f.e];
+            const float2* xc = W + (f.e + c) * S + s0;
+#pragma unroll
+            for (int q = 0; q < 8; q++)
+                if (q < ns) cfma(acc[q], mv, xc[q]);
+        }
+    }
+#pragma unroll
+    for (int q = 0; q < 8; q++) red[g][rl][q] = acc[q];
+    __syncthreads();
+    if (g == 0 && live) {
+        float2* P = part + ((long long)sp * wvl + f.wv + r) * S + s0;
+        for (int q = 0; q < ns; q++) {
+            float2 t = make_float2(0.f, 0.f);
+#pragma unroll
+            for (int gg = 0; gg < 8; gg++) { t.x += red[gg][rl][q].x; t.y += red[gg][rl][q].y; }
+            P[q] = t;
+        }
+    }
+}
+
+__global__ void mf_bwd_bnd_sum_kernel(const int* __restrict__ lst, const FrontMeta* __restrict__ fm, int S, int nsplit,
+                                      long long wvl, const float2* __restrict__ part, float2* __restrict__ w) {
+    const FrontMeta& f = fm[lst[blockIdx.y]];
+    if (f.b == 0) return;
+    const long long tot = (long long)f.e * S;
+    const long long i0 = (long long)blockIdx.x * MF_CHUNK;
+    if (i0 >= tot) return;
+    const long long i1 = min(i0 + MF_CHUNK, tot);
+    float2* W = w + f.wv * S;
+    for (long long idx = i0 + threadIdx.x; idx < i1; idx += blockDim.x) {
+        float2 t = make_float2(0.f, 0.f);
+        for (int sp = 0; sp < nsplit; sp++) {
+            float2 v = part[((long long)sp * wvl + f.wv) * S + idx];
+            t.x += v.x;
+            t.y += v.y;
+        }
+        W[idx].x -= t.x;
+        W[idx].y -= t.y;
+    }
+}
+
 __global__ void __launch_bounds__(256) mf_bwd_bnd_kernel(const int* __restrict__ lst, const FrontMeta* __restrict__ fm,
                                                          int S, const float2* __restrict__ fact, float2* __restrict__ w) {
     __shared__ float2 red[8][32][8];
@@ -887,6 +957,9 @@ struct emfem_mf_s {
     int* d_npert = nullptr;
     long long fact_n = 0, inv_n = 0, piv_n = 0, ws_n = 0, upd_n = 0;
     long long wv_n = 0, uv_n = 0, y_n = 0;        // solve buffer rows
+    std::vector<long long> lvl_wv, lvl_max_ob;    // per level: its fronts' rows (sum of n), largest own boundary
+    long long part_n = 0;                         // split U12 partials: max over levels of chunks x level rows
+    float2* spart = nullptr;                      // (part_n, S) partial sums of the split backward products
     // solve buffers for the current S
     int S = 0;
     float2 *sw = nullptr, *suv = nullptr, *sy = nullptr, *sx = nullptr;
@@ -899,7 +972,7 @@ struct emfem_mf_s {
 
 static void mf_free(emfem_mf_s* m) {
     void* ps[] = {m->d_meta, m->d_lst, m->d_fdof, m->d_ea, m->d_slot, m->d_off, m->d_free, m->d_scale, m->fact, m->inv, m->piv,
-                  m->ws, m->upd, m->invc, m->d_npert, m->sw, m->suv, m->sy, m->sx};
+                  m->ws, m->upd, m->invc, m->d_npert, m->sw, m->suv, m->sy, m->sx, m->spart};
     for (void* p : ps)
         if (p) cudaFree(p);
 }
@@ -911,11 +984,12 @@ static inline unsigned nblk(long long items, long long per) {
 
 static int mf_reserve(emfem_mf_s* m, int S) {
     if (m->S >= S) return EMFEM_OK;
-    void* ps[] = {m->sw, m->suv, m->sy, m->sx};
+    void* ps[] = {m->sw, m->suv, m->sy, m->sx, m->spart};
     for (void* p : ps)
         if (p) cudaFree(p);
-    m->sw = m->suv = m->sy = m->sx = nullptr;
+    m->sw = m->suv = m->sy = m->sx = m->spart = nullptr;
     m->S = 0;
+    if (m->part_n > 0) EMFEM_CUDA(cudaMalloc(&m->spart, sizeof(float2) * m->part_n * S));
     EMFEM_CUDA(cudaMalloc(&m->sw, sizeof(float2) * std::max(1LL, m->wv_n) * S));
     EMFEM_CUDA(cudaMalloc(&m->suv, sizeof(float2) * std::max(1LL, m->uv_n) * S));
     EMFEM_CUDA(cudaMalloc(&m->sy, sizeof(float2) * std::max(1LL, m->y_n) * S));
@@ -970,8 +1044,19 @@ int mf_apply(emfem_mf_s* m, int S, const double2* r, double2* x, cudaStream_t s)
             dim3 g(nblk(maxn * S, MF_CHUNK), ny);
             mf_bwd_gather_kernel<<<g, 256, 0, s>>>(lst + y0, m->d_meta, S, m->d_fdof, m->sy, m->sx, m->sw);
             const unsigned sz = (unsigned)((S + 7) / 8);
-            dim3 gb(nblk(maxe, 32), ny, sz);
-            mf_bwd_bnd_kernel<<<gb, 256, 0, s>>>(lst + y0, m->d_meta, S, m->fact, m->sw);
+            const long long nsplit = (m->lvl_max_ob[L] + MF_CW - 1) / MF_CW;
+            if (nsplit > 1 && nfl < 148) {
+                const unsigned nrg = nblk(maxe, 32);
+                dim3 gb(nrg * (unsigned)nsplit, ny, sz);
+                mf_bwd_bnd_split_kernel<<<gb, 256, 0, s>>>(lst + y0, m->d_meta, S, (int)nrg, m->lvl_wv[L], m->fact,
+                                                          m->sw, m->spart);
+                dim3 gs(nblk(maxe * S, MF_CHUNK), ny);
+                mf_bwd_bnd_sum_kernel<<<gs, 256, 0, s>>>(lst + y0, m->d_meta, S, (int)nsplit, m->lvl_wv[L], m->spart,
+                                                        m->sw);
+            } else {
+                dim3 gb(nblk(maxe, 32), ny, sz);
+                mf_bwd_bnd_kernel<<<gb, 256, 0, s>>>(lst + y0, m->d_meta, S, m->fact, m->sw);
+            }
             const int nblocks = (int)((maxe + MF_SB - 1) / MF_SB);
             for (int bi = nblocks - 1; bi >= 0; bi--) {
                 const int k0 = bi * MF_SB;
@@ -1112,6 +1197,7 @@ int emfem_mf_create(emfem_handle h, int64_t n, int n_fronts, const int32_t* e, c
     };
     long long uv = 0;
     m->lvl_max_e.assign(nl, 0); m->lvl_max_n.assign(nl, 0); m->lvl_max_asm.assign(nl, 0); m->lvl_max_b.assign(nl, 0);
+    m->lvl_wv.assign(nl, 0); m->lvl_max_ob.assign(nl, 0);
     for (int L = 0; L < nl; L++) {
         long long wso = 0, wvo = 0;
         for (int v : m->levels[L]) {
@@ -1125,9 +1211,14 @@ int emfem_mf_create(emfem_handle h, int64_t n, int n_fronts, const int32_t* e, c
             long long cb = 0;
             for (int c : f.child) if (c >= 0) cb = std::max<long long>(cb, m->meta[c].b);
             m->lvl_max_b[L] = std::max(m->lvl_max_b[L], cb);
+            m->lvl_max_ob[L] = std::max<long long>(m->lvl_max_ob[L], f.b);
         }
         ws_max = std::max(ws_max, wso);
         wv_max = std::max(wv_max, wvo);
+        m->lvl_wv[L] = wvo;
+        // levels of few fronts (the top of the tree) split their long boundary products over CTAs
+        const long long nsplit = (m->lvl_max_ob[L] + MF_CW - 1) / MF_CW;
+        if (nsplit > 1 && m->levels[L].size() < 148) m->part_n = std::max(m->part_n, nsplit * wvo);
         // the level's fronts get their update blocks; their children's are freed once the level assembled
         for (int v : m->levels[L]) {
             FrontMeta& f = m->meta[v];

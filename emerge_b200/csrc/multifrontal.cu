@@ -650,30 +650,50 @@ __global__ void __launch_bounds__(256) mf_fwd_block_kernel(const int* __restrict
 // w[r] -= sum_{c in [c0, c1)} M[r, c] x[c] for the rows [r0, r1) of a front, M column-major with leading
 // dimension ldm, x = rows c of w (or of xsrc).  A CTA owns 32 rows; its 8 warps take every 8th column
 // and their sums meet in shared memory.  8 right-hand sides per CTA (grid.z).
-__device__ __forceinline__ void mf_gemv_rows(float2* W, int S, long long r, int rl, int g, bool live, const float2* M,
-                                             long long ldm, long long c0, long long c1, const float2* X,
-                                             long long xrow0, int s0, int ns, float2 (*red)[32][8]) {
-    float2 acc[8];
+// RPL row sets per lane: lane rl of warp g holds rows rb + rl + 32 i (i < RPL), so a warp streams
+// 32 * RPL consecutive rows (256 * RPL contiguous bytes) of every column it visits, with RPL loads in
+// flight per column.  Each row sums its columns in the same order as with one row set (bit-identical).
+constexpr int MF_RPL = 2;
+template <int RPL>
+__device__ __forceinline__ void mf_gemv_rowsets(float2* W, int S, long long rb, int rl, int g, long long rlim,
+                                                const float2* M, long long ldm, long long c0, long long c1,
+                                                const float2* X, long long xrow0, int s0, int ns,
+                                                float2 (*red)[32 * RPL][8]) {
+    float2 acc[RPL][8];
 #pragma unroll
-    for (int q = 0; q < 8; q++) acc[q] = make_float2(0.f, 0.f);
-    if (live) {
-#pragma unroll 8
+    for (int i = 0; i < RPL; i++)
+#pragma unroll
+        for (int q = 0; q < 8; q++) acc[i][q] = make_float2(0.f, 0.f);
+    bool live[RPL];
+#pragma unroll
+    for (int i = 0; i < RPL; i++) live[i] = rb + rl + 32 * i < rlim;
+    if (live[0]) {
+#pragma unroll 4
         for (long long c = c0 + g; c < c1; c += 8) {
-            float2 mv = M[r + c * ldm];
+            float2 mv[RPL];
+#pragma unroll
+            for (int i = 0; i < RPL; i++) mv[i] = live[i] ? M[rb + rl + 32 * i + c * ldm] : make_float2(0.f, 0.f);
             const float2* xc = X + (xrow0 + c - c0) * S + s0;
 #pragma unroll
             for (int q = 0; q < 8; q++)
-                if (q < ns) cfma(acc[q], mv, xc[q]);
+                if (q < ns) {
+                    const float2 xv = xc[q];
+#pragma unroll
+                    for (int i = 0; i < RPL; i++) cfma(acc[i][q], mv[i], xv);
+                }
         }
     }
 #pragma unroll
-    for (int q = 0; q < 8; q++) red[g][rl][q] = acc[q];
+    for (int i = 0; i < RPL; i++)
+#pragma unroll
+        for (int q = 0; q < 8; q++) red[g][rl + 32 * i][q] = acc[i][q];
     __syncthreads();
-    if (g == 0 && live) {
+    if (g < RPL && live[g]) {
+        const long long r = rb + rl + 32 * g;
         for (int q = 0; q < ns; q++) {
             float2 t = make_float2(0.f, 0.f);
 #pragma unroll
-            for (int gg = 0; gg < 8; gg++) { t.x += red[gg][rl][q].x; t.y += red[gg][rl][q].y; }
+            for (int gg = 0; gg < 8; gg++) { t.x += red[gg][rl + 32 * g][q].x; t.y += red[gg][rl + 32 * g][q].y; }
             float2* p = W + r * S + s0 + q;
             p->x -= t.x;
             p->y -= t.y;
@@ -685,17 +705,16 @@ __device__ __forceinline__ void mf_gemv_rows(float2* W, int S, long long r, int 
 __global__ void __launch_bounds__(256) mf_fwd_update_kernel(const int* __restrict__ lst, const FrontMeta* __restrict__ fm,
                                                             int S, int k0, const float2* __restrict__ fact,
                                                             float2* __restrict__ w) {
-    __shared__ float2 red[8][32][8];
+    __shared__ float2 red[8][32 * MF_RPL][8];
     const FrontMeta& f = fm[lst[blockIdx.y]];
     if (k0 >= f.e) return;
     const int k1 = min(k0 + MF_SB, f.e);
-    const long long r0 = k1 + (long long)blockIdx.x * 32;
+    const long long r0 = k1 + (long long)blockIdx.x * 32 * MF_RPL;
     if (r0 >= f.n) return;
     const int s0 = blockIdx.z * 8, ns = min(8, S - s0);
     const int rl = threadIdx.x % 32, g = threadIdx.x / 32;
-    const long long r = r0 + rl;
     float2* W = w + f.wv * S;
-    mf_gemv_rows(W, S, r, rl, g, r < f.n, fact + f.fact, f.n, k0, k1, W, k0, s0, ns, red);
+    mf_gemv_rowsets<MF_RPL>(W, S, r0, rl, g, f.n, fact + f.fact, f.n, k0, k1, W, k0, s0, ns, red);
 }
 
 // own rows -> y store, boundary rows -> update vector for the parent
@@ -805,16 +824,16 @@ __global__ void mf_bwd_bnd_sum_kernel(const int* __restrict__ lst, const FrontMe
 
 __global__ void __launch_bounds__(256) mf_bwd_bnd_kernel(const int* __restrict__ lst, const FrontMeta* __restrict__ fm,
                                                          int S, const float2* __restrict__ fact, float2* __restrict__ w) {
-    __shared__ float2 red[8][32][8];
+    __shared__ float2 red[8][32 * MF_RPL][8];
     const FrontMeta& f = fm[lst[blockIdx.y]];
     if (f.b == 0) return;
-    const long long r0 = (long long)blockIdx.x * 32;
+    const long long r0 = (long long)blockIdx.x * 32 * MF_RPL;
     if (r0 >= f.e) return;
     const int s0 = blockIdx.z * 8, ns = min(8, S - s0);
     const int rl = threadIdx.x % 32, g = threadIdx.x / 32;
-    const long long r = r0 + rl;
     float2* W = w + f.wv * S;
-    mf_gemv_rows(W, S, r, rl, g, r < f.e, fact + f.fact + (long long)f.n * f.e, f.e, 0, f.b, W, f.e, s0, ns, red);
+    mf_gemv_rowsets<MF_RPL>(W, S, r0, rl, g, f.e, fact + f.fact + (long long)f.n * f.e, f.e, 0, f.b, W, f.e, s0, ns,
+                            red);
 }
 
 // Backward solve inside the block [k0, k1), held in shared memory: 32-steps from the last,
@@ -882,17 +901,16 @@ __global__ void __launch_bounds__(256) mf_bwd_block_kernel(const int* __restrict
 __global__ void __launch_bounds__(256) mf_bwd_update_kernel(const int* __restrict__ lst, const FrontMeta* __restrict__ fm,
                                                             int S, int k0, const float2* __restrict__ fact,
                                                             float2* __restrict__ w) {
-    __shared__ float2 red[8][32][8];
+    __shared__ float2 red[8][32 * MF_RPL][8];
     const FrontMeta& f = fm[lst[blockIdx.y]];
     if (k0 >= f.e) return;
     const int k1 = min(k0 + MF_SB, f.e);
-    const long long r0 = (long long)blockIdx.x * 32;
+    const long long r0 = (long long)blockIdx.x * 32 * MF_RPL;
     if (r0 >= k0) return;
     const int s0 = blockIdx.z * 8, ns = min(8, S - s0);
     const int rl = threadIdx.x % 32, g = threadIdx.x / 32;
-    const long long r = r0 + rl;
     float2* W = w + f.wv * S;
-    mf_gemv_rows(W, S, r, rl, g, r < k0, fact + f.fact, f.n, k0, k1, W, k0, s0, ns, red);
+    mf_gemv_rowsets<MF_RPL>(W, S, r0, rl, g, k0, fact + f.fact, f.n, k0, k1, W, k0, s0, ns, red);
 }
 
 __global__ void mf_bwd_finish_kernel(const int* __restrict__ lst, const FrontMeta* __restrict__ fm, int S,
@@ -1027,7 +1045,7 @@ int mf_apply(emfem_mf_s* m, int S, const double2* r, double2* x, cudaStream_t s)
                     mf_fwd_block_kernel<2><<<ny, 256, MF_BLOCK_SMEM2, s>>>(lst + y0, m->d_meta, S, k0, m->fact, m->inv, m->sw);
                 else
                     mf_fwd_block_kernel<1><<<ny, 256, MF_BLOCK_SMEM, s>>>(lst + y0, m->d_meta, S, k0, m->fact, m->inv, m->sw);
-                dim3 gu(nblk(maxn - k0, 32), ny, sz);   // rows [k1, n) of a front: at most n - k0
+                dim3 gu(nblk(maxn - k0, 32 * MF_RPL), ny, sz);   // rows [k1, n) of a front: at most n - k0
                 mf_fwd_update_kernel<<<gu, 256, 0, s>>>(lst + y0, m->d_meta, S, k0, m->fact, m->sw);
             }
             mf_fwd_finish_kernel<<<g, 256, 0, s>>>(lst + y0, m->d_meta, S, m->sw, m->sy, m->suv);
@@ -1054,7 +1072,7 @@ int mf_apply(emfem_mf_s* m, int S, const double2* r, double2* x, cudaStream_t s)
                 mf_bwd_bnd_sum_kernel<<<gs, 256, 0, s>>>(lst + y0, m->d_meta, S, (int)nsplit, m->lvl_wv[L], m->spart,
                                                         m->sw);
             } else {
-                dim3 gb(nblk(maxe, 32), ny, sz);
+                dim3 gb(nblk(maxe, 32 * MF_RPL), ny, sz);
                 mf_bwd_bnd_kernel<<<gb, 256, 0, s>>>(lst + y0, m->d_meta, S, m->fact, m->sw);
             }
             const int nblocks = (int)((maxe + MF_SB - 1) / MF_SB);
@@ -1065,7 +1083,7 @@ int mf_apply(emfem_mf_s* m, int S, const double2* r, double2* x, cudaStream_t s)
                 else
                     mf_bwd_block_kernel<1><<<ny, 256, MF_BLOCK_SMEM, s>>>(lst + y0, m->d_meta, S, k0, m->fact, m->inv, m->sw);
                 if (k0 > 0) {
-                    dim3 gu(nblk(k0, 32), ny, sz);
+                    dim3 gu(nblk(k0, 32 * MF_RPL), ny, sz);
                     mf_bwd_update_kernel<<<gu, 256, 0, s>>>(lst + y0, m->d_meta, S, k0, m->fact, m->sw);
                 }
             }

@@ -225,6 +225,32 @@ struct InvView {
     EMFEM_HD double L(int e) const { return g(INV_L + e); }
 };
 
+// The same accessors over one tet's record in the array-of-structs buffer (records of INV_STRIDE doubles,
+// 16-byte aligned): on the device every complex invariant is one 16-byte load instead of two 8-byte
+// ones, with the same values (so the same results) as InvView.
+struct InvRec {
+    const double* base;
+    EMFEM_HD double g(int f) const { return base[f]; }
+    EMFEM_HD cd c(int f) const {
+#if defined(__CUDA_ARCH__)
+        const double2 v = __ldg(reinterpret_cast<const double2*>(base + f));
+        return mk(v.x, v.y);
+#else
+        return mk(base[f], base[f + 1]);
+#endif
+    }
+    EMFEM_HD cd P(int a, int b) const { return c(INV_P + 2 * (4 * a + b)); }
+    EMFEM_HD cd Q(int a, int b, int cc, int d) const {
+        int p = pair_index(a, b), q = pair_index(cc, d);
+        double s = ((a < b) == (cc < d)) ? 1.0 : -1.0;
+        cd v = c(INV_Q + 2 * (6 * p + q));
+        return mk(s * v.x, s * v.y);
+    }
+    EMFEM_HD double Ds(int a, int b) const { return g(INV_DS + pair_index(a, b)); }
+    EMFEM_HD double L(int e) const { return g(INV_L + e); }
+};
+static_assert(INV_STRIDE % 2 == 0 && INV_P % 2 == 0 && INV_Q % 2 == 0, "complex invariants are 16-byte aligned");
+
 // Volume coefficient table: vc[A*125 + B*25 + C*5 + D] = prod k_i! / (sum k_i + 3)!,
 // letters 1..4 name vertices, 0 = absent (curlcurl.py:64-92).
 EMFEM_HD void fill_volume_table(double* vc) {
@@ -248,7 +274,8 @@ struct VTab {
 // One pair block: row entity slot sx, column entity slot sy (0..5 edges, 6..9 faces).
 // d[0..3] = D at (x1,y1),(x1,y2),(x2,y1),(x2,y2) (1 = first-kind DOF, 2 = second-kind), f[] same for F.
 // Values include the final element scaling.
-EMFEM_HD void pair_block(const InvView& I, const Orient& o, const VTab& T, int sx, int sy, cd d[4], cd f[4]) {
+template <class IV>
+EMFEM_HD void pair_block(const IV& I, const Orient& o, const VTab& T, int sx, int sy, cd d[4], cd f[4]) {
     const bool xe = sx < 6, ye = sy < 6;
     if (xe && ye) {
         int a, b, c, dd; o.edge(sx, a, b); o.edge(sy, c, dd);

@@ -410,11 +410,14 @@ __global__ void __launch_bounds__(NT, MINB) assemble_chunk_kernel(
             if (li >= ninc) continue;
         }
         int sx = (int)((srec[li].z >> 16) & 0xff);  // byte 10 of the record
-        InvView I = SINV ? InvView{sinv + li * INV_SMEM_STRIDE, 1}
-                         : InvView{inv + (long long)(scode[li] >> 4) * INV_STRIDE, 1};
-        Orient o = unpack_rank((int)I.g(INV_RANK));
         cd d[4], f[4];
-        pair_block(I, o, T, sx, sy, d, f);
+        if constexpr (SINV) {
+            const InvView I{sinv + li * INV_SMEM_STRIDE, 1};
+            pair_block(I, unpack_rank((int)I.g(INV_RANK)), T, sx, sy, d, f);
+        } else {
+            const InvRec I{inv + (long long)(scode[li] >> 4) * INV_STRIDE};
+            pair_block(I, unpack_rank((int)I.g(INV_RANK)), T, sx, sy, d, f);
+        }
 #pragma unroll
         for (int q = 0; q < 4; q++) {
             stage[(q * 10 + sy) * (CH + 1) + li] = make_double2(d[q].x, d[q].y);

@@ -477,8 +477,10 @@ def configs_sweep_section(n_meshes: int = 16, tol: float = 1e-8) -> dict:
                       "setup_seconds": t_setup, "iters_max": int(rd.iters.max()),
                       "relres_max": float(rd.relres.max()), "windows": len(rd.windows),
                       "precision": "auto (complex64 first, complex128 for the systems it leaves)",
-                      "factorizations_c128": sum(1 for w in rd.windows if w["precision"] == "c128"),
-                      "c128_frequencies_max": max([w["factored"] for w in rd.windows if w["precision"] == "c128"],
+                      "factorizations_c128": sum(1 for w in rd.windows
+                                                 if w["precision"] == "c128" and w.get("factor_seconds", 0) > 0),
+                      "c128_frequencies_max": max([w["factored"] for w in rd.windows
+                                                   if w["precision"] == "c128" and "error" not in w],
                                                   default=None)},
         "aux_krylov_top8_freqs": {"converged": int((rk.status == 0).sum()), "seconds": rk.seconds,
                                   "iters_max": int(rk.iters.max())},

@@ -509,7 +509,9 @@ class FrequencySweep:
         unconverged are solved again from a complex128 factorization at the same frequency (at low
         frequency the near-null gradient space makes K ill-conditioned enough that complex64 fronts give
         no usable preconditioner).  After a complex128 window that needed fewer than ``iter_band[0]``
-        iterations, the next window tries complex64 again.  Results come back in the order of
+        iterations, the next window tries complex64 again.  If the complex128 workspace does not fit on
+        the device, the complex64 results stand (status shows what did not converge), the window log
+        records the failed switch, and the rest of the sweep stays complex64.  Results come back in the order of
         ``systems``; ``windows`` on the result lists (factored frequency, precision, systems, factor
         seconds, solve seconds, iterations) per attempt."""
         if precision not in ("c64", "c128", "auto"):
@@ -525,6 +527,7 @@ class FrequencySweep:
         log = []
         w0, W = 0, window
         first = "c128" if precision == "c128" else "c64"
+        c128_fits = True
         while w0 < len(freqs):
             wf = freqs[w0:w0 + W]
             w0 += len(wf)
@@ -532,13 +535,24 @@ class FrequencySweep:
             todo = [j for j, (f, _) in enumerate(systems) if f in fw]
             fc = wf[len(wf) // 2]
             imax = 0
-            attempts = [first] if precision != "auto" or first == "c128" else ["c64", "c128"]
+            if precision != "auto" or first == "c128":
+                attempts = [first]
+            else:
+                attempts = ["c64", "c128"] if c128_fits else ["c64"]
             for prec in attempts:
                 if not todo:
                     break
                 last = prec == attempts[-1]
                 imax = 0                          # the window width follows the attempt that finished it
-                lu.set_precision(prec)
+                try:
+                    lu.set_precision(prec)
+                except RuntimeError as exc:
+                    if precision != "auto":
+                        raise
+                    # the complex128 workspace does not fit: the complex64 results stand
+                    c128_fits, first = False, "c64"
+                    log.append(dict(factored=fc, precision=prec, systems=len(todo), error=str(exc)))
+                    break
                 tf = time.perf_counter()
                 lu.factor(fc)
                 tf = time.perf_counter() - tf
@@ -548,22 +562,21 @@ class FrequencySweep:
                     sub = todo[c0:c0 + 64]
                     r = self.solve_lu([systems[j] for j in sub], lu, tol=tol, maxit=it_cap)
                     ok = (r.status == 0) & (r.relres <= tol)
-                    keep = [i for i in range(len(sub)) if ok[i] or last]
-                    ks = [sub[i] for i in keep]
-                    x[:, ks] = r.x[:, keep]
-                    status[ks] = r.status[keep]
-                    iters[ks] = r.iters[keep]
-                    relres[ks] = r.relres[keep]
-                    left += [sub[i] for i in range(len(sub)) if not (ok[i] or last)]
+                    x[:, sub] = r.x
+                    status[sub] = r.status
+                    iters[sub] = r.iters
+                    relres[sub] = r.relres
+                    left += [sub[i] for i in range(len(sub)) if not ok[i]]
                     log.append(dict(factored=fc, precision=prec, systems=len(sub), factor_seconds=tf,
                                     solve_seconds=r.seconds, iters=r.iters.tolist(), perturbed=lu.n_perturbed))
                     tf = 0.0
-                    imax = max(imax, int(r.iters[keep].max()) if keep else it_cap)
-                todo = left
+                    conv = r.iters if last else r.iters[ok]
+                    imax = max(imax, int(conv.max()) if conv.size else it_cap)
+                todo = [] if last else left
                 if precision == "auto":
                     if prec == "c128":
                         first = "c64" if imax < iter_band[0] else "c128"
-                    elif left:
+                    elif left and c128_fits:
                         first = "c128"
             if adaptive:
                 if imax > iter_band[1] and W > 3:

@@ -590,8 +590,11 @@ __device__ __forceinline__ void mf_stage_step(float2* li, float2 (*pan)[MF_NB + 
     cp_async_commit();
 }
 
-template <int NBUF>
-__global__ void __launch_bounds__(256) mf_fwd_block_kernel(const int* __restrict__ lst, const FrontMeta* __restrict__ fm,
+// NT threads: 256 on levels of many fronts (several CTAs per SM), 1024 on levels of few fronts, where the
+// block chain of one front is serial and a step's items (rows x right-hand sides) spread over more threads.
+constexpr int MF_BLOCK_NT_FEW = 1024;
+template <int NBUF, int NT>
+__global__ void __launch_bounds__(NT) mf_fwd_block_kernel(const int* __restrict__ lst, const FrontMeta* __restrict__ fm,
                                                            int S, int k0, const float2* __restrict__ fact,
                                                            const float2* __restrict__ inv, float2* __restrict__ w) {
     extern __shared__ __align__(16) unsigned char mf_smem[];
@@ -839,8 +842,8 @@ __global__ void __launch_bounds__(256) mf_bwd_bnd_kernel(const int* __restrict__
 // Backward solve inside the block [k0, k1), held in shared memory: 32-steps from the last,
 // x_k = Uinv (w_k), then the block's earlier rows.  One CTA per front, 16 right-hand sides at a time;
 // each step's Uinv block and U panel (the block's rows above the step) staged in shared memory first.
-template <int NBUF>
-__global__ void __launch_bounds__(256) mf_bwd_block_kernel(const int* __restrict__ lst, const FrontMeta* __restrict__ fm,
+template <int NBUF, int NT>
+__global__ void __launch_bounds__(NT) mf_bwd_block_kernel(const int* __restrict__ lst, const FrontMeta* __restrict__ fm,
                                                            int S, int k0, const float2* __restrict__ fact,
                                                            const float2* __restrict__ inv, float2* __restrict__ w) {
     extern __shared__ __align__(16) unsigned char mf_smem[];
@@ -1042,9 +1045,10 @@ int mf_apply(emfem_mf_s* m, int S, const double2* r, double2* x, cudaStream_t s)
             const unsigned sz = (unsigned)((S + 7) / 8);
             for (int k0 = 0; k0 < m->lvl_max_e[L]; k0 += MF_SB) {
                 if (ny < 148)   // a few large fronts: the serial step chain, so overlap its copies
-                    mf_fwd_block_kernel<2><<<ny, 256, MF_BLOCK_SMEM2, s>>>(lst + y0, m->d_meta, S, k0, m->fact, m->inv, m->sw);
+                    mf_fwd_block_kernel<2, MF_BLOCK_NT_FEW><<<ny, MF_BLOCK_NT_FEW, MF_BLOCK_SMEM2, s>>>(
+                        lst + y0, m->d_meta, S, k0, m->fact, m->inv, m->sw);
                 else
-                    mf_fwd_block_kernel<1><<<ny, 256, MF_BLOCK_SMEM, s>>>(lst + y0, m->d_meta, S, k0, m->fact, m->inv, m->sw);
+                    mf_fwd_block_kernel<1, 256><<<ny, 256, MF_BLOCK_SMEM, s>>>(lst + y0, m->d_meta, S, k0, m->fact, m->inv, m->sw);
                 dim3 gu(nblk(maxn - k0, 32 * MF_RPL), ny, sz);   // rows [k1, n) of a front: at most n - k0
                 mf_fwd_update_kernel<<<gu, 256, 0, s>>>(lst + y0, m->d_meta, S, k0, m->fact, m->sw);
             }
@@ -1079,9 +1083,10 @@ int mf_apply(emfem_mf_s* m, int S, const double2* r, double2* x, cudaStream_t s)
             for (int bi = nblocks - 1; bi >= 0; bi--) {
                 const int k0 = bi * MF_SB;
                 if (ny < 148)
-                    mf_bwd_block_kernel<2><<<ny, 256, MF_BLOCK_SMEM2, s>>>(lst + y0, m->d_meta, S, k0, m->fact, m->inv, m->sw);
+                    mf_bwd_block_kernel<2, MF_BLOCK_NT_FEW><<<ny, MF_BLOCK_NT_FEW, MF_BLOCK_SMEM2, s>>>(
+                        lst + y0, m->d_meta, S, k0, m->fact, m->inv, m->sw);
                 else
-                    mf_bwd_block_kernel<1><<<ny, 256, MF_BLOCK_SMEM, s>>>(lst + y0, m->d_meta, S, k0, m->fact, m->inv, m->sw);
+                    mf_bwd_block_kernel<1, 256><<<ny, 256, MF_BLOCK_SMEM, s>>>(lst + y0, m->d_meta, S, k0, m->fact, m->inv, m->sw);
                 if (k0 > 0) {
                     dim3 gu(nblk(k0, 32 * MF_RPL), ny, sz);
                     mf_bwd_update_kernel<<<gu, 256, 0, s>>>(lst + y0, m->d_meta, S, k0, m->fact, m->sw);
@@ -1304,16 +1309,16 @@ int emfem_mf_create(emfem_handle h, int64_t n, int n_fronts, const int32_t* e, c
     mk((void**)&m->d_npert, sizeof(int));
     mk((void**)&m->d_scale, sizeof(double) * n);
     if (rc != EMFEM_OK) { mf_free(m); delete m; return rc; }
-    rc = check_cuda(cudaFuncSetAttribute(mf_fwd_block_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    rc = check_cuda(cudaFuncSetAttribute(mf_fwd_block_kernel<1, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)MF_BLOCK_SMEM), "cudaFuncSetAttribute");
     if (rc == EMFEM_OK)
-        rc = check_cuda(cudaFuncSetAttribute(mf_bwd_block_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        rc = check_cuda(cudaFuncSetAttribute(mf_bwd_block_kernel<1, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              (int)MF_BLOCK_SMEM), "cudaFuncSetAttribute");
     if (rc == EMFEM_OK)
-        rc = check_cuda(cudaFuncSetAttribute(mf_fwd_block_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        rc = check_cuda(cudaFuncSetAttribute(mf_fwd_block_kernel<2, MF_BLOCK_NT_FEW>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              (int)MF_BLOCK_SMEM2), "cudaFuncSetAttribute");
     if (rc == EMFEM_OK)
-        rc = check_cuda(cudaFuncSetAttribute(mf_bwd_block_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        rc = check_cuda(cudaFuncSetAttribute(mf_bwd_block_kernel<2, MF_BLOCK_NT_FEW>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              (int)MF_BLOCK_SMEM2), "cudaFuncSetAttribute");
     if (rc != EMFEM_OK) { mf_free(m); delete m; return rc; }
     *out = m;

@@ -764,41 +764,53 @@ __global__ void __launch_bounds__(256) mf_bwd_bnd_split_kernel(const int* __rest
                                                                int S, int nrg, long long wvl,
                                                                const float2* __restrict__ fact,
                                                                const float2* __restrict__ w, float2* __restrict__ part) {
-    __shared__ float2 red[8][32][8];
+    __shared__ float2 red[8][32 * MF_RPL][8];
     const FrontMeta& f = fm[lst[blockIdx.y]];
     if (f.b == 0) return;
     const int rg = blockIdx.x % nrg, sp = blockIdx.x / nrg;
-    const long long r0 = (long long)rg * 32;
+    const long long r0 = (long long)rg * 32 * MF_RPL;
     if (r0 >= f.e) return;
     const int s0 = blockIdx.z * 8, ns = min(8, S - s0);
     const int rl = threadIdx.x % 32, g = threadIdx.x / 32;
-    const long long r = r0 + rl;
-    const bool live = r < f.e;
     const float2* W = w + f.wv * S;
     const float2* M = fact + f.fact + (long long)f.n * f.e;
     const long long c0 = min((long long)sp * MF_CW, (long long)f.b), c1 = min(c0 + MF_CW, (long long)f.b);
-    float2 acc[8];
+    float2 acc[MF_RPL][8];
+    bool live[MF_RPL];
 #pragma unroll
-    for (int q = 0; q < 8; q++) acc[q] = make_float2(0.f, 0.f);
-    if (live) {
-#pragma unroll 8
+    for (int i = 0; i < MF_RPL; i++) {
+        live[i] = r0 + rl + 32 * i < f.e;
+#pragma unroll
+        for (int q = 0; q < 8; q++) acc[i][q] = make_float2(0.f, 0.f);
+    }
+    if (live[0]) {
+#pragma unroll 4
         for (long long c = c0 + g; c < c1; c += 8) {
-            float2 mv = M[r + c * f.e];
+            float2 mv[MF_RPL];
+#pragma unroll
+            for (int i = 0; i < MF_RPL; i++) mv[i] = live[i] ? M[r0 + rl + 32 * i + c * f.e] : make_float2(0.f, 0.f);
             const float2* xc = W + (f.e + c) * S + s0;
 #pragma unroll
             for (int q = 0; q < 8; q++)
-                if (q < ns) cfma(acc[q], mv, xc[q]);
+                if (q < ns) {
+                    const float2 xv = xc[q];
+#pragma unroll
+                    for (int i = 0; i < MF_RPL; i++) cfma(acc[i][q], mv[i], xv);
+                }
         }
     }
 #pragma unroll
-    for (int q = 0; q < 8; q++) red[g][rl][q] = acc[q];
+    for (int i = 0; i < MF_RPL; i++)
+#pragma unroll
+        for (int q = 0; q < 8; q++) red[g][rl + 32 * i][q] = acc[i][q];
     __syncthreads();
-    if (g == 0 && live) {
+    if (g < MF_RPL && live[g]) {
+        const long long r = r0 + rl + 32 * g;
         float2* P = part + ((long long)sp * wvl + f.wv + r) * S + s0;
         for (int q = 0; q < ns; q++) {
             float2 t = make_float2(0.f, 0.f);
 #pragma unroll
-            for (int gg = 0; gg < 8; gg++) { t.x += red[gg][rl][q].x; t.y += red[gg][rl][q].y; }
+            for (int gg = 0; gg < 8; gg++) { t.x += red[gg][rl + 32 * g][q].x; t.y += red[gg][rl + 32 * g][q].y; }
             P[q] = t;
         }
     }
@@ -1068,7 +1080,7 @@ int mf_apply(emfem_mf_s* m, int S, const double2* r, double2* x, cudaStream_t s)
             const unsigned sz = (unsigned)((S + 7) / 8);
             const long long nsplit = (m->lvl_max_ob[L] + MF_CW - 1) / MF_CW;
             if (nsplit > 1 && nfl < 148) {
-                const unsigned nrg = nblk(maxe, 32);
+                const unsigned nrg = nblk(maxe, 32 * MF_RPL);
                 dim3 gb(nrg * (unsigned)nsplit, ny, sz);
                 mf_bwd_bnd_split_kernel<<<gb, 256, 0, s>>>(lst + y0, m->d_meta, S, (int)nrg, m->lvl_wv[L], m->fact,
                                                           m->sw, m->spart);

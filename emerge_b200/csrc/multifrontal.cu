@@ -1,27 +1,31 @@
-// Multifrontal sparse LU of the sweep system on the device (complex64 fronts), the direct solve that
-// replaces the reference's SolverSuperLU (src/emerge/_emerge/solver.py:535-572).
+// Multifrontal sparse LU of the sweep system on the device, the direct solve that replaces the
+// reference's SolverSuperLU (src/emerge/_emerge/solver.py:535-572).  It factors the equilibrated
+// D^-1/2 K D^-1/2 (D = |diag K|) with complex64 fronts, or complex128 fronts after
+// emfem_mf_set_precision(lu, 128); the factor store is complex64 either way.
 //
 // The symbolic structure (nested-dissection tree, front DOF lists, extend-add maps, assembly lists) is
 // built on the host (emerge_b200/direct.py) and uploaded once per mesh.  The numeric factorization runs
 // level by level over the tree (all fronts of one height at once):
-//   1. every front of the level is zeroed and gets its own entries of K (FP64 -> FP32) and the Schur
-//      complements of its children (extend-add, one child slot after the other: no atomics);
+//   1. every front of the level is zeroed and gets its own entries of the scaled K (FP64 -> front
+//      precision) and the Schur complements of its children (extend-add, one child slot after the other:
+//      no atomics);
 //   2. the first e columns of every front are eliminated in steps of 32: LU with partial pivoting inside
 //      the 32 x 32 diagonal block (diag_kernel, one warp per front, also forming the explicit inverses
 //      of its L and U), the block row (row swaps + L^-1) and block column (U^-1) of the panel
 //      (panel_kernel), and the rank-32 update of the trailing matrix (trail_kernel: 64 x 64 tiles,
 //      4 x 4 complex register tiles per thread), every kernel batched over the level's fronts;
 //   3. the factor columns, the U block row and the Schur complement are copied out of the level
-//      workspace (compact_kernel): factors to the factor store, the Schur complement to the update store
-//      until the parent's level consumes it.
+//      workspace (compact_kernel): factors to the factor store (rounded to complex64), the Schur
+//      complement to the update store (front precision) until the parent's level consumes it.
 // Pivoting stays inside each 32-row diagonal block (rows are never exchanged across blocks), so row swaps
 // touch only the block row; the solves apply them step by step.  A pivot smaller than 1e-6 of its block's
 // largest entry is raised to that floor and counted: the factorization is a preconditioner under an FP64
 // Krylov iteration, which removes such perturbations.
 //
-// Solves (M^-1 r for S right-hand sides, FP64 in and out, FP32 inside) run the same tree: forward in
-// level order (gather, children's update vectors, blocked L solve with 256-row blocks, update vector for
-// the parent), backward in reverse (gather of the solved boundary, U12 product, blocked U solve).
+// Solves (M^-1 r for S right-hand sides, FP64 in and out, FP32 inside, scaled by D^-1/2 on the way in
+// and out) run the same tree: forward in level order (gather, children's update vectors, blocked L solve
+// with 256-row blocks, update vector for the parent), backward in reverse (gather of the solved boundary,
+// U12 product, blocked U solve).
 #include "emfem_internal.cuh"
 
 #include <algorithm>
